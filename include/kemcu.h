@@ -1,0 +1,175 @@
+/*
+ * kemcu.h -- C ABI of the B200 (sm_100a) backend for KEMField's electrostatic
+ * boundary-element hot path.
+ *
+ * Plain C: pointers, sizes and status codes only. A context owns one CUDA device and one
+ * stream; it is not re-entrant (the reference's solvers are not either, they keep static
+ * locals, KBoundaryIntegralMatrix.hh:42-44), but separate contexts may be used from
+ * separate threads. All functions return KEMCU_OK (0) or a negative KEMCU_E* code; the
+ * message of the last failure is kemcu_last_error(ctx). There is no CPU fallback: a missing
+ * or failing GPU is reported, never worked around.
+ *
+ * Element encoding (the flattened KSurfaceContainer, KSurfaceContainer.cc:36-72; element
+ * index = matrix row/column index):
+ *   shape[i]    KEMCU_TRIANGLE | KEMCU_RECTANGLE | KEMCU_LINE_SEGMENT
+ *   boundary[i] KEMCU_DIRICHLET (value = potential, KDirichletBoundary::GetBoundaryValue)
+ *               KEMCU_NEUMANN   (value = normal boundary flux, KNeumannBoundary)
+ *   geom[11*i]  triangle / rectangle: A, B, P0(xyz), N1(xyz), N2(xyz)
+ *               (KTriangle.hh:125-130, KRectangle.hh:132-137; P1 = P0 + A*N1, P2 = P0 + B*N2)
+ *               line segment: P0(xyz), P1(xyz), diameter, 0, 0, 0, 0 (KLineSegment.hh:74-76)
+ * Units are SI; 1/(4 pi eps0) and eps0 come from kemcu_config (KEMConstants, KEMConstants.cc:11-12).
+ */
+#ifndef KEMCU_H
+#define KEMCU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KEMCU_OK 0
+#define KEMCU_EINVAL (-1)       /* invalid argument or size */
+#define KEMCU_ECUDA (-2)        /* CUDA runtime / launch failure, or no usable device */
+#define KEMCU_ENONFINITE (-3)   /* a result contains NaN or Inf */
+#define KEMCU_ENOTCONVERGED (-4)/* solver stopped before reaching its tolerance */
+#define KEMCU_ETIMEOUT (-5)     /* step/time budget exhausted (tracker) */
+#define KEMCU_ENOMEM (-6)       /* device allocation failed or budget exceeded */
+#define KEMCU_ESTATE (-7)       /* call out of order (e.g. no geometry set) */
+
+enum kemcu_shape { KEMCU_TRIANGLE = 0, KEMCU_RECTANGLE = 1, KEMCU_LINE_SEGMENT = 2 };
+enum kemcu_boundary { KEMCU_DIRICHLET = 0, KEMCU_NEUMANN = 1 };
+/* arithmetic form of the element integrals */
+enum kemcu_precision {
+    KEMCU_FP64 = 0,  /* every node in FP64: the plain form */
+    KEMCU_MIXED = 1  /* FP64 near field (RWG / analytic), FP64 centroid term + FP32 node
+                        correction for the cubature bands, FP64 compensated accumulation */
+};
+/* which quantities a field evaluation produces (out4 = Ex, Ey, Ez, phi) */
+enum kemcu_what { KEMCU_FIELD_AND_POTENTIAL = 0, KEMCU_POTENTIAL = 1, KEMCU_FIELD = 2 };
+/* charge-density solve strategies */
+enum kemcu_solve_mode {
+    KEMCU_SOLVE_PLAIN = 0,     /* GMRES, FP64 matrix-free matvec (the reference algorithm) */
+    KEMCU_SOLVE_MIXED = 1,     /* iterative refinement: inner GMRES on the MIXED matrix-free
+                                  operator, FP64 matrix-free residual and correction */
+    KEMCU_SOLVE_ASSEMBLED = 2  /* operator assembled once in HBM (FP64, plus an FP32 copy);
+                                  inner GMRES on FP32, FP64 residual (refinement) */
+};
+
+typedef struct kemcu_ctx kemcu_ctx;
+
+typedef struct {
+    int device;                    /* CUDA device ordinal */
+    double one_over_four_pi_eps0;  /* KEMConstants::OneOverFourPiEps0 (KEMConstants.cc:12) */
+    double eps0;                   /* KEMConstants::Eps0 (KEMConstants.cc:11) */
+    size_t assembled_budget_bytes; /* device bytes an assembled operator may take; 0 = 70% of free */
+} kemcu_config;
+
+typedef struct {
+    int iterations;          /* total Krylov iterations (all refinement steps) */
+    int outer;               /* refinement steps (1 for KEMCU_SOLVE_PLAIN) */
+    int fp64_matvecs;        /* FP64 operator applications */
+    int low_matvecs;         /* reduced-precision operator applications */
+    double rel_residual;     /* max over RHS of |b - A x| / |b|, A applied in FP64 */
+    double rel_residual_estimate; /* GMRES implicit estimate |p_{j+1}| / |b| of the last cycle */
+    double seconds;          /* device time of the solve */
+} kemcu_solve_stats;
+
+/* per-iteration hook, the analogue of KIterativeSolver visitors (KIterativeSolver.hh:57-134):
+   return nonzero to stop the solve (KTimeTerminator-style) */
+typedef int (*kemcu_iteration_callback)(void* user, int iteration, double rel_residual_estimate);
+
+typedef struct {
+    double sphere_radius;    /* electrode hit when |x| <= sphere_radius (0 disables) */
+    double max_radius;       /* track leaves the volume when |x| >= max_radius (0 disables) */
+} kemcu_hit_model;
+
+enum kemcu_track_status { KEMCU_TRACK_ACTIVE = 0, KEMCU_TRACK_HIT = 1, KEMCU_TRACK_MAX_STEPS = 2,
+                          KEMCU_TRACK_LEFT = 3, KEMCU_TRACK_NONFINITE = 4 };
+
+typedef struct {
+    long long steps;         /* RK8 steps taken by all tracks */
+    long long field_evals;   /* field evaluations (13 per step) */
+    int hit, max_steps, left, nonfinite, active;
+    double seconds;
+} kemcu_track_stats;
+
+/* ---- context (KElectrostaticBoundaryIntegratorPolicy / use_opencl analogue,
+        KIntegratingElectrostaticFieldSolver.cc:44-69) ---- */
+void kemcu_default_config(kemcu_config* cfg);
+int kemcu_create(kemcu_ctx** ctx, const kemcu_config* cfg);
+int kemcu_destroy(kemcu_ctx* ctx);
+const char* kemcu_last_error(const kemcu_ctx* ctx);
+/* device milliseconds of the last call's kernels (0 if none) */
+double kemcu_last_kernel_ms(const kemcu_ctx* ctx);
+
+/* ---- geometry (KOpenCLSurfaceContainer analogue, KOpenCLSurfaceContainer.cc:10-204) ---- */
+int kemcu_set_geometry(kemcu_ctx* ctx, size_t n, const int32_t* shape, const int32_t* boundary,
+                       const double* geom11, const double* value);
+size_t kemcu_num_elements(const kemcu_ctx* ctx);
+/* charge densities (KElectrostaticBasis::GetSolution, KElectrostaticBasis.hh:22), n values */
+int kemcu_set_sigma(kemcu_ctx* ctx, const double* sigma);
+int kemcu_get_sigma(kemcu_ctx* ctx, double* sigma);
+/* right-hand side b_i = KBoundaryIntegralVector(i) (KBoundaryIntegralVector.hh:60-78) */
+int kemcu_rhs(kemcu_ctx* ctx, double* b);
+
+/* ---- direct summation (KIntegratingFieldSolver::{Potential,ElectricField,
+        ElectricFieldAndPotential}, KElectrostaticIntegratingFieldSolver.hh:261-339),
+        batched over n points: P is n x 3, out4 is n x 4 (Ex, Ey, Ez, phi) ---- */
+int kemcu_field(kemcu_ctx* ctx, const double* P, size_t n, double* out4, int precision, int what);
+/* same with device pointers, ordered on the context stream, synchronous on return */
+int kemcu_field_dev(kemcu_ctx* ctx, const double* dP, size_t n, double* dout4, int precision, int what);
+
+/* ---- boundary-integral matrix (KBoundaryIntegralMatrix, KBoundaryIntegralMatrix.hh:16-99) ---- */
+/* single entry A(i, j) = BoundaryIntegral(source j, target i) (KBoundaryIntegralMatrix.hh:31-55) */
+int kemcu_matrix_element(kemcu_ctx* ctx, size_t i, size_t j, double* a);
+/* y = A x for n_rhs right-hand sides (x, y: n_rhs x n), KMatrix::Multiply (KMatrix.hh:87-99);
+   assembled != 0 uses (and on first use builds) the assembled FP64 operator */
+int kemcu_matvec(kemcu_ctx* ctx, const double* x, double* y, int n_rhs, int precision, int assembled);
+
+/* ---- charge-density solve (KSimpleIterativeKrylovSolver<double, KGeneralizedMinimalResidual>::Solve,
+        KSimpleIterativeKrylovSolver.hh:139-194; KGeneralizedMinimalResidual.hh:178-337) ----
+   b: n_rhs x n right-hand sides, or NULL for the boundary values (single RHS);
+   x: n_rhs x n solution. For n_rhs == 1 the solution is also stored as the context's sigma. */
+int kemcu_gmres(kemcu_ctx* ctx, const double* b, double* x, int n_rhs, double rel_tol, int max_iter, int mode,
+                kemcu_solve_stats* stats);
+void kemcu_set_iteration_callback(kemcu_ctx* ctx, kemcu_iteration_callback cb, void* user);
+
+/* ---- batched exact-trajectory RK8 tracking in the electrostatic field (KSMathRK8::Integrate,
+        Kassiopeia/Math/Include/KSMathRK8.h:45-226; KSTrajTermPropagation::Differentiate,
+        KSTrajTermPropagation.cxx:25-35) ----
+   state: n x 8 (t, s, x, y, z, px, py, pz), updated in place; steps: n step counters
+   (in/out, tracks stop at max_steps); status: n kemcu_track_status values (in/out, only
+   KEMCU_TRACK_ACTIVE tracks advance). step_budget bounds the steps of this call per track
+   (<= 0: no extra bound). */
+int kemcu_track_rk8(kemcu_ctx* ctx, double* state, int32_t* steps, int32_t* status, size_t n, double dt,
+                    int max_steps, int step_budget, double charge, double mass, const kemcu_hit_model* hit,
+                    int precision, kemcu_track_stats* stats);
+
+/* ---- adjoint: vector-Jacobian product of the direct sum (no reference counterpart) ----
+   w: n x 4 weights on (Ex, Ey, Ez, phi) at points P (n x 3); L = sum_p w_p . out_p.
+   Outputs (either may be NULL):
+   dsigma[N]    = dL/dsigma_j
+   dvert[N x 9] = dL/d(P0, P1, P2) of element j, the three defining vertices
+                  (triangle: P0, P0 + A N1, P0 + B N2; rectangle: P0, P0 + A N1, P0 + B N2),
+                  within the quadrature band each (element, point) pair has; zeros for line
+                  segments. precision selects the arithmetic of the dsigma sums. */
+int kemcu_field_vjp(kemcu_ctx* ctx, const double* P, size_t n, const double* w, double* dsigma, double* dvert,
+                    int precision);
+
+/* ---- diagnostics (no device needed) ----
+   nodes and weights of the cubature rules the kernels use, on the canonical element
+   node = P0 + s (P1 - P0) + t (P2 - P0) (triangle) or P0 + s A N1 + t B N2 (rectangle):
+   which 0..2 = triangle 7/12/33-point (KElectrostaticCubatureTriangleIntegrator.cc:36-268),
+   3..5 = rectangle 7/12/33-point (KElectrostaticCubatureRectangleIntegrator.cc:46-290),
+   6 = 4-node and 7 = 16-node Gauss-Legendre half rules (x, w, 0) on [-1, 1]
+   (KElectrostaticQuadratureLineSegmentIntegrator.hh:47-80).
+   out: up to 33 x 3 (s, t, w); returns the node count or KEMCU_EINVAL. */
+int kemcu_rule_nodes(int which, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KEMCU_H */

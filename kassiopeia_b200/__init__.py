@@ -1,0 +1,203 @@
+"""kassiopeia_b200 -- B200-native (sm_100a) backend for KEMField's electrostatic BEM hot path.
+
+The product is ``libkemcu.so`` (C ABI: ``include/kemcu.h``) built from ``csrc/``. This module
+is a thin Python mirror of the reference-facing interface, used by the tests and the
+benchmark, with the reference's names:
+
+* :class:`CUDAElectrostaticContext` -- one GPU context holding a flattened surface container
+  (the KOpenCLSurfaceContainer analogue) and its charge densities;
+* :meth:`~CUDAElectrostaticContext.ElectricFieldAndPotential` / ``Potential`` /
+  ``ElectricField`` -- batched KIntegratingFieldSolver (direct summation);
+* :meth:`~CUDAElectrostaticContext.Multiply` -- KBoundaryIntegralMatrix::Multiply;
+* :meth:`~CUDAElectrostaticContext.Solve` -- the GMRES charge-density solve;
+* :meth:`~CUDAElectrostaticContext.TrackRK8` -- batched exact-trajectory RK8 steps;
+* :meth:`~CUDAElectrostaticContext.FieldVJP` -- adjoint of the direct sum.
+
+Every call goes to the GPU; a missing library or device raises instead of falling back.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from ._native import (FIELD, FIELD_AND_POTENTIAL, FP64, MIXED, POTENTIAL, SOLVE_ASSEMBLED, SOLVE_MIXED, SOLVE_PLAIN,
+                      KemcuError)
+
+__all__ = ["CUDAElectrostaticContext", "KemcuError", "FP64", "MIXED", "SOLVE_PLAIN", "SOLVE_MIXED",
+           "SOLVE_ASSEMBLED", "FIELD_AND_POTENTIAL", "POTENTIAL", "FIELD"]
+
+ONE_OVER_FOUR_PI_EPS0 = 1.0 / (4.0 * np.pi * 8.8541878128e-12)  # KEMConstants (KConst epoch 2021)
+EPS0 = 8.8541878128e-12
+
+
+def _d(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _i(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+class CUDAElectrostaticContext:
+    """One device context; not re-entrant (use one per thread)."""
+
+    def __init__(self, device: int = 0, assembled_budget_bytes: int = 0):
+        L = N.lib()
+        cfg = N.Config()
+        L.kemcu_default_config(C.byref(cfg))
+        cfg.device = device
+        cfg.one_over_four_pi_eps0 = ONE_OVER_FOUR_PI_EPS0
+        cfg.eps0 = EPS0
+        cfg.assembled_budget_bytes = assembled_budget_bytes
+        h = C.c_void_p()
+        rc = L.kemcu_create(C.byref(h), C.byref(cfg))
+        self._h = h
+        self._cb = None
+        if rc != N.OK:
+            msg = L.kemcu_last_error(h).decode() if h else "context creation failed"
+            L.kemcu_destroy(h)
+            self._h = None
+            raise KemcuError(rc, msg)
+        self.n = 0
+
+    # -- plumbing
+    def _check(self, rc):
+        if rc != N.OK:
+            raise KemcuError(rc, N.lib().kemcu_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().kemcu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def last_kernel_ms(self) -> float:
+        return N.lib().kemcu_last_kernel_ms(self._h)
+
+    # -- container
+    def SetGeometry(self, mesh):
+        self._shape = np.ascontiguousarray(mesh.shape, np.int32)
+        self._bnd = np.ascontiguousarray(mesh.boundary, np.int32)
+        self._geom = np.ascontiguousarray(mesh.geom, np.float64)
+        self._val = np.ascontiguousarray(mesh.value, np.float64)
+        self._check(N.lib().kemcu_set_geometry(self._h, mesh.n, _i(self._shape), _i(self._bnd), _d(self._geom),
+                                               _d(self._val)))
+        self.n = mesh.n
+
+    def SetSigma(self, sigma):
+        s = np.ascontiguousarray(sigma, np.float64)
+        assert s.shape == (self.n,)
+        self._check(N.lib().kemcu_set_sigma(self._h, _d(s)))
+
+    def GetSigma(self):
+        s = np.zeros(self.n)
+        self._check(N.lib().kemcu_get_sigma(self._h, _d(s)))
+        return s
+
+    def RHS(self):
+        b = np.zeros(self.n)
+        self._check(N.lib().kemcu_rhs(self._h, _d(b)))
+        return b
+
+    # -- direct summation
+    def ElectricFieldAndPotential(self, P, precision=FP64, what=FIELD_AND_POTENTIAL):
+        P = np.ascontiguousarray(P, np.float64).reshape(-1, 3)
+        out = np.zeros((P.shape[0], 4))
+        self._check(N.lib().kemcu_field(self._h, _d(P), P.shape[0], _d(out), precision, what))
+        return out
+
+    def Potential(self, P, precision=FP64):
+        return self.ElectricFieldAndPotential(P, precision, POTENTIAL)[:, 3]
+
+    def ElectricField(self, P, precision=FP64):
+        return self.ElectricFieldAndPotential(P, precision, FIELD)[:, :3]
+
+    def FieldDevice(self, d_points_ptr: int, n: int, d_out_ptr: int, precision=FP64, what=FIELD_AND_POTENTIAL):
+        """Device-pointer variant (e.g. torch tensors' data_ptr())."""
+        self._check(N.lib().kemcu_field_dev(self._h, C.c_void_p(d_points_ptr), n, C.c_void_p(d_out_ptr), precision,
+                                            what))
+
+    # -- matrix
+    def MatrixElement(self, i, j):
+        a = C.c_double()
+        self._check(N.lib().kemcu_matrix_element(self._h, i, j, C.byref(a)))
+        return a.value
+
+    def Multiply(self, x, precision=FP64, assembled=False):
+        x = np.ascontiguousarray(x, np.float64)
+        nr = 1 if x.ndim == 1 else x.shape[0]
+        y = np.zeros_like(x)
+        self._check(N.lib().kemcu_matvec(self._h, _d(x), _d(y), nr, precision, int(bool(assembled))))
+        return y
+
+    # -- solve
+    def SetIterationCallback(self, fn):
+        """fn(iteration, rel_residual_estimate) -> bool (True stops the solve)."""
+        if fn is None:
+            self._cb = None
+            N.lib().kemcu_set_iteration_callback(self._h, N.ITER_CB(), None)
+            return
+        self._cb = N.ITER_CB(lambda user, it, r: int(bool(fn(it, r))))
+        N.lib().kemcu_set_iteration_callback(self._h, self._cb, None)
+
+    def Solve(self, b=None, tol=1e-10, max_iter=500, mode=SOLVE_PLAIN, raise_on_failure=True):
+        """GMRES charge-density solve; returns (x, stats dict). b: None (boundary values),
+        [n] or [n_rhs, n]."""
+        if b is None:
+            x = np.zeros(self.n)
+            bp, nr = None, 1
+        else:
+            bb = np.ascontiguousarray(b, np.float64)
+            nr = 1 if bb.ndim == 1 else bb.shape[0]
+            x = np.zeros_like(bb)
+            bp = _d(bb)
+        st = N.SolveStats()
+        rc = N.lib().kemcu_gmres(self._h, bp, _d(x), nr, tol, max_iter, mode, C.byref(st))
+        stats = {k: getattr(st, k) for k, _ in N.SolveStats._fields_}
+        stats["status"] = rc
+        if rc != N.OK and raise_on_failure:
+            self._check(rc)
+        return x, stats
+
+    # -- tracking
+    def TrackRK8(self, state, dt, max_steps, steps=None, status=None, step_budget=0, charge=None, mass=None,
+                 sphere_radius=0.0, max_radius=0.0, precision=FP64):
+        from .geometry import ELECTRON_MASS, ELEMENTARY_CHARGE
+        st = np.ascontiguousarray(state, np.float64).copy()
+        n = st.shape[0]
+        steps = np.zeros(n, np.int32) if steps is None else np.ascontiguousarray(steps, np.int32).copy()
+        status = np.zeros(n, np.int32) if status is None else np.ascontiguousarray(status, np.int32).copy()
+        hit = N.HitModel(sphere_radius, max_radius)
+        ts = N.TrackStats()
+        q = -ELEMENTARY_CHARGE if charge is None else charge
+        m = ELECTRON_MASS if mass is None else mass
+        self._check(N.lib().kemcu_track_rk8(self._h, _d(st), _i(steps), _i(status), n, dt, max_steps, step_budget, q, m,
+                                            C.byref(hit), precision, C.byref(ts)))
+        return st, steps, status, {k: getattr(ts, k) for k, _ in N.TrackStats._fields_}
+
+    # -- adjoint
+    def FieldVJP(self, P, w, precision=FP64, want_sigma=True, want_vertices=True):
+        """Adjoint of the direct sum: (dL/dsigma [N], dL/dvertices [N, 9]) for L = sum_p w_p . out_p."""
+        P = np.ascontiguousarray(P, np.float64).reshape(-1, 3)
+        w = np.ascontiguousarray(w, np.float64).reshape(-1, 4)
+        ds = np.zeros(self.n) if want_sigma else None
+        dv = np.zeros((self.n, 9)) if want_vertices else None
+        null = C.cast(None, C.POINTER(C.c_double))
+        self._check(N.lib().kemcu_field_vjp(self._h, _d(P), P.shape[0], _d(w), _d(ds) if ds is not None else null,
+                                            _d(dv) if dv is not None else null, precision))
+        return ds, dv

@@ -1,0 +1,587 @@
+// Device-side element integrals for the electrostatic BEM hot path (sm_100a).
+//
+// One element-point interaction (EPI) = the field and/or potential of one charged element
+// with unit charge density at one point. The numeric policy of the reference picks the rule
+// per (element, point) from the distance ratio |P - centroid| / size
+// (KElectrostaticCubatureTriangleIntegrator.cc:453-522, ...RectangleIntegrator.cc:462-520,
+// ...QuadratureLineSegmentIntegrator.cc:193-240):
+//
+//   triangle  : RWG analytic <= 3.42 < 33-point <= 30.4 < 12-point <= 131.4 < 7-point
+//   rectangle : RWG analytic <= 4.6  < 33-point <= 44.6 < 12-point <= 196.2 < 7-point
+//   line      : analytic     <= 2    < 16-node Gauss <= 27.7 < 4-node Gauss
+//
+// The band test is evaluated with the same FP64 operations and rounding (no FMA
+// contraction) as the reference so that band boundaries agree bit for bit.
+//
+// Two arithmetic forms of the cubature bands are provided:
+//   * FP64   -- node by node in double precision with IEEE-accurate rsqrt (the plain form);
+//   * MIXED  -- 33-point band: FP64 nodes with an FP32 hardware rsqrt estimate refined by one
+//               FP64 Newton step (<= 4e-13 relative); 12- and 7-point bands: an FP64 centroid
+//               term plus an FP32 node correction written without cancellation (cub_mixed,
+//               ~1e-7 |o|/R < 2e-9 relative per element there).
+// RWG near-field integrals and the analytic line segment are always FP64.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+namespace kemcu
+{
+
+enum Shape : int
+{
+    kTriangle = 0,
+    kRectangle = 1,
+    kLineSegment = 2
+};
+
+// Element record in device memory, 32 doubles (256 B, one element per 2 x 128 B lines).
+// Offsets into the record:
+enum Rec : int
+{
+    rA = 0,        // side length A (line: length)
+    rB = 1,        // side length B (line: diameter)
+    rP0 = 2,       // P0 xyz (line: P0)
+    rN1 = 5,       // N1 xyz (line: P1)
+    rN2 = 8,       // N2 xyz
+    rEa = 11,      // A * N1 (line: P1 - P0)
+    rEb = 14,      // B * N2
+    rCen = 17,     // centroid (reference formula)
+    rN3 = 20,      // unit normal N1 x N2 / |N1 x N2| (line: unused)
+    rInvSize = 23, // 1 / size for the distance ratio
+    rPrefac = 24,  // area / (4 pi eps0)   (line: diameter / (4 eps0))
+    rType = 25,    // shape as double
+    rCen2 = 26,    // centroid xyz as KRectangle::Centroid()/KSolidAngle form it (rectangles; else = rCen)
+    rCut = 29,     // 3 squared distances (cut / invSize)^2 of the band boundaries, nearest first
+    rRecSize = 32
+};
+
+static_assert(rCut + 3 <= rRecSize, "element record layout overflows its 32 slots");
+
+struct Constants
+{
+    double one_over_four_pi_eps0;
+    double eps0;
+    double pi;
+};
+
+// Cubature rules in barycentric-like (s, t) form: node = P0 + s * (A N1) + t * (B N2),
+// weights normalised to 1 over the element. Offsets into c_rules (triples s, t, w):
+//   tri7 [0,7) tri12 [7,19) tri33 [19,52) rect7 [52,59) rect12 [59,71) rect33 [71,104)
+// Line Gauss-Legendre half rules (x, w) pairs: gl4 [0,2), gl16 [2,10).
+constexpr int kTri7 = 0, kTri12 = 7, kTri33 = 19, kRect7 = 52, kRect12 = 59, kRect33 = 71, kNumNodes = 104;
+__constant__ double c_rules[kNumNodes * 3];
+__constant__ float c_rules_f[kNumNodes * 4];  // s - s_c, t - t_c, w, 0 (centroid-relative)
+__constant__ double c_gl[10 * 2];
+__constant__ Constants c_k;
+__constant__ double c_wsum[kNumNodes];  // FP64 sum of the rule's weights, indexed by rule offset
+
+// ------------------------------------------------------------------------- helpers
+struct V3
+{
+    double x, y, z;
+};
+__device__ __forceinline__ V3 v3(double x, double y, double z)
+{
+    return V3{x, y, z};
+}
+__device__ __forceinline__ V3 operator-(V3 a, V3 b)
+{
+    return v3(a.x - b.x, a.y - b.y, a.z - b.z);
+}
+__device__ __forceinline__ V3 operator+(V3 a, V3 b)
+{
+    return v3(a.x + b.x, a.y + b.y, a.z + b.z);
+}
+__device__ __forceinline__ V3 operator*(double s, V3 a)
+{
+    return v3(s * a.x, s * a.y, s * a.z);
+}
+__device__ __forceinline__ double dot(V3 a, V3 b)
+{
+    return a.x * b.x + a.y * b.y + a.z * b.z;
+}
+__device__ __forceinline__ V3 cross(V3 a, V3 b)
+{
+    return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double norm(V3 a)
+{
+    return sqrt(dot(a, a));
+}
+__device__ __forceinline__ V3 ld3(const double* p)
+{
+    return v3(p[0], p[1], p[2]);
+}
+// sum of squares in the reference's left-to-right order without FMA contraction
+__device__ __forceinline__ double sumsq_rn(double a, double b, double c)
+{
+    return __dadd_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)), __dmul_rn(c, c));
+}
+
+struct Out4
+{
+    double ex, ey, ez, phi;
+};
+
+// ------------------------------------------------------------------------- band test
+// 0 = analytic (RWG / analytic line), 1 = 33-point / 16-node, 2 = 12-point / 4-node, 3 = 7-point
+// The squared centre distance is compared with the squared cut distances stored in the record;
+// only when it lies within a relative 1e-12 of a cut is the reference's exact expression
+// ratio = sqrt(r2) * (1 / size) evaluated, so the decision is the reference's bit for bit.
+__device__ __forceinline__ int band_exact(const double* e, double r2)
+{
+    const double ratio = __dmul_rn(__dsqrt_rn(r2), e[rInvSize]);
+    const int type = (int) e[rType];
+    if (type == kTriangle)
+        return ratio > 131.4 ? 3 : ratio > 30.4 ? 2 : ratio > 3.42 ? 1 : 0;
+    if (type == kRectangle)
+        return ratio > 196.2 ? 3 : ratio > 44.6 ? 2 : ratio > 4.6 ? 1 : 0;
+    return ratio > 27.7 ? 2 : ratio > 2. ? 1 : 0;
+}
+
+__device__ __forceinline__ int band_of(const double* e, V3 P)
+{
+    const double dx = __dadd_rn(e[rCen], -P.x);
+    const double dy = __dadd_rn(e[rCen + 1], -P.y);
+    const double dz = __dadd_rn(e[rCen + 2], -P.z);
+    const double r2 = sumsq_rn(dx, dy, dz);
+    int band = 0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const double c = e[rCut + k];
+        if (r2 > c * (1. + 1e-12))
+            band = k + 1;
+        else if (r2 >= c * (1. - 1e-12))
+            return band_exact(e, r2);
+        else
+            break;
+    }
+    return band;
+}
+
+__device__ __forceinline__ int rule_offset(int type, int band, int& n)
+{
+    if (type == kTriangle) {
+        n = band == 1 ? 33 : band == 2 ? 12 : 7;
+        return band == 1 ? kTri33 : band == 2 ? kTri12 : kTri7;
+    }
+    n = band == 1 ? 33 : band == 2 ? 12 : 7;
+    return band == 1 ? kRect33 : band == 2 ? kRect12 : kRect7;
+}
+
+// ------------------------------------------------------------------------- FP64 cubature
+// Sum over nodes of w (P-Q)/|P-Q|^3 and w/|P-Q| times area/(4 pi eps0)
+// (Potential_TriNP / ElectricField_TriNP, KElectrostaticCubatureTriangleIntegrator.cc:271-450;
+// the rectangle versions are identical in form).
+// FP64 reciprocal square root from the FP32 hardware estimate plus one Newton step in FP64:
+// relative error <= ~4e-13 (the estimate's 2^-22 squared), used by the MIXED form only.
+__device__ __forceinline__ double rsqrt_newton(double x)
+{
+    const double y = (double) rsqrtf((float) x);
+    const double h = fma(-0.5 * x * y, y, 0.5);
+    return fma(y, h, y);
+}
+
+template<bool POT, bool FIELD, bool FAST = false>
+__device__ __forceinline__ Out4 cub64(const double* e, V3 P, int off, int n)
+{
+    const V3 d0 = P - ld3(e + rP0);
+    const V3 a = ld3(e + rEa), b = ld3(e + rEb);
+    double sx = 0., sy = 0., sz = 0., sp = 0.;
+#pragma unroll 4
+    for (int k = 0; k < n; k++) {
+        const double s = c_rules[3 * (off + k)], t = c_rules[3 * (off + k) + 1], w = c_rules[3 * (off + k) + 2];
+        const double qx = d0.x - s * a.x - t * b.x;
+        const double qy = d0.y - s * a.y - t * b.y;
+        const double qz = d0.z - s * a.z - t * b.z;
+        const double q2 = qx * qx + qy * qy + qz * qz;
+        const double ir = FAST ? rsqrt_newton(q2) : rsqrt(q2);
+        const double wi = w * ir;
+        if (POT)
+            sp += wi;
+        if (FIELD) {
+            const double wi3 = wi * ir * ir;
+            sx += wi3 * qx;
+            sy += wi3 * qy;
+            sz += wi3 * qz;
+        }
+    }
+    const double pf = e[rPrefac];
+    return Out4{pf * sx, pf * sy, pf * sz, pf * sp};
+}
+
+// ------------------------------------------------------------------------- mixed cubature
+// Split of each node term around the centroid c: with d = P - c (FP64), R = |d| and the node
+// offset o = Q - c, |P - Q|^2 = R^2 (1 - eps), eps = (2 d.o - o.o) / R^2, so
+//   1/|P-Q|   = (1/R)   (1 + f),  f = (1-eps)^(-1/2) - 1 = eps y / (1 + (1-eps) y)
+//   1/|P-Q|^3 = (1/R^3) (1 + g),  g = (1-eps)^(-3/2) - 1 = f (y^2 + y + 1)
+// with y = rsqrt(1 - eps). The rule weights sum to W, so the element sums are
+//   phi = pf/R (W + sum w f),  E = pf/R^3 (d (W + sum w g) - sum w (1+g) o).
+// The large terms W/R and W d/R^3 are FP64; f and g are formed in FP32 without
+// cancellation (absolute error ~1e-7 |f|), so the per-element relative error is about
+// 1e-7 |o|/R: ~2e-8 at the inner edge of the 33-point band, < 3e-9 beyond the 12-point cut.
+template<bool POT, bool FIELD>
+__device__ __forceinline__ Out4 cub_mixed(const double* e, V3 P, int off, int n)
+{
+    const V3 d = P - ld3(e + rCen);
+    const double R2 = dot(d, d);
+    const double iR = rsqrt(R2);
+    const double iR2 = iR * iR;
+    // scaled direction u = 2 d / R^2 and v = 1 / R^2 in FP32
+    const float ux = (float) (2. * d.x * iR2), uy = (float) (2. * d.y * iR2), uz = (float) (2. * d.z * iR2);
+    const float v = (float) iR2;
+    const float ax = (float) e[rEa], ay = (float) e[rEa + 1], az = (float) e[rEa + 2];
+    const float bx = (float) e[rEb], by = (float) e[rEb + 1], bz = (float) e[rEb + 2];
+    float sf = 0.f, sg = 0.f, sox = 0.f, soy = 0.f, soz = 0.f;
+#pragma unroll 4
+    for (int k = 0; k < n; k++) {
+        const float4 r = *reinterpret_cast<const float4*>(&c_rules_f[4 * (off + k)]);
+        const float ox = r.x * ax + r.y * bx, oy = r.x * ay + r.y * by, oz = r.x * az + r.y * bz;
+        const float oo = ox * ox + oy * oy + oz * oz;
+        const float eps = ux * ox + uy * oy + uz * oz - v * oo;
+        const float om = 1.f - eps;
+        const float y0 = rsqrtf(om);
+        const float y = fmaf(y0, fmaf(-0.5f * om * y0, y0, 0.5f), y0);
+        const float f = eps * y * __fdividef(1.f, 1.f + om * y);
+        if (POT)
+            sf += r.z * f;
+        if (FIELD) {
+            const float g = f * (y * y + y + 1.f);
+            sg += r.z * g;
+            const float wy3 = r.z * (1.f + g);
+            sox += wy3 * ox;
+            soy += wy3 * oy;
+            soz += wy3 * oz;
+        }
+    }
+    const double pf = e[rPrefac];
+    Out4 o{0., 0., 0., 0.};
+    const double Wd = c_wsum[off];
+    if (POT)
+        o.phi = pf * iR * (Wd + (double) sf);
+    if (FIELD) {
+        const double iR3 = iR * iR2;
+        const double s = Wd + (double) sg;
+        o.ex = pf * iR3 * (d.x * s - (double) sox);
+        o.ey = pf * iR3 * (d.y * s - (double) soy);
+        o.ez = pf * iR3 * (d.z * s - (double) soz);
+    }
+    return o;
+}
+
+// ------------------------------------------------------------------------- RWG (analytic)
+// Analytic potential and field of a uniformly charged planar polygon (triangle NV = 3,
+// rectangle NV = 4): phi = (-h Omega - sum_i t_i L_i) / (4 pi eps0),
+// E = (N3 Omega + sum_i m_i L_i) / (4 pi eps0), with Omega the signed solid angle, m_i the
+// outward in-plane edge normals, t_i = m_i.(P - edge midpoint) and L_i the log line
+// integral of each edge (KElectrostaticRWGTriangleIntegrator.cc:20-208 IqL,
+// :607-814 Potential, :817-1011 ElectricField; KElectrostaticRWGRectangleIntegrator.cc:20-240,
+// :713-1174). Points on an edge line use the second-order log-argument expansion; points
+// on two edge lines (a vertex) are averaged over P +- 1e-7 N3.
+template<int NV> struct Polygon
+{
+    V3 v[NV];    // vertices in positive rotation order
+    V3 L[NV];    // edge vectors used for the on-line test
+    double len[NV];
+    V3 u[NV];    // edge unit vectors
+    V3 mid[NV];  // edge midpoints
+    V3 m[NV];    // outward edge normals u x N3
+    V3 n3;       // unit normal
+    V3 n3raw;    // N1 x N2 (rectangle solid-angle plane test)
+    V3 cen;
+};
+
+__device__ __forceinline__ void make_polygon(const double* g, Polygon<3>& q)
+{
+    const double A = g[rA], B = g[rB];
+    const V3 P0 = ld3(g + rP0), N1 = ld3(g + rN1), N2 = ld3(g + rN2);
+    q.v[0] = P0;
+    q.v[1] = v3(__dadd_rn(P0.x, __dmul_rn(A, N1.x)), __dadd_rn(P0.y, __dmul_rn(A, N1.y)),
+                __dadd_rn(P0.z, __dmul_rn(A, N1.z)));
+    q.v[2] = v3(__dadd_rn(P0.x, __dmul_rn(B, N2.x)), __dadd_rn(P0.y, __dmul_rn(B, N2.y)),
+                __dadd_rn(P0.z, __dmul_rn(B, N2.z)));
+    V3 n = cross(N1, N2);
+    q.n3raw = n;
+    q.n3 = (1. / norm(n)) * n;
+    q.cen = ld3(g + rCen);
+    const V3 e12 = q.v[2] - q.v[1];
+    const double l12 = norm(e12);
+    q.L[0] = A * N1;
+    q.L[1] = e12;
+    q.L[2] = (-B) * N2;
+    q.len[0] = A;
+    q.len[1] = l12;
+    q.len[2] = B;
+    q.u[0] = N1;
+    q.u[1] = (1. / l12) * e12;
+    q.u[2] = v3(-N2.x, -N2.y, -N2.z);
+    for (int i = 0; i < 3; i++) {
+        q.mid[i] = (0.5 * q.len[i]) * q.u[i] + q.v[i];
+        q.m[i] = cross(q.u[i], q.n3);
+    }
+}
+
+__device__ __forceinline__ void make_polygon(const double* g, Polygon<4>& q)
+{
+    const double A = g[rA], B = g[rB];
+    const V3 P0 = ld3(g + rP0), N1 = ld3(g + rN1), N2 = ld3(g + rN2);
+    const V3 aN1 = v3(__dmul_rn(A, N1.x), __dmul_rn(A, N1.y), __dmul_rn(A, N1.z));
+    const V3 bN2 = v3(__dmul_rn(B, N2.x), __dmul_rn(B, N2.y), __dmul_rn(B, N2.z));
+    q.v[0] = P0;
+    q.v[1] = v3(__dadd_rn(P0.x, aN1.x), __dadd_rn(P0.y, aN1.y), __dadd_rn(P0.z, aN1.z));
+    q.v[2] = v3(__dadd_rn(q.v[1].x, bN2.x), __dadd_rn(q.v[1].y, bN2.y), __dadd_rn(q.v[1].z, bN2.z));
+    q.v[3] = v3(__dadd_rn(P0.x, bN2.x), __dadd_rn(P0.y, bN2.y), __dadd_rn(P0.z, bN2.z));
+    V3 n = cross(N1, N2);
+    q.n3raw = n;
+    q.n3 = (1. / norm(n)) * n;
+    q.cen = ld3(g + rCen2);
+    q.L[0] = aN1;
+    q.L[1] = bN2;
+    q.L[2] = v3(-aN1.x, -aN1.y, -aN1.z);
+    q.L[3] = v3(-bN2.x, -bN2.y, -bN2.z);
+    q.len[0] = A;
+    q.len[1] = B;
+    q.len[2] = A;
+    q.len[3] = B;
+    q.u[0] = N1;
+    q.u[1] = N2;
+    q.u[2] = v3(-N1.x, -N1.y, -N1.z);
+    q.u[3] = v3(-N2.x, -N2.y, -N2.z);
+    for (int i = 0; i < 4; i++) {
+        q.mid[i] = (0.5 * q.len[i]) * q.u[i] + q.v[i];
+        q.m[i] = cross(q.u[i], q.n3);
+    }
+}
+
+// signed solid angle (Van Oosterom-Strackee), KEMField/Source/Surfaces/include/KSolidAngle.hh:58-…
+__device__ __forceinline__ double tri_solid_angle(V3 a, V3 b, V3 c, V3 P)
+{
+    const V3 ua = (1. / norm(a - P)) * (a - P);
+    const V3 ub = (1. / norm(b - P)) * (b - P);
+    const V3 uc = (1. / norm(c - P)) * (c - P);
+    const double x = 1. + dot(ua, ub) + dot(ua, uc) + dot(ub, uc);
+    const double y = fabs(dot(ua, cross(ub, uc)));
+    return fabs(2. * atan2(y, x));
+}
+
+template<int NV> __device__ double solid_angle(const Polygon<NV>& q, V3 P)
+{
+    if (NV == 3) {
+        const double h = dot(q.n3, P - q.cen);
+        double res;
+        if (norm(P - q.cen) <= 1e-12)
+            res = 2. * c_k.pi;
+        else
+            res = tri_solid_angle(q.v[0], q.v[1], q.v[2], P);
+        return h < 0. ? -res : res;
+    }
+    else {
+        const double h = dot(q.n3raw, P - q.cen);
+        double res;
+        if (fabs(h) < 1e-12) {
+            const V3 dP = q.v[0] - P;
+            const double l1 = -dot(dP, q.L[0]) / (q.len[0] * q.len[0]);
+            const double l2 = -dot(dP, q.L[1]) / (q.len[1] * q.len[1]);
+            res = (l1 > 0. && l1 < 1. && l2 > 0. && l2 < 1.) ? 2. * c_k.pi : 0.;
+        }
+        else
+            res = tri_solid_angle(q.v[0], q.v[1], q.v[2], P) + tri_solid_angle(q.v[2], q.v[3], q.v[0], P);
+        return h < 0. ? -res : res;
+    }
+}
+
+// line integrals of the edges; counter/line/dist describe an on-line field point
+template<int NV, bool POT, bool FIELD>
+__device__ void edge_logs(const Polygon<NV>& q, V3 P, int counter, int line, double dist, double& il, V3& iv)
+{
+    il = 0.;
+    iv = v3(0., 0., 0.);
+    double rm[NV];
+    V3 dv[NV];
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+        dv[i] = q.v[i] - P;
+        rm[i] = norm(dv[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+        const int j = (i + 1) % NV;
+        const double rM = rm[i], rP = rm[j];
+        const double sM = dot(dv[i], q.u[i]), sP = dot(dv[j], q.u[i]);
+        double term = 0.;
+        bool have = false;
+        if (counter == 1 && line == i) {
+            if (fabs(dist / sM) < 1e-6) {
+                double quot = fabs(dist / sM);
+                if (quot < 1e-14)
+                    quot = 1e-14;
+                const double taylor = 0.5 * fabs(sM) * quot * quot;
+                term = log(rP + sP) - log(taylor);
+                have = true;
+            }
+        }
+        if (line != i) {
+            double nom, den;
+            if ((rM + sM) > (rP - sP)) {
+                nom = rP + sP;
+                den = rM + sM;
+            }
+            else {
+                nom = rM - sM;
+                den = rP - sP;
+            }
+            term += log(nom) - log(den);
+            have = true;
+        }
+        if (have) {
+            if (POT)
+                il += dot(q.m[i], P - q.mid[i]) * term;
+            if (FIELD)
+                iv = iv + term * q.m[i];
+        }
+    }
+}
+
+template<int NV, bool POT, bool FIELD> __device__ Out4 rwg_at(const Polygon<NV>& q, V3 P, int counter, int line, double dist)
+{
+    double il;
+    V3 iv;
+    edge_logs<NV, POT, FIELD>(q, P, counter, line, dist, il, iv);
+    const double om = solid_angle<NV>(q, P);
+    Out4 o{0., 0., 0., 0.};
+    if (POT)
+        o.phi = -dot(q.n3, P - q.cen) * om - il;
+    if (FIELD) {
+        o.ex = q.n3.x * om + iv.x;
+        o.ey = q.n3.y * om + iv.y;
+        o.ez = q.n3.z * om + iv.z;
+    }
+    return o;
+}
+
+template<int NV, bool POT, bool FIELD> __device__ __noinline__ Out4 rwg64(const double* e, V3 P)
+{
+    Polygon<NV> q;
+    make_polygon(e, q);
+    int counter = 0, line = 99;
+    double dmin = 0.;
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+        const V3 dv = q.v[i] - P;
+        const double inv = 1. / q.len[i];
+        const double dl = norm(cross(q.L[i], dv)) * inv;
+        const double lam = -dot(dv, q.L[i]) * (inv * inv);
+        if (dl < 1e-14 && lam >= -1e-15 && lam <= 1. + 1e-15) {
+            dmin = dl;
+            counter++;
+            line = i;
+        }
+    }
+    const double k = c_k.one_over_four_pi_eps0;
+    Out4 o;
+    if (counter == 2) {
+        const V3 up = P + 1e-7 * q.n3, dn = P - 1e-7 * q.n3;
+        const Out4 a = rwg_at<NV, POT, FIELD>(q, up, 9, 9, 9.), b = rwg_at<NV, POT, FIELD>(q, dn, 9, 9, 9.);
+        o = Out4{0.5 * (a.ex + b.ex), 0.5 * (a.ey + b.ey), 0.5 * (a.ez + b.ez), 0.5 * (a.phi + b.phi)};
+    }
+    else
+        o = rwg_at<NV, POT, FIELD>(q, P, counter, line, dmin);
+    return Out4{k * o.ex, k * o.ey, k * o.ez, k * o.phi};
+}
+
+// ------------------------------------------------------------------------- line segments
+// Gauss-Legendre over the segment (KElectrostaticQuadratureLineSegmentIntegrator.cc:8-185)
+template<bool POT, bool FIELD> __device__ __forceinline__ Out4 line_gauss(const double* e, V3 P, int off, int half)
+{
+    const V3 p0 = ld3(e + rP0), p1 = ld3(e + rN1);
+    const double len = e[rA];
+    const V3 c = 0.5 * (p0 + p1);
+    const V3 u = (1. / len) * (p1 - p0);
+    const double hl = 0.5 * len;
+    double sp = 0.;
+    V3 sv = v3(0., 0., 0.);
+    for (int i = 0; i < half; i++) {
+        const double wf = c_gl[2 * (off + i) + 1] * hl, x = c_gl[2 * (off + i)] * hl;
+        const V3 dp = P - (c + x * u), dn = P - (c - x * u);
+        const double ip = rsqrt(dot(dp, dp)), in = rsqrt(dot(dn, dn));
+        if (POT)
+            sp += wf * (ip + in);
+        if (FIELD)
+            sv = sv + wf * ((ip * ip * ip) * dp + (in * in * in) * dn);
+    }
+    const double pf = 0.25 * e[rB] / c_k.eps0;
+    return Out4{pf * sv.x, pf * sv.y, pf * sv.z, pf * sp};
+}
+
+// analytic line segment (KElectrostaticAnalyticLineSegmentIntegrator.cc:15-82)
+template<bool POT, bool FIELD> __device__ __noinline__ Out4 line_analytic(const double* e, V3 P)
+{
+    const V3 p0 = ld3(e + rP0), p1 = ld3(e + rN1);
+    const double diam = e[rB];
+    const double L = norm(p1 - p0);
+    Out4 o{0., 0., 0., 0.};
+    const double Da0 = norm(p0 - P), Db0 = norm(p1 - P);
+    // shared "inside the wire" classification
+    bool inside = false;
+    V3 pp = v3(0., 0., 0.);
+    if (!((Da0 + Db0) > (L + diam))) {
+        const V3 u = (1. / L) * (p1 - p0);
+        const double p = dot(P - p0, u);
+        if (!(p < -diam * .5 || p > L + diam * .5)) {
+            pp = p0 + p * u;
+            if (!(norm(P - pp) >= diam * .5))
+                inside = true;
+        }
+    }
+    if (POT) {
+        double Da = Da0, Db = Db0;
+        if (inside) {
+            Da = sqrt(dot(p0 - pp, p0 - pp) + diam * diam * .25);
+            Db = sqrt(dot(p1 - pp, p1 - pp) + diam * diam * .25);
+        }
+        o.phi = diam / (4. * c_k.eps0) * log((Da + Db + L) / (Da + Db - L));
+    }
+    if (FIELD) {
+        double Da = Da0, Db = Db0;
+        if (inside) {
+            Da = norm(p0 - pp);
+            Db = norm(p1 - pp);
+        }
+        double den = (Da * (Da + Db + L) * (Da + Db - L) * Db) * 4. * c_k.eps0;
+        den = -1. / den;
+        const double s = 2. * L * diam * den;
+        o.ex = s * (p1.x * Da - P.x * (Da + Db) + p0.x * Db);
+        o.ey = s * (p1.y * Da - P.y * (Da + Db) + p0.y * Db);
+        o.ez = s * (p1.z * Da - P.z * (Da + Db) + p0.z * Db);
+    }
+    return o;
+}
+
+// ------------------------------------------------------------------------- one EPI
+// MIXED selects the FP32-split form for the cubature bands; everything else is FP64.
+template<bool MIXED, bool POT, bool FIELD> __device__ __forceinline__ Out4 epi(const double* e, V3 P)
+{
+    const int band = band_of(e, P);
+    const int type = (int) e[rType];
+    if (type == kLineSegment) {
+        if (band == 0)
+            return line_analytic<POT, FIELD>(e, P);
+        return band == 1 ? line_gauss<POT, FIELD>(e, P, 2, 8) : line_gauss<POT, FIELD>(e, P, 0, 2);
+    }
+    if (band == 0)
+        return type == kTriangle ? rwg64<3, POT, FIELD>(e, P) : rwg64<4, POT, FIELD>(e, P);
+    int n;
+    const int off = rule_offset(type, band, n);
+    if (MIXED) {
+        // 33-point band: FP64 nodes with the Newton reciprocal square root; 12- and 7-point
+        // bands (|o|/R < 0.02): FP64 centroid term + FP32 node correction
+        if (band == 1)
+            return cub64<POT, FIELD, true>(e, P, off, n);
+        return cub_mixed<POT, FIELD>(e, P, off, n);
+    }
+    return cub64<POT, FIELD>(e, P, off, n);
+}
+
+}  // namespace kemcu

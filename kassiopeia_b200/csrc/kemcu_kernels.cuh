@@ -1,0 +1,371 @@
+// Direct-summation kernels: field evaluation at many points (K1), the matrix-free
+// boundary-integral matvec (K2), operator assembly and the dense (assembled) matvec.
+//
+// Layout: one thread owns one evaluation point (a field point, or a target centroid for the
+// matvec); a CTA of kThreads points streams a contiguous slice of the element records through
+// shared memory in tiles of kTile elements (256 B records, copied with 16 B vector loads), and
+// every thread sums the tile's contributions with Kahan compensation, as the reference's
+// KIntegratingFieldSolver does (KElectrostaticIntegratingFieldSolver.hh:261-339). When there
+// are too few points to fill the GPU the element list is split over gridDim.y; each split
+// writes a partial sum to scratch and reduce_splits adds the splits in a fixed order, so the
+// result does not depend on scheduling.
+#pragma once
+
+#include "kemcu_device.cuh"
+
+namespace kemcu
+{
+
+constexpr int kThreads = 128;
+constexpr int kTile = 32;
+
+struct Kahan
+{
+    double s = 0., c = 0.;
+    __device__ __forceinline__ void add(double v)
+    {
+        const double y = v - c;
+        const double t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+};
+
+// cooperative copy of `count` element records (256 B each) into shared memory
+__device__ __forceinline__ void load_tile(double* sm, const double* __restrict__ rec, int first, int count)
+{
+    const double2* src = reinterpret_cast<const double2*>(rec + (size_t) first * rRecSize);
+    double2* dst = reinterpret_cast<double2*>(sm);
+    const int n2 = count * (rRecSize / 2);
+    for (int i = threadIdx.x; i < n2; i += blockDim.x)
+        dst[i] = __ldg(src + i);
+}
+
+// K1: field and/or potential at points. out layout per point: (Ex, Ey, Ez, phi).
+// nsplit == gridDim.y; partial != nullptr when nsplit > 1 (then out is untouched).
+template<bool MIXED, bool POT, bool FIELD>
+__global__ void __launch_bounds__(kThreads) field_kernel(const double* __restrict__ rec, const double* __restrict__ sigma,
+                                                         int n_elem, const double* __restrict__ pts, int n_pts,
+                                                         double* __restrict__ out, double* __restrict__ partial)
+{
+    __shared__ __align__(16) double s_rec[kTile * rRecSize];
+    __shared__ double s_sig[kTile];
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = p < n_pts;
+    V3 P = v3(0., 0., 0.);
+    if (active)
+        P = v3(pts[3 * p], pts[3 * p + 1], pts[3 * p + 2]);
+    const int per = (n_elem + gridDim.y - 1) / gridDim.y;
+    const int e0 = blockIdx.y * per;
+    const int e1 = min(n_elem, e0 + per);
+    Kahan kx, ky, kz, kp;
+    for (int t0 = e0; t0 < e1; t0 += kTile) {
+        const int cnt = min(kTile, e1 - t0);
+        __syncthreads();
+        load_tile(s_rec, rec, t0, cnt);
+        if (threadIdx.x < cnt)
+            s_sig[threadIdx.x] = sigma[t0 + threadIdx.x];
+        __syncthreads();
+        if (active) {
+            for (int j = 0; j < cnt; j++) {
+                const double* e = s_rec + j * rRecSize;
+                const Out4 r = epi<MIXED, POT, FIELD>(e, P);
+                const double sg = s_sig[j];
+                if (FIELD) {
+                    kx.add(r.ex * sg);
+                    ky.add(r.ey * sg);
+                    kz.add(r.ez * sg);
+                }
+                if (POT)
+                    kp.add(r.phi * sg);
+            }
+        }
+    }
+    if (!active)
+        return;
+    double* o = partial ? partial + ((size_t) blockIdx.y * n_pts + p) * 4 : out + (size_t) p * 4;
+    o[0] = kx.s;
+    o[1] = ky.s;
+    o[2] = kz.s;
+    o[3] = kp.s;
+}
+
+// fixed-order sum of gridDim.y partial results: out[i] = sum_s partial[s][i]
+__global__ void reduce_splits(const double* __restrict__ partial, int nsplit, size_t n, double* __restrict__ out)
+{
+    const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    Kahan k;
+    for (int s = 0; s < nsplit; s++)
+        k.add(partial[(size_t) s * n + i]);
+    out[i] = k.s;
+}
+
+// Target description for matrix rows: centroid, boundary kind, outward normal and the
+// Neumann self-term value (KElectrostaticBoundaryIntegrator.hh:260-280)
+struct TargetRec
+{
+    double cen[3];
+    double normal[3];
+    double diag;      // (1 + eps_r) / (1 - eps_r) / (2 eps0) for Neumann rows
+    double neumann;   // 0 Dirichlet, 1 Neumann
+};
+
+// one matrix entry A(i, j) with source record e and target t
+template<bool MIXED> __device__ __forceinline__ double entry(const double* e, const TargetRec& t, V3 C)
+{
+    if (t.neumann == 0.) {
+        return epi<MIXED, true, false>(e, C).phi;
+    }
+    const V3 cs = ld3(e + rCen2);
+    const double dist = norm(cs - C);
+    if (dist >= 1e-12) {
+        const Out4 r = epi<MIXED, false, true>(e, C);
+        return r.ex * t.normal[0] + r.ey * t.normal[1] + r.ez * t.normal[2];
+    }
+    return t.diag;
+}
+
+// K2: y[r][i] = sum_j A(i, j) x[r][j] for r < nrhs (nrhs <= kMaxRhs), entries recomputed
+// on the fly (KMatrix::Multiply over KBoundaryIntegralMatrix::operator(),
+// KMatrix.hh:92-99, KBoundaryIntegralMatrix.hh:31-55).
+constexpr int kMaxRhs = 8;
+template<bool MIXED>
+__global__ void __launch_bounds__(kThreads) matvec_kernel(const double* __restrict__ rec, const TargetRec* __restrict__ tgt,
+                                                          int n, const double* __restrict__ x, int nrhs,
+                                                          double* __restrict__ y, double* __restrict__ partial)
+{
+    __shared__ __align__(16) double s_rec[kTile * rRecSize];
+    __shared__ double s_x[kMaxRhs][kTile];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = i < n;
+    TargetRec t{};
+    V3 C = v3(0., 0., 0.);
+    if (active) {
+        t = tgt[i];
+        C = v3(t.cen[0], t.cen[1], t.cen[2]);
+    }
+    const int per = (n + gridDim.y - 1) / gridDim.y;
+    const int e0 = blockIdx.y * per;
+    const int e1 = min(n, e0 + per);
+    Kahan acc[kMaxRhs];
+    for (int t0 = e0; t0 < e1; t0 += kTile) {
+        const int cnt = min(kTile, e1 - t0);
+        __syncthreads();
+        load_tile(s_rec, rec, t0, cnt);
+        for (int q = threadIdx.x; q < cnt * nrhs; q += blockDim.x)
+            s_x[q / cnt][q % cnt] = x[(size_t) (q / cnt) * n + t0 + q % cnt];
+        __syncthreads();
+        if (active) {
+            for (int j = 0; j < cnt; j++) {
+                const double a = entry<MIXED>(s_rec + j * rRecSize, t, C);
+#pragma unroll
+                for (int r = 0; r < kMaxRhs; r++)
+                    if (r < nrhs)
+                        acc[r].add(a * s_x[r][j]);
+            }
+        }
+    }
+    if (!active)
+        return;
+    for (int r = 0; r < nrhs; r++) {
+        if (partial)
+            partial[((size_t) blockIdx.y * nrhs + r) * n + i] = acc[r].s;
+        else
+            y[(size_t) r * n + i] = acc[r].s;
+    }
+}
+
+// operator assembly: column-major dense A (A[j * n + i] = A(i, j)) for columns [j0, j1),
+// written in FP64 and, when a32 != nullptr, also rounded to FP32
+template<bool MIXED>
+__global__ void __launch_bounds__(kThreads) assemble_kernel(const double* __restrict__ rec, const TargetRec* __restrict__ tgt,
+                                                            int n, int j0, int j1, double* __restrict__ a64,
+                                                            float* __restrict__ a32)
+{
+    __shared__ __align__(16) double s_rec[kTile * rRecSize];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = i < n;
+    TargetRec t{};
+    V3 C = v3(0., 0., 0.);
+    if (active) {
+        t = tgt[i];
+        C = v3(t.cen[0], t.cen[1], t.cen[2]);
+    }
+    const int span = j1 - j0;
+    const int per = (span + gridDim.y - 1) / gridDim.y;
+    const int e0 = j0 + blockIdx.y * per;
+    const int e1 = min(j1, e0 + per);
+    for (int t0 = e0; t0 < e1; t0 += kTile) {
+        const int cnt = min(kTile, e1 - t0);
+        __syncthreads();
+        load_tile(s_rec, rec, t0, cnt);
+        __syncthreads();
+        if (active) {
+            for (int j = 0; j < cnt; j++) {
+                const double a = entry<MIXED>(s_rec + j * rRecSize, t, C);
+                const size_t idx = (size_t) (t0 + j - j0) * n + i;
+                if (a64)
+                    a64[idx] = a;
+                if (a32)
+                    a32[idx] = (float) a;
+            }
+        }
+    }
+}
+
+// dense matvec on the assembled column-major operator: y[r][i] = sum_j A[j*n+i] x[r][j].
+// Threads own rows i (coalesced column reads); the column range is split over gridDim.y.
+template<typename T>
+__global__ void __launch_bounds__(256) dense_matvec_kernel(const T* __restrict__ A, int n, const double* __restrict__ x,
+                                                           int nrhs, double* __restrict__ y, double* __restrict__ partial)
+{
+    __shared__ double s_x[kMaxRhs][256];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int per = (n + gridDim.y - 1) / gridDim.y;
+    const int e0 = blockIdx.y * per;
+    const int e1 = min(n, e0 + per);
+    double acc[kMaxRhs];
+#pragma unroll
+    for (int r = 0; r < kMaxRhs; r++)
+        acc[r] = 0.;
+    for (int t0 = e0; t0 < e1; t0 += 256) {
+        const int cnt = min(256, e1 - t0);
+        __syncthreads();
+        for (int q = threadIdx.x; q < cnt; q += blockDim.x)
+            for (int r = 0; r < nrhs; r++)
+                s_x[r][q] = x[(size_t) r * n + t0 + q];
+        __syncthreads();
+        if (i < n) {
+            const T* col = A + (size_t) t0 * n + i;
+#pragma unroll 8
+            for (int j = 0; j < cnt; j++) {
+                const double a = (double) __ldcs(col + (size_t) j * n);
+#pragma unroll
+                for (int r = 0; r < kMaxRhs; r++)
+                    if (r < nrhs)
+                        acc[r] += a * s_x[r][j];
+            }
+        }
+    }
+    if (i >= n)
+        return;
+    for (int r = 0; r < nrhs; r++) {
+        if (partial)
+            partial[((size_t) blockIdx.y * nrhs + r) * n + i] = acc[r];
+        else
+            y[(size_t) r * n + i] = acc[r];
+    }
+}
+
+}  // namespace kemcu
+
+namespace kemcu
+{
+// ------------------------------------------------------------------------- point ordering
+// Points are evaluated in Morton (Z-curve) order so that the 32 points of a warp are close
+// together and take the same quadrature band for almost every element: the band branch is
+// then warp-uniform. The permutation is applied on the device and undone on the results.
+
+__device__ __forceinline__ unsigned long long spread3(unsigned v)
+{
+    unsigned long long x = v & 0x1fffffu;
+    x = (x | x << 32) & 0x1f00000000ffffULL;
+    x = (x | x << 16) & 0x1f0000ff0000ffULL;
+    x = (x | x << 8) & 0x100f00f00f00f00fULL;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ULL;
+    x = (x | x << 2) & 0x1249249249249249ULL;
+    return x;
+}
+
+// bounding box: box[0..2] = min, box[3..5] = max; partial[gridDim.x][6]; last block reduces
+__global__ void bbox_kernel(const double* __restrict__ P, int n, double* __restrict__ partial,
+                            unsigned* __restrict__ counter, double* __restrict__ box)
+{
+    __shared__ double sh[6][256];
+    __shared__ bool last;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (int c = 0; c < 3; c++) {
+            const double v = P[3 * i + c];
+            lo[c] = fmin(lo[c], v);
+            hi[c] = fmax(hi[c], v);
+        }
+    for (int c = 0; c < 3; c++) {
+        sh[c][threadIdx.x] = lo[c];
+        sh[3 + c][threadIdx.x] = hi[c];
+    }
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int c = 0; c < 3; c++) {
+                sh[c][threadIdx.x] = fmin(sh[c][threadIdx.x], sh[c][threadIdx.x + s]);
+                sh[3 + c][threadIdx.x] = fmax(sh[3 + c][threadIdx.x], sh[3 + c][threadIdx.x + s]);
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x < 6)
+        partial[blockIdx.x * 6 + threadIdx.x] = sh[threadIdx.x][0];
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0)
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last)
+        return;
+    __threadfence();
+    if (threadIdx.x < 6) {
+        double v = threadIdx.x < 3 ? 1e300 : -1e300;
+        for (int b = 0; b < (int) gridDim.x; b++) {
+            const double q = __ldcg(partial + b * 6 + threadIdx.x);
+            v = threadIdx.x < 3 ? fmin(v, q) : fmax(v, q);
+        }
+        box[threadIdx.x] = v;
+    }
+    if (threadIdx.x == 0)
+        *counter = 0u;
+}
+
+__global__ void morton_kernel(const double* __restrict__ P, int n, const double* __restrict__ box,
+                              unsigned long long* __restrict__ key, int* __restrict__ idx)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    unsigned q[3];
+    for (int c = 0; c < 3; c++) {
+        const double ext = box[3 + c] - box[c];
+        const double t = ext > 0. ? (P[3 * i + c] - box[c]) / ext : 0.;
+        q[c] = (unsigned) fmin(fmax(t * 2097151.0, 0.), 2097151.0);
+    }
+    key[i] = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
+    idx[i] = i;
+}
+
+__global__ void gather_points_kernel(const double* __restrict__ P, const int* __restrict__ perm, int n,
+                                     double* __restrict__ Q)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const int j = perm[i];
+    Q[3 * i] = P[3 * j];
+    Q[3 * i + 1] = P[3 * j + 1];
+    Q[3 * i + 2] = P[3 * j + 2];
+}
+
+__global__ void scatter_out_kernel(const double* __restrict__ src, const int* __restrict__ perm, int n,
+                                   double* __restrict__ dst)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const int j = perm[i];
+    // scalar stores: dst may be a caller's device pointer with only 8-byte alignment
+    dst[4 * (size_t) j] = src[4 * (size_t) i];
+    dst[4 * (size_t) j + 1] = src[4 * (size_t) i + 1];
+    dst[4 * (size_t) j + 2] = src[4 * (size_t) i + 2];
+    dst[4 * (size_t) j + 3] = src[4 * (size_t) i + 3];
+}
+}  // namespace kemcu

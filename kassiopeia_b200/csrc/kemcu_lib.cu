@@ -1,0 +1,1026 @@
+// libkemcu: host side of the C ABI declared in include/kemcu.h.
+//
+// One translation unit so the __constant__ rule tables are shared by every kernel without
+// relocatable device code. Host code here is C++17; nothing crosses the ABI but plain types.
+
+#include "kemcu.h"
+#include "kemcu_device.cuh"
+#include "kemcu_kernels.cuh"
+#include "kemcu_solver.cuh"
+#include "kemcu_tables.cuh"
+#include "kemcu_track.cuh"
+#include "kemcu_adjoint.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace kemcu;
+
+// ------------------------------------------------------------------------------- context
+struct DevBuf
+{
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct kemcu_ctx
+{
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int num_sms = 0;
+    Constants k{};
+    size_t assembled_budget = 0;
+    std::string err;
+    double last_ms = 0.;
+    // geometry
+    size_t n = 0;
+    std::vector<double> h_rec;         // n x 32 element records
+    std::vector<TargetRec> h_tgt;      // n matrix-row targets
+    std::vector<double> h_rhs;         // boundary values
+    std::vector<int32_t> h_shape;
+    double* d_rec = nullptr;
+    TargetRec* d_tgt = nullptr;
+    double* d_sigma = nullptr;
+    bool have_sigma = false;
+    // assembled operator (column-major)
+    double* d_a64 = nullptr;
+    float* d_a32 = nullptr;
+    // grow-only scratch
+    DevBuf scratch[9];
+    unsigned* d_counter = nullptr;
+    int* d_flag = nullptr;
+    kemcu_iteration_callback cb = nullptr;
+    void* cb_user = nullptr;
+};
+
+namespace
+{
+enum Scratch
+{
+    sPts = 0,
+    sOut,
+    sPartial,
+    sVec0,
+    sVec1,
+    sVec2,
+    sBasis,
+    sMisc,
+    sSort  // Morton-ordering workspace of kemcu_field_dev (never aliases a caller's staging slot)
+};
+
+int fail(kemcu_ctx* c, int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c)
+        c->err = buf;
+    return code;
+}
+
+#define KC(call)                                                                                        \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            return fail(ctx, KEMCU_ECUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                        __LINE__);                                                                      \
+    } while (0)
+
+#define KCHECK_LAUNCH() KC(cudaGetLastError())
+
+int ensure(kemcu_ctx* ctx, int slot, size_t bytes, void** out)
+{
+    DevBuf& b = ctx->scratch[slot];
+    if (b.bytes < bytes) {
+        if (b.p)
+            KC(cudaFree(b.p));
+        b.p = nullptr;
+        b.bytes = 0;
+        const size_t want = std::max(bytes, (size_t) 256);
+        if (cudaMalloc(&b.p, want) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ctx, KEMCU_ENOMEM, "device allocation of %zu bytes failed", want);
+        }
+        b.bytes = want;
+    }
+    *out = b.p;
+    return KEMCU_OK;
+}
+
+// element record and matrix-row target of one element, in the reference's FP64 operation
+// order (no FMA: the host compiler targets baseline x86-64)
+void build_record(const double* g, int shape, int boundary, double value, const Constants& K, double* r,
+                  TargetRec& t, double& rhs)
+{
+    for (int i = 0; i < rRecSize; i++)
+        r[i] = 0.;
+    r[rType] = (double) shape;
+    if (shape == kLineSegment) {
+        const double d0 = g[3] - g[0], d1 = g[4] - g[1], d2 = g[5] - g[2];
+        const double len = std::sqrt((d0 * d0) + (d1 * d1) + (d2 * d2));
+        r[rA] = len;
+        r[rB] = g[6];
+        for (int c = 0; c < 3; c++) {
+            r[rP0 + c] = g[c];
+            r[rN1 + c] = g[3 + c];
+            r[rEa + c] = g[3 + c] - g[c];
+            r[rCen + c] = (g[c] + g[3 + c]) * 0.5;
+            r[rCen2 + c] = r[rCen + c];
+        }
+        r[rInvSize] = 1. / len;
+        r[rPrefac] = g[6] / (4. * K.eps0);
+        // KLineSegment::Normal() (KLineSegment.cc:27-33)
+        double nx, ny, nz;
+        if (d0 > 1.e-10) {  // d x (1,0,0)
+            nx = 0.;
+            ny = d2;
+            nz = -d1;
+        }
+        else {  // d x (0,1,0)
+            nx = -d2;
+            ny = 0.;
+            nz = d0;
+        }
+        const double m = std::sqrt(nx * nx + ny * ny + nz * nz);
+        t.normal[0] = nx / m;
+        t.normal[1] = ny / m;
+        t.normal[2] = nz / m;
+    }
+    else {
+        const double A = g[0], B = g[1];
+        for (int i = 0; i < 11; i++)
+            r[i] = g[i];
+        for (int c = 0; c < 3; c++) {
+            r[rEa + c] = A * g[5 + c];
+            r[rEb + c] = B * g[8 + c];
+        }
+        const double cx = g[6] * g[10] - g[7] * g[9], cy = g[7] * g[8] - g[5] * g[10], cz = g[5] * g[9] - g[6] * g[8];
+        const double cm = std::sqrt((cx * cx) + (cy * cy) + (cz * cz));
+        r[rN3] = cx * (1. / cm);
+        r[rN3 + 1] = cy * (1. / cm);
+        r[rN3 + 2] = cz * (1. / cm);
+        if (shape == kTriangle) {
+            double p1[3], p2[3];
+            for (int c = 0; c < 3; c++) {
+                p1[c] = g[2 + c] + (A * g[5 + c]);
+                p2[c] = g[2 + c] + (B * g[8 + c]);
+                r[rCen + c] = g[2 + c] + (A * g[5 + c] + B * g[8 + c]) / 3.;
+                r[rCen2 + c] = r[rCen + c];
+            }
+            const double l12 = std::sqrt(((p2[0] - p1[0]) * (p2[0] - p1[0])) + ((p2[1] - p1[1]) * (p2[1] - p1[1])) +
+                                         ((p2[2] - p1[2]) * (p2[2] - p1[2])));
+            const double size = (A + B + l12) / 3.;
+            r[rInvSize] = 1. / size;
+            r[rPrefac] = 0.5 * A * B * cm * K.one_over_four_pi_eps0;
+            for (int c = 0; c < 3; c++)
+                t.normal[c] = r[rN3 + c];
+        }
+        else {
+            for (int c = 0; c < 3; c++) {
+                r[rCen + c] = g[2 + c] + 0.5 * (A * g[5 + c] + B * g[8 + c]);
+                r[rCen2 + c] = (g[2 + c] + A * g[5 + c] * .5) + B * g[8 + c] * .5;
+            }
+            const double size = 0.5 * (A + B);
+            r[rInvSize] = 1. / size;
+            r[rPrefac] = A * B * K.one_over_four_pi_eps0;
+            // KRectangle::Normal() returns N1 x N2 unnormalised (KRectangle.cc:7-16)
+            t.normal[0] = cx;
+            t.normal[1] = cy;
+            t.normal[2] = cz;
+        }
+    }
+    // squared band cut distances (ratio = |P - c| / size); ambiguous cases are resolved
+    // on the device with the reference's exact expression
+    const double tri_cut[3] = {3.42, 30.4, 131.4}, rect_cut[3] = {4.6, 44.6, 196.2}, line_cut[3] = {2., 27.7, 1e300};
+    const double* cut = shape == kTriangle ? tri_cut : shape == kRectangle ? rect_cut : line_cut;
+    for (int k = 0; k < 3; k++) {
+        const double dcut = cut[k] / r[rInvSize];
+        r[rCut + k] = cut[k] > 1e299 ? 1e300 : dcut * dcut;
+    }
+    for (int c = 0; c < 3; c++)
+        t.cen[c] = r[rCen2 + c];
+    t.neumann = boundary == KEMCU_NEUMANN ? 1. : 0.;
+    t.diag = boundary == KEMCU_NEUMANN ? ((1. + value) / (1. - value)) / (2. * K.eps0) : 0.;
+    rhs = boundary == KEMCU_NEUMANN ? 0. : value;
+}
+
+int grid_split(const kemcu_ctx* ctx, size_t n_pts, size_t n_elem)
+{
+    const size_t blocks = (n_pts + kThreads - 1) / kThreads;
+    const size_t want = (size_t) ctx->num_sms * 8;
+    size_t split = blocks >= want ? 1 : (want + blocks - 1) / blocks;
+    split = std::min(split, std::max((size_t) 1, n_elem / 64));
+    split = std::min(split, (size_t) 65535);
+    return (int) std::max((size_t) 1, split);
+}
+
+// field at device points; d_out n x 4
+int launch_field(kemcu_ctx* ctx, const double* d_pts, size_t n, double* d_out, int precision, int what)
+{
+    const int split = grid_split(ctx, n, ctx->n);
+    double* partial = nullptr;
+    if (split > 1) {
+        void* p;
+        int rc = ensure(ctx, sPartial, (size_t) split * n * 4 * sizeof(double), &p);
+        if (rc)
+            return rc;
+        partial = (double*) p;
+    }
+    dim3 grid((unsigned) ((n + kThreads - 1) / kThreads), (unsigned) split);
+    const bool mixed = precision == KEMCU_MIXED;
+    const double* sg = ctx->d_sigma;
+    const int ne = (int) ctx->n;
+    if (what == KEMCU_POTENTIAL) {
+        if (mixed)
+            field_kernel<true, true, false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial);
+        else
+            field_kernel<false, true, false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial);
+    }
+    else if (what == KEMCU_FIELD) {
+        if (mixed)
+            field_kernel<true, false, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial);
+        else
+            field_kernel<false, false, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial);
+    }
+    else {
+        if (mixed)
+            field_kernel<true, true, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial);
+        else
+            field_kernel<false, true, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial);
+    }
+    KCHECK_LAUNCH();
+    if (split > 1) {
+        const size_t m = n * 4;
+        reduce_splits<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(partial, split, m, d_out);
+        KCHECK_LAUNCH();
+    }
+    return KEMCU_OK;
+}
+
+constexpr size_t kSortMin = 4096;  // below this the point set is evaluated in caller order
+
+size_t cub_sort_bytes(size_t n)
+{
+    size_t b = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, b, (const unsigned long long*) nullptr, (unsigned long long*) nullptr,
+                                    (const int*) nullptr, (int*) nullptr, (int) n, 0, 63);
+    return b;
+}
+
+int check_finite(kemcu_ctx* ctx, const double* d, size_t m, const char* what)
+{
+    KC(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+    finite_kernel<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(d, m, ctx->d_flag);
+    KCHECK_LAUNCH();
+    int flag = 0;
+    KC(cudaMemcpyAsync(&flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    KC(cudaStreamSynchronize(ctx->stream));
+    if (flag)
+        return fail(ctx, KEMCU_ENONFINITE, "%s contains NaN or Inf", what);
+    return KEMCU_OK;
+}
+
+int check_ready(kemcu_ctx* ctx, bool need_sigma)
+{
+    if (!ctx)
+        return KEMCU_EINVAL;
+    if (ctx->n == 0)
+        return fail(ctx, KEMCU_ESTATE, "no geometry set");
+    if (need_sigma && !ctx->have_sigma)
+        return fail(ctx, KEMCU_ESTATE, "no charge densities set (kemcu_set_sigma or kemcu_gmres first)");
+    return KEMCU_OK;
+}
+
+struct Timer
+{
+    kemcu_ctx* ctx;
+    explicit Timer(kemcu_ctx* c) : ctx(c)
+    {
+        cudaEventRecord(ctx->ev0, ctx->stream);
+    }
+    void stop()
+    {
+        cudaEventRecord(ctx->ev1, ctx->stream);
+        cudaEventSynchronize(ctx->ev1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        ctx->last_ms = ms;
+    }
+};
+
+// ------------------------------------------------------------------------------- operators
+enum OpKind
+{
+    kFree64 = 0,
+    kFreeMixed,
+    kDense64,
+    kDense32
+};
+
+int apply_op(kemcu_ctx* ctx, int op, const double* d_x, double* d_y, int nrhs)
+{
+    const int n = (int) ctx->n;
+    if (op == kFree64 || op == kFreeMixed) {
+        const int split = grid_split(ctx, n, n);
+        double* partial = nullptr;
+        if (split > 1) {
+            void* p;
+            int rc = ensure(ctx, sPartial, (size_t) split * nrhs * n * sizeof(double), &p);
+            if (rc)
+                return rc;
+            partial = (double*) p;
+        }
+        dim3 grid((n + kThreads - 1) / kThreads, split);
+        if (op == kFree64)
+            matvec_kernel<false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, ctx->d_tgt, n, d_x, nrhs, d_y, partial);
+        else
+            matvec_kernel<true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, ctx->d_tgt, n, d_x, nrhs, d_y, partial);
+        KCHECK_LAUNCH();
+        if (split > 1) {
+            const size_t m = (size_t) nrhs * n;
+            reduce_splits<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(partial, split, m, d_y);
+            KCHECK_LAUNCH();
+        }
+        return KEMCU_OK;
+    }
+    const size_t rows_blocks = (n + 255) / 256;
+    size_t split = std::max((size_t) 1, (size_t) ctx->num_sms * 4 / rows_blocks);
+    split = std::min(split, (size_t) std::max(1, n / 256));
+    double* partial = nullptr;
+    if (split > 1) {
+        void* p;
+        int rc = ensure(ctx, sPartial, split * nrhs * n * sizeof(double), &p);
+        if (rc)
+            return rc;
+        partial = (double*) p;
+    }
+    dim3 grid((unsigned) rows_blocks, (unsigned) split);
+    if (op == kDense64)
+        dense_matvec_kernel<double><<<grid, 256, 0, ctx->stream>>>(ctx->d_a64, n, d_x, nrhs, d_y, partial);
+    else
+        dense_matvec_kernel<float><<<grid, 256, 0, ctx->stream>>>(ctx->d_a32, n, d_x, nrhs, d_y, partial);
+    KCHECK_LAUNCH();
+    if (split > 1) {
+        const size_t m = (size_t) nrhs * n;
+        reduce_splits<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(partial, (int) split, m, d_y);
+        KCHECK_LAUNCH();
+    }
+    return KEMCU_OK;
+}
+
+int assemble(kemcu_ctx* ctx, bool want32)
+{
+    const size_t n = ctx->n;
+    if (ctx->d_a64 && (!want32 || ctx->d_a32))
+        return KEMCU_OK;
+    const size_t bytes64 = n * n * sizeof(double), bytes32 = want32 ? n * n * sizeof(float) : 0;
+    size_t budget = ctx->assembled_budget;
+    if (budget == 0) {
+        size_t fr = 0, tot = 0;
+        KC(cudaMemGetInfo(&fr, &tot));
+        budget = (size_t) (0.7 * (double) fr) + (ctx->d_a64 ? bytes64 : 0);
+    }
+    if (bytes64 + bytes32 > budget)
+        return fail(ctx, KEMCU_ENOMEM, "assembled operator needs %zu bytes, budget %zu", bytes64 + bytes32, budget);
+    if (!ctx->d_a64 && cudaMalloc(&ctx->d_a64, bytes64) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->d_a64 = nullptr;
+        return fail(ctx, KEMCU_ENOMEM, "allocation of the assembled operator failed");
+    }
+    const bool fill32 = want32 && !ctx->d_a32;
+    if (fill32 && cudaMalloc(&ctx->d_a32, bytes32) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->d_a32 = nullptr;
+        return fail(ctx, KEMCU_ENOMEM, "allocation of the FP32 operator copy failed");
+    }
+    const int split = grid_split(ctx, n, n);
+    dim3 grid((unsigned) ((n + kThreads - 1) / kThreads), (unsigned) split);
+    assemble_kernel<false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, ctx->d_tgt, (int) n, 0, (int) n, ctx->d_a64,
+                                                              fill32 ? ctx->d_a32 : nullptr);
+    KCHECK_LAUNCH();
+    return KEMCU_OK;
+}
+
+// ------------------------------------------------------------------------------- GMRES
+// GMRES(m) without restart from x0 = 0, as KGeneralizedMinimalResidual (x = V y, residual
+// estimate |p_{j+1}| relative to |b|). Orthogonalisation is classical Gram-Schmidt applied
+// twice (CGS2), which is as accurate as the reference's modified Gram-Schmidt and reads the
+// basis with two batched passes instead of j sequential ones. The j x j triangular solve
+// uses back-substitution (KGeneralizedMinimalResidual::UseBackSubstitution).
+int gmres_core(kemcu_ctx* ctx, int op, const double* d_b, double* d_x, int nrhs, double tol, int max_iter,
+               int& iters, double& est, int& matvecs)
+{
+    const int n = (int) ctx->n;
+    const int m = std::max(1, max_iter);
+    const int hs = m + 2;
+    void *pV, *pW, *pH, *pP;
+    int rc;
+    if ((rc = ensure(ctx, sBasis, (size_t) (m + 1) * nrhs * n * sizeof(double), &pV)))
+        return rc;
+    if ((rc = ensure(ctx, sVec2, (size_t) nrhs * n * sizeof(double), &pW)))
+        return rc;
+    if ((rc = ensure(ctx, sMisc, (size_t) nrhs * hs * 3 * sizeof(double) + 64 * (size_t) nrhs * kDotBlocks * sizeof(double), &pH)))
+        return rc;
+    double* V = (double*) pV;
+    double* w = (double*) pW;
+    double* h = (double*) pH;             // [nrhs][hs] first projection
+    double* h2 = h + (size_t) nrhs * hs;  // [nrhs][hs] second projection / norms
+    double* yv = h2 + (size_t) nrhs * hs; // [nrhs][hs] solution coefficients
+    double* part = yv + (size_t) nrhs * hs;
+    (void) pP;
+    const dim3 vg((n + 255) / 256, nrhs);
+    // |b| and v0 = b / |b|
+    KC(cudaMemcpyAsync(V, d_b, (size_t) nrhs * n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    multi_dot_kernel<<<dim3(kDotBlocks, nrhs), kDotThreads, 0, ctx->stream>>>(V, V, n, nrhs, 0, 1, part, ctx->d_counter, h2, hs);
+    KCHECK_LAUNCH();
+    scale_kernel<<<vg, 256, 0, ctx->stream>>>(V, V, n, h2, hs, 0);
+    KCHECK_LAUNCH();
+    std::vector<double> hb((size_t) nrhs * hs);
+    KC(cudaMemcpyAsync(hb.data(), h2, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    KC(cudaStreamSynchronize(ctx->stream));
+    std::vector<double> bnorm(nrhs), p((size_t) nrhs * hs, 0.), cs((size_t) nrhs * hs), sn((size_t) nrhs * hs);
+    std::vector<std::vector<double>> H(nrhs, std::vector<double>((size_t) hs * hs, 0.));  // column-major R
+    std::vector<int> kfin(nrhs, 0);
+    std::vector<char> done(nrhs, 0);
+    for (int r = 0; r < nrhs; r++) {
+        bnorm[r] = std::sqrt(hb[(size_t) r * hs]);
+        p[(size_t) r * hs] = bnorm[r];
+        if (!(bnorm[r] > 0.))
+            done[r] = 1;
+    }
+    iters = 0;
+    est = 0.;
+    std::vector<double> hcol((size_t) nrhs * hs), hcol2((size_t) nrhs * hs);
+    for (int j = 0; j < m; j++) {
+        bool all = true;
+        for (int r = 0; r < nrhs; r++)
+            all = all && done[r];
+        if (all)
+            break;
+        double* vj = V + (size_t) j * nrhs * n;
+        double* vn = V + (size_t) (j + 1) * nrhs * n;
+        if ((rc = apply_op(ctx, op, vj, w, nrhs)))
+            return rc;
+        matvecs++;
+        for (int pass = 0; pass < 2; pass++) {
+            double* hh = pass == 0 ? h : h2;
+            for (int k0 = 0; k0 <= j; k0 += 64) {
+                const int nk = std::min(64, j + 1 - k0);
+                multi_dot_kernel<<<dim3(kDotBlocks, nrhs), kDotThreads, 0, ctx->stream>>>(V, w, n, nrhs, k0, nk, part,
+                                                                                         ctx->d_counter, hh, hs);
+                KCHECK_LAUNCH();
+            }
+            for (int k0 = 0; k0 <= j; k0 += 64) {
+                const int nk = std::min(64, j + 1 - k0);
+                gs_update_kernel<<<vg, 256, 0, ctx->stream>>>(V, w, n, nrhs, k0, nk, hh, hs, nullptr);
+                KCHECK_LAUNCH();
+            }
+        }
+        // beta^2 into h2[r][j+1]
+        multi_dot_kernel<<<dim3(kDotBlocks, nrhs), kDotThreads, 0, ctx->stream>>>(w - 0, w, n, nrhs, 0, 1, part, ctx->d_counter,
+                                                                                 yv, hs);
+        KCHECK_LAUNCH();
+        scale_kernel<<<vg, 256, 0, ctx->stream>>>(w, vn, n, yv, hs, 0);
+        KCHECK_LAUNCH();
+        KC(cudaMemcpyAsync(hcol.data(), h, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        KC(cudaMemcpyAsync(hcol2.data(), h2, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        std::vector<double> b2(nrhs * (size_t) hs);
+        KC(cudaMemcpyAsync(b2.data(), yv, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        KC(cudaStreamSynchronize(ctx->stream));
+        iters = j + 1;
+        double worst = 0.;
+        for (int r = 0; r < nrhs; r++) {
+            if (done[r])
+                continue;
+            double* col = H[r].data() + (size_t) j * hs;
+            for (int k = 0; k <= j; k++)
+                col[k] = hcol[(size_t) r * hs + k] + hcol2[(size_t) r * hs + k];
+            const double beta = std::sqrt(b2[(size_t) r * hs]);
+            // apply previous Givens rotations (KGeneralizedMinimalResidual.hh:240-246)
+            for (int k = 0; k < j; k++) {
+                const double a = col[k], b = col[k + 1];
+                col[k] = cs[(size_t) r * hs + k] * a + sn[(size_t) r * hs + k] * b;
+                col[k + 1] = -sn[(size_t) r * hs + k] * a + cs[(size_t) r * hs + k] * b;
+            }
+            const double gam = std::sqrt(col[j] * col[j] + beta * beta);
+            cs[(size_t) r * hs + j] = col[j] / gam;
+            sn[(size_t) r * hs + j] = beta / gam;
+            col[j] = gam;
+            p[(size_t) r * hs + j + 1] = -sn[(size_t) r * hs + j] * p[(size_t) r * hs + j];
+            p[(size_t) r * hs + j] = cs[(size_t) r * hs + j] * p[(size_t) r * hs + j];
+            const double rel = std::fabs(p[(size_t) r * hs + j + 1]) / bnorm[r];
+            kfin[r] = j + 1;
+            if (rel <= tol || !(beta > 0.))
+                done[r] = 1;
+            worst = std::max(worst, rel);
+        }
+        est = worst;
+        if (ctx->cb && ctx->cb(ctx->cb_user, iters, worst))
+            break;
+    }
+    // y = R^-1 p, x = V y
+    std::vector<double> y((size_t) nrhs * hs, 0.);
+    for (int r = 0; r < nrhs; r++) {
+        const int k = kfin[r];
+        for (int i = k - 1; i >= 0; i--) {
+            double s = p[(size_t) r * hs + i];
+            for (int c = i + 1; c < k; c++)
+                s -= H[r][(size_t) c * hs + i] * y[(size_t) r * hs + c];
+            y[(size_t) r * hs + i] = s / H[r][(size_t) i * hs + i];
+        }
+    }
+    int* d_k;
+    void* pk;
+    if ((rc = ensure(ctx, sVec1, (size_t) nrhs * sizeof(int) + 256, &pk)))
+        return rc;
+    d_k = (int*) pk;
+    KC(cudaMemcpyAsync(yv, y.data(), (size_t) nrhs * hs * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    KC(cudaMemcpyAsync(d_k, kfin.data(), (size_t) nrhs * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    KC(cudaMemsetAsync(d_x, 0, (size_t) nrhs * n * sizeof(double), ctx->stream));
+    combine_kernel<<<vg, 256, 0, ctx->stream>>>(V, yv, hs, n, nrhs, d_k, d_x);
+    KCHECK_LAUNCH();
+    KC(cudaStreamSynchronize(ctx->stream));
+    return KEMCU_OK;
+}
+
+double inner_tolerance()
+{
+    const char* s = getenv("KEMCU_INNER_TOL");
+    return s ? atof(s) : 1e-6;
+}
+}  // namespace
+
+// ------------------------------------------------------------------------------- C ABI
+extern "C" {
+
+void kemcu_default_config(kemcu_config* cfg)
+{
+    if (!cfg)
+        return;
+    cfg->device = 0;
+    cfg->one_over_four_pi_eps0 = 1. / (4. * 3.141592653589793238462643383279502884 * 8.8541878128e-12);
+    cfg->eps0 = 8.8541878128e-12;
+    cfg->assembled_budget_bytes = 0;
+}
+
+int kemcu_create(kemcu_ctx** out, const kemcu_config* cfg)
+{
+    if (!out)
+        return KEMCU_EINVAL;
+    *out = nullptr;
+    kemcu_config def;
+    kemcu_default_config(&def);
+    if (!cfg)
+        cfg = &def;
+    auto* ctx = new kemcu_ctx();
+    ctx->device = cfg->device;
+    ctx->k.one_over_four_pi_eps0 = cfg->one_over_four_pi_eps0;
+    ctx->k.eps0 = cfg->eps0;
+    ctx->k.pi = 3.141592653589793238462643383279502884;
+    ctx->assembled_budget = cfg->assembled_budget_bytes;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev <= cfg->device || cfg->device < 0) {
+        cudaGetLastError();
+        *out = ctx;
+        return fail(ctx, KEMCU_ECUDA, "no usable CUDA device %d (%s)", cfg->device,
+                    e == cudaSuccess ? "ordinal out of range" : cudaGetErrorString(e));
+    }
+    *out = ctx;
+    KC(cudaSetDevice(ctx->device));
+    cudaDeviceProp prop;
+    KC(cudaGetDeviceProperties(&prop, ctx->device));
+    if (prop.major < 10)
+        return fail(ctx, KEMCU_ECUDA, "device %s is sm_%d%d; this library is built for sm_100a", prop.name, prop.major,
+                    prop.minor);
+    ctx->num_sms = prop.multiProcessorCount;
+    KC(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    KC(cudaEventCreate(&ctx->ev0));
+    KC(cudaEventCreate(&ctx->ev1));
+    KC(cudaMalloc(&ctx->d_counter, 64 * sizeof(unsigned)));
+    KC(cudaMemset(ctx->d_counter, 0, 64 * sizeof(unsigned)));
+    KC(cudaMalloc(&ctx->d_flag, sizeof(int)));
+    // rule tables
+    std::vector<double> rules(kNumNodes * 3), gl(20), wsum(kNumNodes, 0.);
+    std::vector<float> rf(kNumNodes * 4, 0.f);
+    tables::build(rules.data(), gl.data());
+    const int offs[7] = {kTri7, kTri12, kTri33, kRect7, kRect12, kRect33, kNumNodes};
+    for (int q = 0; q < 6; q++) {
+        const double sc = q < 3 ? 1. / 3. : 0.5;
+        double ws = 0.;
+        for (int k = offs[q]; k < offs[q + 1]; k++) {
+            rf[4 * k] = (float) (rules[3 * k] - sc);
+            rf[4 * k + 1] = (float) (rules[3 * k + 1] - sc);
+            rf[4 * k + 2] = (float) rules[3 * k + 2];
+            ws += rules[3 * k + 2];
+        }
+        wsum[offs[q]] = ws;
+    }
+    KC(cudaMemcpyToSymbol(c_rules, rules.data(), rules.size() * sizeof(double)));
+    KC(cudaMemcpyToSymbol(c_rules_f, rf.data(), rf.size() * sizeof(float)));
+    KC(cudaMemcpyToSymbol(c_gl, gl.data(), gl.size() * sizeof(double)));
+    KC(cudaMemcpyToSymbol(c_wsum, wsum.data(), wsum.size() * sizeof(double)));
+    KC(cudaMemcpyToSymbol(c_k, &ctx->k, sizeof(Constants)));
+    double rk[kStages][kStages];
+    rk8_table(rk);
+    KC(cudaMemcpyToSymbol(c_rk8, rk, sizeof rk));
+    return KEMCU_OK;
+}
+
+int kemcu_destroy(kemcu_ctx* ctx)
+{
+    if (!ctx)
+        return KEMCU_OK;
+    if (ctx->stream) {
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+        for (auto& b : ctx->scratch)
+            if (b.p)
+                cudaFree(b.p);
+        cudaFree(ctx->d_rec);
+        cudaFree(ctx->d_tgt);
+        cudaFree(ctx->d_sigma);
+        cudaFree(ctx->d_a64);
+        cudaFree(ctx->d_a32);
+        cudaFree(ctx->d_counter);
+        cudaFree(ctx->d_flag);
+        cudaEventDestroy(ctx->ev0);
+        cudaEventDestroy(ctx->ev1);
+        cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+    return KEMCU_OK;
+}
+
+const char* kemcu_last_error(const kemcu_ctx* ctx)
+{
+    return ctx ? ctx->err.c_str() : "null context";
+}
+
+double kemcu_last_kernel_ms(const kemcu_ctx* ctx)
+{
+    return ctx ? ctx->last_ms : 0.;
+}
+
+size_t kemcu_num_elements(const kemcu_ctx* ctx)
+{
+    return ctx ? ctx->n : 0;
+}
+
+int kemcu_set_geometry(kemcu_ctx* ctx, size_t n, const int32_t* shape, const int32_t* boundary, const double* geom11,
+                       const double* value)
+{
+    if (!ctx || !ctx->stream)
+        return ctx ? fail(ctx, KEMCU_ESTATE, "context has no device") : KEMCU_EINVAL;
+    if (n == 0 || n > (size_t) 0x7fffffff || !shape || !boundary || !geom11 || !value)
+        return fail(ctx, KEMCU_EINVAL, "invalid geometry arguments (n = %zu)", n);
+    KC(cudaSetDevice(ctx->device));
+    for (size_t i = 0; i < n; i++) {
+        if (shape[i] < 0 || shape[i] > 2 || (boundary[i] != 0 && boundary[i] != 1))
+            return fail(ctx, KEMCU_EINVAL, "element %zu: shape %d / boundary %d not supported", i, shape[i], boundary[i]);
+        for (int c = 0; c < 11; c++)
+            if (!std::isfinite(geom11[11 * i + c]))
+                return fail(ctx, KEMCU_EINVAL, "element %zu: non-finite geometry", i);
+        const double* g = geom11 + 11 * i;
+        if (shape[i] != kLineSegment && !(g[0] > 0. && g[1] > 0.))
+            return fail(ctx, KEMCU_EINVAL, "element %zu: side lengths must be positive", i);
+    }
+    // release everything that depends on the old geometry
+    cudaFree(ctx->d_rec);
+    cudaFree(ctx->d_tgt);
+    cudaFree(ctx->d_sigma);
+    cudaFree(ctx->d_a64);
+    cudaFree(ctx->d_a32);
+    ctx->d_rec = nullptr;
+    ctx->d_tgt = nullptr;
+    ctx->d_sigma = nullptr;
+    ctx->d_a64 = nullptr;
+    ctx->d_a32 = nullptr;
+    ctx->have_sigma = false;
+    ctx->n = 0;
+    ctx->h_rec.assign(n * rRecSize, 0.);
+    ctx->h_tgt.assign(n, TargetRec{});
+    ctx->h_rhs.assign(n, 0.);
+    ctx->h_shape.assign(shape, shape + n);
+    for (size_t i = 0; i < n; i++)
+        build_record(geom11 + 11 * i, shape[i], boundary[i], value[i], ctx->k, ctx->h_rec.data() + i * rRecSize,
+                     ctx->h_tgt[i], ctx->h_rhs[i]);
+    KC(cudaMalloc(&ctx->d_rec, n * rRecSize * sizeof(double)));
+    KC(cudaMalloc(&ctx->d_tgt, n * sizeof(TargetRec)));
+    KC(cudaMalloc(&ctx->d_sigma, n * sizeof(double)));
+    KC(cudaMemcpy(ctx->d_rec, ctx->h_rec.data(), n * rRecSize * sizeof(double), cudaMemcpyHostToDevice));
+    KC(cudaMemcpy(ctx->d_tgt, ctx->h_tgt.data(), n * sizeof(TargetRec), cudaMemcpyHostToDevice));
+    KC(cudaMemset(ctx->d_sigma, 0, n * sizeof(double)));
+    ctx->n = n;
+    return KEMCU_OK;
+}
+
+int kemcu_set_sigma(kemcu_ctx* ctx, const double* sigma)
+{
+    int rc = check_ready(ctx, false);
+    if (rc)
+        return rc;
+    if (!sigma)
+        return fail(ctx, KEMCU_EINVAL, "null sigma");
+    KC(cudaMemcpy(ctx->d_sigma, sigma, ctx->n * sizeof(double), cudaMemcpyHostToDevice));
+    ctx->have_sigma = true;
+    return KEMCU_OK;
+}
+
+int kemcu_get_sigma(kemcu_ctx* ctx, double* sigma)
+{
+    int rc = check_ready(ctx, true);
+    if (rc)
+        return rc;
+    KC(cudaMemcpy(sigma, ctx->d_sigma, ctx->n * sizeof(double), cudaMemcpyDeviceToHost));
+    return KEMCU_OK;
+}
+
+int kemcu_rhs(kemcu_ctx* ctx, double* b)
+{
+    int rc = check_ready(ctx, false);
+    if (rc)
+        return rc;
+    std::memcpy(b, ctx->h_rhs.data(), ctx->n * sizeof(double));
+    return KEMCU_OK;
+}
+
+int kemcu_field_dev(kemcu_ctx* ctx, const double* dP, size_t n, double* dout4, int precision, int what)
+{
+    int rc = check_ready(ctx, true);
+    if (rc)
+        return rc;
+    if (n == 0)
+        return KEMCU_OK;
+    if (!dP || !dout4 || n > (size_t) 0x7fffffff || (precision != KEMCU_FP64 && precision != KEMCU_MIXED) || what < 0 ||
+        what > 2)
+        return fail(ctx, KEMCU_EINVAL, "invalid field arguments");
+    KC(cudaSetDevice(ctx->device));
+    Timer t(ctx);
+    if (n < kSortMin) {
+        if ((rc = launch_field(ctx, dP, n, dout4, precision, what)))
+            return rc;
+    }
+    else {
+        // Morton order: bbox -> keys -> radix sort -> gather -> evaluate -> scatter back
+        const size_t cub_bytes = cub_sort_bytes(n);
+        const size_t need = n * (2 * sizeof(unsigned long long) + 2 * sizeof(int) + 7 * sizeof(double)) + cub_bytes +
+                            1024 + 128 * 6 * sizeof(double);
+        void* base;
+        if ((rc = ensure(ctx, sSort, need, &base)))
+            return rc;
+        char* q = (char*) base;
+        auto take = [&q](size_t b) {
+            char* r = q;
+            q += (b + 255) & ~(size_t) 255;
+            return r;
+        };
+        auto* k0 = (unsigned long long*) take(n * 8);
+        auto* k1 = (unsigned long long*) take(n * 8);
+        auto* i0 = (int*) take(n * 4);
+        auto* i1 = (int*) take(n * 4);
+        auto* ps = (double*) take(n * 24);
+        auto* os = (double*) take(n * 32);
+        auto* box = (double*) take(6 * sizeof(double));
+        auto* part = (double*) take(128 * 6 * sizeof(double));
+        void* tmp = take(cub_bytes);
+        bbox_kernel<<<128, 256, 0, ctx->stream>>>(dP, (int) n, part, ctx->d_counter + 32, box);
+        KCHECK_LAUNCH();
+        morton_kernel<<<(unsigned) ((n + 255) / 256), 256, 0, ctx->stream>>>(dP, (int) n, box, k0, i0);
+        KCHECK_LAUNCH();
+        size_t tb = cub_bytes;
+        KC(cub::DeviceRadixSort::SortPairs(tmp, tb, k0, k1, i0, i1, (int) n, 0, 63, ctx->stream));
+        gather_points_kernel<<<(unsigned) ((n + 255) / 256), 256, 0, ctx->stream>>>(dP, i1, (int) n, ps);
+        KCHECK_LAUNCH();
+        if ((rc = launch_field(ctx, ps, n, os, precision, what)))
+            return rc;
+        scatter_out_kernel<<<(unsigned) ((n + 255) / 256), 256, 0, ctx->stream>>>(os, i1, (int) n, dout4);
+        KCHECK_LAUNCH();
+    }
+    t.stop();
+    return check_finite(ctx, dout4, n * 4, "field result");
+}
+
+int kemcu_field(kemcu_ctx* ctx, const double* P, size_t n, double* out4, int precision, int what)
+{
+    int rc = check_ready(ctx, true);
+    if (rc)
+        return rc;
+    if (n == 0)
+        return KEMCU_OK;
+    if (!P || !out4)
+        return fail(ctx, KEMCU_EINVAL, "null point or output buffer");
+    KC(cudaSetDevice(ctx->device));
+    void *dp, *dout;
+    if ((rc = ensure(ctx, sPts, n * 3 * sizeof(double), &dp)) || (rc = ensure(ctx, sOut, n * 4 * sizeof(double), &dout)))
+        return rc;
+    KC(cudaMemcpyAsync(dp, P, n * 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = kemcu_field_dev(ctx, (const double*) dp, n, (double*) dout, precision, what)))
+        return rc;
+    KC(cudaMemcpyAsync(out4, dout, n * 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    KC(cudaStreamSynchronize(ctx->stream));
+    return KEMCU_OK;
+}
+
+int kemcu_matrix_element(kemcu_ctx* ctx, size_t i, size_t j, double* a)
+{
+    int rc = check_ready(ctx, false);
+    if (rc)
+        return rc;
+    if (i >= ctx->n || j >= ctx->n || !a)
+        return fail(ctx, KEMCU_EINVAL, "matrix index out of range");
+    KC(cudaSetDevice(ctx->device));
+    // one column j applied to the unit vector restricted to row i: y = A e_j, read y_i
+    void *dx, *dy;
+    if ((rc = ensure(ctx, sVec0, ctx->n * sizeof(double), &dx)) || (rc = ensure(ctx, sVec1, ctx->n * sizeof(double), &dy)))
+        return rc;
+    KC(cudaMemsetAsync(dx, 0, ctx->n * sizeof(double), ctx->stream));
+    const double one = 1.;
+    KC(cudaMemcpyAsync((double*) dx + j, &one, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = apply_op(ctx, kFree64, (const double*) dx, (double*) dy, 1)))
+        return rc;
+    KC(cudaMemcpyAsync(a, (double*) dy + i, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    KC(cudaStreamSynchronize(ctx->stream));
+    return KEMCU_OK;
+}
+
+int kemcu_matvec(kemcu_ctx* ctx, const double* x, double* y, int n_rhs, int precision, int assembled)
+{
+    int rc = check_ready(ctx, false);
+    if (rc)
+        return rc;
+    if (!x || !y || n_rhs < 1 || n_rhs > kMaxRhs)
+        return fail(ctx, KEMCU_EINVAL, "invalid matvec arguments (n_rhs must be 1..%d)", kMaxRhs);
+    KC(cudaSetDevice(ctx->device));
+    const size_t m = (size_t) n_rhs * ctx->n;
+    void *dx, *dy;
+    if ((rc = ensure(ctx, sVec0, m * sizeof(double), &dx)) || (rc = ensure(ctx, sVec1, m * sizeof(double), &dy)))
+        return rc;
+    KC(cudaMemcpyAsync(dx, x, m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    Timer t(ctx);
+    int op = precision == KEMCU_MIXED ? kFreeMixed : kFree64;
+    if (assembled) {
+        if ((rc = assemble(ctx, precision == KEMCU_MIXED)))
+            return rc;
+        op = precision == KEMCU_MIXED ? kDense32 : kDense64;
+    }
+    if ((rc = apply_op(ctx, op, (const double*) dx, (double*) dy, n_rhs)))
+        return rc;
+    t.stop();
+    KC(cudaMemcpyAsync(y, dy, m * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    KC(cudaStreamSynchronize(ctx->stream));
+    return KEMCU_OK;
+}
+
+void kemcu_set_iteration_callback(kemcu_ctx* ctx, kemcu_iteration_callback cb, void* user)
+{
+    if (!ctx)
+        return;
+    ctx->cb = cb;
+    ctx->cb_user = user;
+}
+
+int kemcu_gmres(kemcu_ctx* ctx, const double* b, double* x, int n_rhs, double rel_tol, int max_iter, int mode,
+                kemcu_solve_stats* stats)
+{
+    int rc = check_ready(ctx, false);
+    if (rc)
+        return rc;
+    if (!x || n_rhs < 1 || n_rhs > kMaxRhs || (b == nullptr && n_rhs != 1) || !(rel_tol > 0.) || max_iter < 1 ||
+        mode < 0 || mode > 2)
+        return fail(ctx, KEMCU_EINVAL, "invalid gmres arguments");
+    KC(cudaSetDevice(ctx->device));
+    const int n = (int) ctx->n;
+    const size_t m = (size_t) n_rhs * n;
+    // device vectors: b, x, residual/correction
+    double *d_b, *d_x, *d_r, *d_d;
+    size_t need = 4 * m * sizeof(double);
+    void* p;
+    if ((rc = ensure(ctx, sVec0, need, &p)))
+        return rc;
+    d_b = (double*) p;
+    d_x = d_b + m;
+    d_r = d_x + m;
+    d_d = d_r + m;
+    if (b)
+        KC(cudaMemcpyAsync(d_b, b, m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    else
+        KC(cudaMemcpyAsync(d_b, ctx->h_rhs.data(), m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    kemcu_solve_stats st{};
+    Timer t(ctx);
+    auto t0 = std::chrono::steady_clock::now();
+    int iters = 0, fp64 = 0, low = 0;
+    double est = 0., rel = 0.;
+    if (mode == KEMCU_SOLVE_PLAIN) {
+        if ((rc = gmres_core(ctx, kFree64, d_b, d_x, n_rhs, rel_tol, max_iter, iters, est, fp64)))
+            return rc;
+        st.outer = 1;
+        rel = est;
+    }
+    else {
+        int low_op = kFreeMixed, hi_op = kFree64;
+        if (mode == KEMCU_SOLVE_ASSEMBLED) {
+            if ((rc = assemble(ctx, true)))
+                return rc;
+            low_op = kDense32;
+            hi_op = kDense64;
+        }
+        const double tin = std::max(rel_tol, inner_tolerance());
+        KC(cudaMemsetAsync(d_x, 0, m * sizeof(double), ctx->stream));
+        KC(cudaMemcpyAsync(d_r, d_b, m * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+        std::vector<double> hb(m);
+        KC(cudaMemcpyAsync(hb.data(), d_b, m * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        KC(cudaStreamSynchronize(ctx->stream));
+        std::vector<double> bn(n_rhs, 0.);
+        for (int r = 0; r < n_rhs; r++) {
+            for (int i = 0; i < n; i++)
+                bn[r] += hb[(size_t) r * n + i] * hb[(size_t) r * n + i];
+            bn[r] = std::sqrt(bn[r]);
+        }
+        rel = 1.;
+        for (int outer = 0; outer < 20; outer++) {
+            int it = 0;
+            if ((rc = gmres_core(ctx, low_op, d_r, d_d, n_rhs, tin, max_iter, it, est, low)))
+                return rc;
+            iters += it;
+            axpy_kernel<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(1., d_d, d_x, m);
+            KCHECK_LAUNCH();
+            if ((rc = apply_op(ctx, hi_op, d_x, d_r, n_rhs)))
+                return rc;
+            fp64++;
+            residual_kernel<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(d_b, d_r, m);
+            KCHECK_LAUNCH();
+            KC(cudaMemcpyAsync(hb.data(), d_r, m * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+            KC(cudaStreamSynchronize(ctx->stream));
+            rel = 0.;
+            for (int r = 0; r < n_rhs; r++) {
+                double s = 0.;
+                for (int i = 0; i < n; i++)
+                    s += hb[(size_t) r * n + i] * hb[(size_t) r * n + i];
+                rel = std::max(rel, bn[r] > 0. ? std::sqrt(s) / bn[r] : 0.);
+            }
+            st.outer = outer + 1;
+            if (rel <= rel_tol || it == 0)
+                break;
+        }
+    }
+    t.stop();
+    st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    st.iterations = iters;
+    st.fp64_matvecs = fp64;
+    st.low_matvecs = low;
+    st.rel_residual = rel;
+    st.rel_residual_estimate = est;
+    if (stats)
+        *stats = st;
+    if ((rc = check_finite(ctx, d_x, m, "solution")))
+        return rc;
+    KC(cudaMemcpyAsync(x, d_x, m * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (n_rhs == 1) {
+        KC(cudaMemcpyAsync(ctx->d_sigma, d_x, (size_t) n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+        ctx->have_sigma = true;
+    }
+    KC(cudaStreamSynchronize(ctx->stream));
+    if (rel > rel_tol)
+        return fail(ctx, KEMCU_ENOTCONVERGED, "GMRES stopped at relative residual %.3e > %.3e after %d iterations", rel,
+                    rel_tol, iters);
+    return KEMCU_OK;
+}
+
+int kemcu_rule_nodes(int which, double* out)
+{
+    if (which < 0 || which > 7 || !out)
+        return KEMCU_EINVAL;
+    std::vector<double> rules(kNumNodes * 3), gl(20);
+    tables::build(rules.data(), gl.data());
+    if (which >= 6) {
+        const int off = which == 6 ? 0 : 2, half = which == 6 ? 2 : 8;
+        for (int i = 0; i < half; i++) {
+            out[3 * i] = gl[2 * (off + i)];
+            out[3 * i + 1] = gl[2 * (off + i) + 1];
+            out[3 * i + 2] = 0.;
+        }
+        return half;
+    }
+    const int offs[7] = {kTri7, kTri12, kTri33, kRect7, kRect12, kRect33, kNumNodes};
+    const int n = offs[which + 1] - offs[which];
+    std::memcpy(out, rules.data() + 3 * offs[which], (size_t) n * 3 * sizeof(double));
+    return n;
+}
+
+}  // extern "C"
+
+#include "kemcu_track_host.inc"
+#include "kemcu_adjoint_host.inc"

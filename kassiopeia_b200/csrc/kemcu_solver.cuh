@@ -1,0 +1,139 @@
+// Krylov-vector kernels for the device GMRES (K6): batched inner products with a fixed-order
+// in-kernel final reduction, Gram-Schmidt updates and basis combinations. Every kernel takes
+// the right-hand-side index from blockIdx.y so all RHS of a multi-RHS solve share launches.
+//
+// Basis layout: V[k][r][i] (k = Krylov index, r = RHS, i = element), i.e. each Krylov column
+// V[k] is one contiguous [nrhs][n] block, the layout the matvec kernels take as x.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace kemcu
+{
+
+constexpr int kDotThreads = 256;
+constexpr int kDotBlocks = 64;  // chunks per vector; partials are summed by the last block
+
+__device__ __forceinline__ double block_sum(double v, double* sh)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_down_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0)
+        sh[w] = v;
+    __syncthreads();
+    v = 0.;
+    if (threadIdx.x < (blockDim.x >> 5))
+        v = sh[threadIdx.x];
+    if (w == 0)
+        for (int o = 16; o > 0; o >>= 1)
+            v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;  // valid in thread 0
+}
+
+// h[r][k0 + k] = sum_i V[k0 + k][r][i] * w[r][i] for k < nk (nk <= 64 per launch); h row stride hs.
+// grid (kDotBlocks, nrhs); partial[r][k][blk]; counter[r] must start at 0 and is reset.
+__global__ void __launch_bounds__(kDotThreads) multi_dot_kernel(const double* __restrict__ V, const double* __restrict__ w,
+                                                                int n, int nrhs, int k0, int nk, double* __restrict__ partial,
+                                                                unsigned* __restrict__ counter, double* __restrict__ h, int hs)
+{
+    __shared__ double sh[32];
+    __shared__ bool last;
+    const int r = blockIdx.y;
+    const int per = (n + gridDim.x - 1) / gridDim.x;
+    const int i0 = blockIdx.x * per, i1 = min(n, i0 + per);
+    const double* wr = w + (size_t) r * n;
+    for (int k = 0; k < nk; k++) {
+        const double* vk = V + ((size_t) (k0 + k) * nrhs + r) * n;
+        double s = 0.;
+        for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x)
+            s += vk[i] * wr[i];
+        s = block_sum(s, sh);
+        if (threadIdx.x == 0)
+            partial[((size_t) r * 64 + k) * gridDim.x + blockIdx.x] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0)
+        last = atomicAdd(counter + r, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last)
+        return;
+    __threadfence();
+    for (int k = threadIdx.x; k < nk; k += blockDim.x) {
+        double s = 0.;
+        for (int b = 0; b < (int) gridDim.x; b++)
+            s += __ldcg(partial + ((size_t) r * 64 + k) * gridDim.x + b);
+        h[(size_t) r * hs + k0 + k] = s;
+    }
+    if (threadIdx.x == 0)
+        counter[r] = 0u;
+}
+
+// w[r][i] -= sum_{k < nk} h[r][k0 + k] V[k0 + k][r][i];   grid (ceil(n/256), nrhs)
+__global__ void gs_update_kernel(const double* __restrict__ V, double* __restrict__ w, int n, int nrhs, int k0, int nk,
+                                 const double* __restrict__ h, int hs, const int* __restrict__ active)
+{
+    const int r = blockIdx.y;
+    if (active && !active[r])
+        return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    double s = 0.;
+    for (int k = 0; k < nk; k++)
+        s += h[(size_t) r * hs + k0 + k] * V[((size_t) (k0 + k) * nrhs + r) * n + i];
+    w[(size_t) r * n + i] -= s;
+}
+
+// dst[r][i] = src[r][i] * scale[r] (scale given as 1 / norm); grid (ceil(n/256), nrhs)
+__global__ void scale_kernel(const double* __restrict__ src, double* __restrict__ dst, int n, const double* __restrict__ nrm,
+                             int nrm_stride, int nrm_index)
+{
+    const int r = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const double v = nrm[(size_t) r * nrm_stride + nrm_index];
+    dst[(size_t) r * n + i] = v > 0. ? src[(size_t) r * n + i] * (1. / sqrt(v)) : 0.;
+}
+
+// x[r][i] += sum_k y[r][k] V[k][r][i];   grid (ceil(n/256), nrhs)
+__global__ void combine_kernel(const double* __restrict__ V, const double* __restrict__ y, int ystride, int n, int nrhs,
+                               const int* __restrict__ nk, double* __restrict__ x)
+{
+    const int r = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    double s = 0.;
+    for (int k = 0; k < nk[r]; k++)
+        s += y[(size_t) r * ystride + k] * V[((size_t) k * nrhs + r) * n + i];
+    x[(size_t) r * n + i] += s;
+}
+
+// r = b - r (in place on r), used for residuals r = b - A x
+__global__ void residual_kernel(const double* __restrict__ b, double* __restrict__ r, size_t n)
+{
+    const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        r[i] = b[i] - r[i];
+}
+
+__global__ void axpy_kernel(double a, const double* __restrict__ x, double* __restrict__ y, size_t n)
+{
+    const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        y[i] += a * x[i];
+}
+
+// non-finite check: flag[0] |= 1 when any value is NaN or Inf
+__global__ void finite_kernel(const double* __restrict__ v, size_t n, int* __restrict__ flag)
+{
+    const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && !isfinite(v[i]))
+        atomicOr(flag, 1);
+}
+
+}  // namespace kemcu

@@ -1,0 +1,215 @@
+"""Generate the golden fixtures in this directory from the reference's own FP64 CPU code.
+
+    make -C oracle ref          # builds oracle/_ref/libkemref.so from the reference tree
+    python tests/golden/make_golden.py
+
+Every array is produced by unmodified reference classes driven through oracle/ref_harness.cc
+(KSurfaceContainer + KEBIFactory::MakeNumeric() + KIntegratingFieldSolver /
+KBoundaryIntegralMatrix / KSimpleIterativeKrylovSolver<double, KGeneralizedMinimalResidual> /
+KSMathRK8). Inputs are seeded; the seeds are fixed below.
+
+Fixtures:
+  rules          nodes and weights of the six cubature rules on canonical elements
+  integrators    the IntegratorsTest.cc rectangle and triangle (UnitTest/KEMField/Fields/src/
+                 IntegratorsTest.cc:28-60, 106-135) with their evaluation points (corner, on
+                 surface, centroid, in-plane far, on side line, arbitrary) plus seeded near
+                 points, vertices and edge midpoints: per-element normalised field and potential
+  lines          wires: near (analytic, inside and outside the wire), 16-node and 4-node bands
+  icosphere_L2   320-triangle sphere at 1 V: GMRES sigma (rel. tol 1e-12), field at shell and
+                 near-surface points, capacitance
+  mixed_small    triangles (Dirichlet), rectangles (Neumann, flux 0.4) and wires (Dirichlet):
+                 full boundary-integral matrix, right-hand side, GMRES solution
+  coax_small     reduced coax (960 rectangles + 288 cap triangles): sigma and gap field
+  rk8            4 electrons x 40 RK8 steps of 1e-11 s in the icosphere_L2 field
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from kassiopeia_b200 import geometry as G  # noqa: E402
+from oracle import ref  # noqa: E402
+
+
+def save(name, **arrays):
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
+    print(f"{name}: " + ", ".join(f"{k}{list(np.shape(v))}" for k, v in arrays.items()))
+
+
+def mesh_arrays(m, prefix=""):
+    return {prefix + "shape": m.shape, prefix + "boundary": m.boundary, prefix + "geom": m.geom,
+            prefix + "value": m.value}
+
+
+def rules():
+    out = {}
+    for i, name in enumerate(["tri7", "tri12", "tri33", "rect7", "rect12", "rect33"]):
+        buf = np.zeros((33, 3))
+        n = ref.lib().kemref_rule_nodes(i, buf.ctypes.data_as(ref._dp))
+        out[name] = buf[:n].copy()
+    save("rules", **out)
+
+
+def integrators():
+    rng = np.random.default_rng(11)
+    rect = G.rectangles_from_corners([-2., -2., 0.], [2., -2., 0.], [-2., 2., 0.], 10.)
+    tri = G.triangles_from_vertices([-1.75, 0.25, 0.], [1.75, 0.25, 0.], [0., 2.25, 0.], 10.)
+    rect_pts = [[-2., -2., 0.], [0.1, -1.5, 0.], [0., 0., 0.], [10., 10., 0.], [0., -2., 0.], [10., -20.5, 33.58],
+                [-1., -1., 0.]]
+    tri_pts = [[-1.75, 0.25, 0.], [0.01, 0.5, 0.], list(tri.centroids()[0]), [10., 1., 0.], [0., 0.25, 0.],
+               [10., -20.5, 33.58]]
+    extra_r = [[2., 2., 0.], [2., 0., 0.], [-2., 0.5, 0.], [0., 0., 1e-3], [0., 0., -0.7], [3., 1., 0.2],
+               [-2., -2., 0.5], [2.5, 2.5, 0.], [0.3, 0.4, 1e-9]]
+    extra_t = [[1.75, 0.25, 0.], [0., 2.25, 0.], [0.875, 1.25, 0.], [-0.875, 1.25, 0.], [0., 1., 0.5],
+               [0., 1., -2e-3], [3., 3., 1.], [0.2, 0.9, 1e-10]]
+    near_r = rng.uniform(-6, 6, size=(40, 3)) * np.array([1, 1, 0.5])
+    near_t = rng.uniform(-4, 4, size=(40, 3)) * np.array([1, 1, 0.5]) + np.array([0, 1, 0])
+    far = rng.normal(size=(20, 3))
+    far /= np.linalg.norm(far, axis=1)[:, None]
+    far_r = far * rng.uniform(20, 1500, size=(20, 1))
+    far_t = far * rng.uniform(15, 900, size=(20, 1))
+    P_r = np.concatenate([rect_pts, extra_r, near_r, far_r])
+    P_t = np.concatenate([tri_pts, extra_t, near_t, far_t])
+    pr = ref.RefProblem(rect)
+    pt = ref.RefProblem(tri)
+    save("integrators", rect_points=P_r, rect_field=pr.element_field(0, P_r), tri_points=P_t,
+         tri_field=pt.element_field(0, P_t), **mesh_arrays(rect, "rect_"), **mesh_arrays(tri, "tri_"))
+
+
+def lines():
+    rng = np.random.default_rng(12)
+    p0 = np.array([[0., 0., 0.], [0.3, 0.1, -0.2], [1., 1., 1.]])
+    p1 = np.array([[1., 0., 0.], [0.3, 0.6, 0.4], [1.2, 0.9, 1.5]])
+    diam = 2e-3
+    m = G.line_segments(p0, p1, diam, 5.0)
+    pts = [[0.5, 0.0005, 0.], [0.5, 0.002, 0.], [0.5, 0., 0.], [-0.0005, 0.0002, 0.], [1.0003, 0., 0.0001],
+           [0.5, 0.3, 0.], [2., 1., 1.], [40., 3., 2.], [0.3, 0.35, 0.1 + 1e-4]]
+    pts = np.concatenate([np.array(pts), rng.uniform(-1.5, 2.5, size=(30, 3)),
+                          rng.normal(size=(10, 3)) * rng.uniform(5, 80, size=(10, 1))])
+    p = ref.RefProblem(m)
+    fields = np.stack([p.element_field(k, pts) for k in range(m.n)])
+    save("lines", points=pts, element_field=fields, **mesh_arrays(m))
+
+
+def icosphere():
+    m = G.icosphere(2)
+    p = ref.RefProblem(m)
+    x, it, r = p.gmres(1e-12)
+    # the reference GMRES's SVD least-squares step (kfm_matrix_svd) is not accurate enough here:
+    # its sigma has a true relative residual ~2e-5 although its implicit estimate reads ~6e-14;
+    # the direct solution of the reference's own matrix is kept alongside as the solve oracle
+    A = p.matrix()
+    b = p.rhs()
+    xd = np.linalg.solve(A, b)
+    pts = np.concatenate([G.shell_points(64, seed=3), G.shell_points(16, 1.005, 1.1, seed=4)])
+    p.set_sigma(x)
+    f = p.field(pts)
+    cap = float((x * m.areas()).sum() * ref.constant("one_over_four_pi_eps0"))
+    save("icosphere_L2", sigma=x, sigma_direct=xd, gmres_true_residual=np.array(np.linalg.norm(b - A @ x) / np.linalg.norm(b)),
+         iterations=np.array(it), residual=np.array(r), points=pts, field=f,
+         capacitance=np.array(cap), **mesh_arrays(m))
+
+
+def mixed_small():
+    rng = np.random.default_rng(13)
+    # a bent triangle strip (Dirichlet), a Neumann rectangle patch, and two wires
+    v = np.array([[0, 0, 0], [0.2, 0, 0.02], [0, 0.2, 0.01], [0.2, 0.2, 0.05], [0.4, 0.05, 0.0], [0.4, 0.25, 0.04]],
+                 float)
+    tri = G.triangles_from_vertices(v[[0, 1, 3, 1]], v[[1, 3, 1, 4]], v[[2, 2, 4, 5]], 1.0)
+    tri.value[:] = [1.0, 1.0, 0.5, 0.5]
+    ro = np.array([[0., 0., 0.3], [0.15, 0., 0.3], [0., 0.12, 0.3], [0.15, 0.12, 0.3]])
+    rect = G.rectangles_from_corners(ro, ro + [0.15, 0, 0.], ro + [0., 0.12, 0.], 0.4, boundary=G.NEUMANN)
+    wire = G.line_segments([[-0.1, 0., 0.1], [-0.1, 0.1, 0.1]], [[-0.1, 0.1, 0.1], [-0.1, 0.2, 0.12]], 3e-3, -0.5)
+    m = tri.concat(rect).concat(wire)
+    p = ref.RefProblem(m)
+    A = p.matrix()
+    b = p.rhs()
+    x, it, r = p.gmres(1e-12)
+    xv = rng.normal(size=m.n)
+    save("mixed_small", A=A, b=b, x=x, x_direct=np.linalg.solve(A, b), xv=xv, Axv=p.matvec(xv), **mesh_arrays(m))
+
+
+def coax_small():
+    m = G.coax(n_phi=24, n_z=20, n_cap_rings=3)
+    p = ref.RefProblem(m)
+    x, it, r = p.gmres(1e-10)
+    A = p.matrix()
+    b = p.rhs()
+    pts = G.gap_points(200, seed=21)
+    p.set_sigma(x)
+    f = p.field(pts)
+    save("coax_small", sigma=x, sigma_direct=np.linalg.solve(A, b),
+         gmres_true_residual=np.array(np.linalg.norm(b - A @ x) / np.linalg.norm(b)), iterations=np.array(it),
+         points=pts, field=f, **mesh_arrays(m))
+
+
+def rk8():
+    fx = dict(np.load(os.path.join(HERE, "icosphere_L2.npz")))
+    from oracle.golden import mesh_from
+    m = mesh_from(fx)
+    p = ref.RefProblem(m)
+    p.set_sigma(fx["sigma"] * 1e4)  # scale the charge so the 1-18.6 keV tracks bend visibly
+    st0 = G.electrons(4, seed=5)
+    trajs = []
+    for k in range(4):
+        _, n, tr = p.rk8_track(st0[k], 1e-11, 40, record=True)
+        trajs.append(tr)
+    save("rk8", state0=st0, traj=np.stack(trajs), sigma_scale=np.array(1e4), dt=np.array(1e-11),
+         charge=np.array(-ref.constant("q")), mass=np.array(ref.constant("m_el")))
+
+
+def adjoint():
+    """icosphere L2 with sigma = solved sigma * (1 + 0.1 N(0,1)), 32 shell probes, seeded
+    weights w on (E, phi); L = sum_p w_p . out_p. dL/dsigma from the per-element fields, and
+    central differences (h = 1e-6 m) of L over the defining vertices of six elements."""
+    fx = dict(np.load(os.path.join(HERE, "icosphere_L2.npz")))
+    from oracle.golden import mesh_from
+    m = mesh_from(fx)
+    rng = np.random.default_rng(41)
+    sigma = fx["sigma"] * (1.0 + 0.1 * rng.normal(size=m.n))
+    P = G.shell_points(32, seed=42)
+    w = rng.normal(size=(32, 4))
+    w[:, :3] *= 1e-1  # E is ~10x phi here; keep both parts of L comparable
+    p = ref.RefProblem(m)
+    dsig = np.array([np.sum(w * p.element_field(k, P)) for k in range(m.n)])
+    elems = np.array([0, 7, 55, 120, 211, 319])
+    h = 1e-6
+    verts = np.zeros((m.n, 3, 3))
+    g = m.geom
+    verts[:, 0] = g[:, 2:5]
+    verts[:, 1] = g[:, 2:5] + g[:, 0:1] * g[:, 5:8]
+    verts[:, 2] = g[:, 2:5] + g[:, 1:2] * g[:, 8:11]
+
+    def L_of(vv):
+        mm = G.triangles_from_vertices(vv[:, 0], vv[:, 1], vv[:, 2], 1.0)
+        q = ref.RefProblem(mm)
+        q.set_sigma(sigma)
+        return float(np.sum(w * q.field(P)))
+
+    fd = np.zeros((len(elems), 9))
+    for a, j in enumerate(elems):
+        for c in range(9):
+            vp, vm = verts.copy(), verts.copy()
+            vp[j, c // 3, c % 3] += h
+            vm[j, c // 3, c % 3] -= h
+            fd[a, c] = (L_of(vp) - L_of(vm)) / (2 * h)
+    save("adjoint", sigma=sigma, points=P, w=w, dsigma=dsig, elems=elems, dvert_fd=fd, h=np.array(h),
+         vertices=verts, **mesh_arrays(m))
+
+
+if __name__ == "__main__":
+    rules()
+    integrators()
+    lines()
+    icosphere()
+    mixed_small()
+    coax_small()
+    rk8()
+    adjoint()

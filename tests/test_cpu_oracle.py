@@ -1,0 +1,51 @@
+"""CPU checks of the oracle itself: the golden fixtures are reproduced by the reference build
+(when it is present) and satisfy the reference's own known answers."""
+
+import numpy as np
+import pytest
+
+from kassiopeia_b200 import geometry as G
+from oracle import golden, ref
+
+needs_ref = pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built (reference tree absent)")
+
+
+def test_sphere_capacitance_known_answer():
+    # SphereCapacitanceTest.cc:110-133: C = sum sigma_i A_i / (4 pi eps0 R) = 1 within 5e-2
+    fx = golden.load("icosphere_L2")
+    assert abs(float(fx["capacitance"]) - 1.0) < 5e-2
+    # the discretisation bound of the analytic 1/r potential outside the sphere
+    r = np.linalg.norm(fx["points"], axis=1)
+    far = r > 1.2
+    assert np.max(np.abs(fx["field"][far, 3] * r[far] - 1.0)) < 3e-2
+
+
+def test_integrators_cross_agreement_shape():
+    # IntegratorsTest.cc checks RWG vs analytic to 2.5 %; the fixture holds the numeric
+    # policy's values, which must be finite at every special point (corners, edges, plane)
+    fx = golden.load("integrators")
+    assert np.all(np.isfinite(fx["rect_field"])) and np.all(np.isfinite(fx["tri_field"]))
+
+
+@needs_ref
+def test_reference_reproduces_fixtures():
+    fx = golden.load("icosphere_L2")
+    p = ref.RefProblem(golden.mesh_from(fx))
+    p.set_sigma(fx["sigma"])
+    np.testing.assert_array_equal(p.field(fx["points"][:10]), fx["field"][:10])
+    mx = golden.load("mixed_small")
+    q = ref.RefProblem(golden.mesh_from(mx))
+    np.testing.assert_array_equal(q.matrix(), mx["A"])
+
+
+@needs_ref
+def test_reference_container_order_is_grouped_by_type():
+    # KSurfaceContainer groups elements by (boundary, shape) type in first-seen order;
+    # the harness maps caller order <-> container order explicitly
+    mx = golden.load("mixed_small")
+    m = golden.mesh_from(mx)
+    perm = np.r_[m.n - 1, 0:m.n - 1]  # put a wire first
+    m2 = G.Mesh(m.shape[perm], m.boundary[perm], m.geom[perm], m.value[perm])
+    q = ref.RefProblem(m2)
+    A2 = q.matrix()
+    np.testing.assert_allclose(A2, mx["A"][np.ix_(perm, perm)], rtol=1e-15, atol=0)

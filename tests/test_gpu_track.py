@@ -1,0 +1,91 @@
+"""GPU parity of the persistent RK8 tracker against the reference's own KSMathRK8 driven by the
+reference field solver (golden fixture rk8: 4 electrons x 40 steps of 1e-11 s)."""
+
+import numpy as np
+import pytest
+
+import kassiopeia_b200 as K
+from kassiopeia_b200 import geometry as G
+from oracle import golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = K.CUDAElectrostaticContext(0)
+    fx = golden.load("icosphere_L2")
+    rk = golden.load("rk8")
+    c.SetGeometry(golden.mesh_from(fx))
+    c.SetSigma(fx["sigma"] * float(rk["sigma_scale"]))
+    yield c
+    c.close()
+
+
+def _run_steps(ctx, rk, precision):
+    st = rk["state0"].copy()
+    steps = np.zeros(4, np.int32)
+    status = np.zeros(4, np.int32)
+    traj = []
+    for k in range(rk["traj"].shape[1]):
+        st, steps, status, _ = ctx.TrackRK8(st, float(rk["dt"]), 10000, steps=steps, status=status, step_budget=1,
+                                            charge=float(rk["charge"]), mass=float(rk["mass"]), precision=precision)
+        traj.append(st.copy())
+    return np.stack(traj, axis=1), steps, status
+
+
+def test_rk8_steps_match_reference(ctx):
+    rk = golden.load("rk8")
+    traj, steps, status = _run_steps(ctx, rk, K.FP64)
+    ref = rk["traj"]
+    assert np.all(steps == ref.shape[1]) and np.all(status == K._native.TRACK_ACTIVE)
+    x_err = np.max(np.abs(traj[..., 2:5] - ref[..., 2:5])) / np.max(np.abs(ref[..., 2:5]))
+    p_err = np.max(np.abs(traj[..., 5:8] - ref[..., 5:8])) / np.max(np.abs(ref[..., 5:8]))
+    t_err = np.max(np.abs(traj[..., 0:2] - ref[..., 0:2]) / np.abs(ref[..., 0:2]))
+    assert x_err < 1e-12 and p_err < 1e-12 and t_err < 1e-13, (x_err, p_err, t_err)
+    # the field must actually bend the tracks for this to mean anything
+    dp = np.abs(ref[:, -1, 5:8] - rk["state0"][:, 5:8]).max() / np.abs(rk["state0"][:, 5:8]).max()
+    assert dp > 1e-6
+
+
+def test_rk8_mixed_within_tolerance(ctx):
+    rk = golden.load("rk8")
+    traj, _, _ = _run_steps(ctx, rk, K.MIXED)
+    ref = rk["traj"]
+    x_err = np.max(np.abs(traj[..., 2:5] - ref[..., 2:5])) / np.max(np.abs(ref[..., 2:5]))
+    p_err = np.max(np.abs(traj[..., 5:8] - ref[..., 5:8])) / np.max(np.abs(ref[..., 5:8]))
+    assert x_err < 1e-9 and p_err < 1e-9, (x_err, p_err)
+
+
+def test_multi_step_launch_equals_single_steps(ctx):
+    rk = golden.load("rk8")
+    st, steps, status, stats = ctx.TrackRK8(rk["state0"], float(rk["dt"]), 10000, step_budget=40,
+                                            charge=float(rk["charge"]), mass=float(rk["mass"]))
+    np.testing.assert_allclose(st, rk["traj"][:, -1], rtol=1e-12, atol=0)
+    assert stats["steps"] == 160 and stats["field_evals"] == 13 * 160
+
+
+def test_uneven_tracks_terminate_with_status(ctx):
+    # tracks aimed at the sphere hit it, others leave a 3.2 m volume or run out of steps;
+    # the work queue keeps slots busy while their lengths differ
+    n = 600
+    st = G.electrons(n, r_min=1.2, r_max=1.5, seed=17)
+    x = st[:, 2:5]
+    inward = -x / np.linalg.norm(x, axis=1)[:, None]
+    half = n // 2
+    pmag = np.linalg.norm(st[:, 5:8], axis=1)
+    st[:half, 5:8] = pmag[:half, None] * inward[:half]
+    out, steps, status, stats = ctx.TrackRK8(st, 1e-10, 400, sphere_radius=1.0, max_radius=3.2)
+    T = K._native
+    assert set(np.unique(status)) <= {T.TRACK_HIT, T.TRACK_LEFT, T.TRACK_MAX_STEPS}
+    assert np.all(status[:half] == T.TRACK_HIT)
+    r_end = np.linalg.norm(out[:, 2:5], axis=1)
+    assert np.all(r_end[status == T.TRACK_HIT] <= 1.0)
+    assert np.all(r_end[status == T.TRACK_LEFT] >= 3.2)
+    assert np.all(steps[status == T.TRACK_MAX_STEPS] == 400)
+    assert stats["steps"] == int(steps.sum())
+    assert len(np.unique(steps)) > 10  # genuinely uneven lengths
+    # an already finished set is left untouched
+    out2, steps2, status2, stats2 = ctx.TrackRK8(out, 1e-10, 400, steps=steps, status=status, sphere_radius=1.0,
+                                                 max_radius=3.2)
+    assert stats2["steps"] == 0 and np.array_equal(out2, out)
