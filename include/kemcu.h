@@ -167,6 +167,15 @@ int kemcu_field_vjp(kemcu_ctx* ctx, const double* P, size_t n, const double* w, 
    (KElectrostaticQuadratureLineSegmentIntegrator.hh:47-80).
    out: up to 33 x 3 (s, t, w); returns the node count or KEMCU_EINVAL. */
 int kemcu_rule_nodes(int which, double* out);
+/* number of this library's own kernel launches on the context since it was created */
+unsigned long long kemcu_launch_count(const kemcu_ctx* ctx);
+/* quadrature-band histogram over all (element, point) pairs for points P (n x 3):
+   counts[shape * 4 + band], band 0 = analytic (RWG / analytic wire), 1 = 33-point / 16-node,
+   2 = 12-point / 4-node, 3 = 7-point; the algorithmic work of a field evaluation */
+int kemcu_band_histogram(kemcu_ctx* ctx, const double* P, size_t n, long long* counts12);
+/* measured FMA throughput of the context's device, FP64 and FP32 CUDA-core pipes (TFLOP/s,
+   2 flops per FMA), from independent dependent-FMA chains */
+int kemcu_fma_peak(kemcu_ctx* ctx, double* fp64_tflops, double* fp32_tflops);
 
 #ifdef __cplusplus
 }

@@ -59,7 +59,7 @@ _lib = None
 def header_symbols() -> list[str]:
     """Every function the C header declares (the ABI surface the library must export)."""
     txt = open(HEADER).read()
-    decl = r"^\s*(?:int|void|double|size_t|const\s+char\s*\*)\s*(kemcu_[a-z0-9_]+)\s*\("
+    decl = r"^\s*(?:int|void|double|size_t|unsigned\s+long\s+long|const\s+char\s*\*)\s*(kemcu_[a-z0-9_]+)\s*\("
     return sorted(set(re.findall(decl, txt, flags=re.M)))
 
 
@@ -97,5 +97,9 @@ def lib():
                                   C.c_double, C.POINTER(HitModel), C.c_int, C.POINTER(TrackStats)]
     L.kemcu_field_vjp.argtypes = [vp, _dp, C.c_size_t, _dp, _dp, _dp, C.c_int]
     L.kemcu_rule_nodes.argtypes = [C.c_int, _dp]
+    L.kemcu_launch_count.argtypes = [vp]
+    L.kemcu_launch_count.restype = C.c_ulonglong
+    L.kemcu_band_histogram.argtypes = [vp, _dp, C.c_size_t, C.POINTER(C.c_longlong)]
+    L.kemcu_fma_peak.argtypes = [vp, _dp, _dp]
     _lib = L
     return L

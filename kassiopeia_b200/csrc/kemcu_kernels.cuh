@@ -369,3 +369,51 @@ __global__ void scatter_out_kernel(const double* __restrict__ src, const int* __
     dst[4 * (size_t) j + 3] = src[4 * (size_t) i + 3];
 }
 }  // namespace kemcu
+
+namespace kemcu
+{
+// ------------------------------------------------------------------------- diagnostics
+// band histogram over all (element, point) pairs: counts[shape * 4 + band]
+__global__ void band_histogram_kernel(const double* __restrict__ rec, int n_elem, const double* __restrict__ pts,
+                                      int n_pts, unsigned long long* __restrict__ counts)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned c[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (p < n_pts) {
+        const V3 P = v3(pts[3 * p], pts[3 * p + 1], pts[3 * p + 2]);
+        for (int j = 0; j < n_elem; j++) {
+            const double* e = rec + (size_t) j * rRecSize;
+            c[(int) e[rType] * 4 + band_of(e, P)]++;
+        }
+    }
+    for (int k = 0; k < 12; k++) {
+        unsigned v = c[k];
+        for (int o = 16; o > 0; o >>= 1)
+            v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0 && v)
+            atomicAdd(counts + k, (unsigned long long) v);
+    }
+}
+
+// FMA throughput probe: kProbeChains independent dependent chains per thread
+constexpr int kProbeChains = 8;
+template<typename T> __global__ void fma_probe_kernel(T* __restrict__ sink, int iters)
+{
+    T a[kProbeChains];
+    const T x = (T) 0.999999, y = (T) 1e-7;
+#pragma unroll
+    for (int k = 0; k < kProbeChains; k++)
+        a[k] = (T) (threadIdx.x + k);
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < kProbeChains; k++)
+            a[k] = fma(a[k], x, y);
+    }
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < kProbeChains; k++)
+        s += a[k];
+    if (s == (T) -1)  // never true; keeps the chains alive
+        sink[threadIdx.x] = s;
+}
+}  // namespace kemcu

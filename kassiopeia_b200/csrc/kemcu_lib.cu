@@ -61,6 +61,7 @@ struct kemcu_ctx
     int* d_flag = nullptr;
     kemcu_iteration_callback cb = nullptr;
     void* cb_user = nullptr;
+    unsigned long long launches = 0;
 };
 
 namespace
@@ -98,7 +99,12 @@ int fail(kemcu_ctx* c, int code, const char* fmt, ...)
                         __LINE__);                                                                      \
     } while (0)
 
-#define KCHECK_LAUNCH() KC(cudaGetLastError())
+// every launch of this library's own kernels is followed by KCHECK_LAUNCH, which also counts it
+#define KCHECK_LAUNCH()      \
+    do {                     \
+        ctx->launches++;     \
+        KC(cudaGetLastError()); \
+    } while (0)
 
 int ensure(kemcu_ctx* ctx, int slot, size_t bytes, void** out)
 {
@@ -996,6 +1002,66 @@ int kemcu_gmres(kemcu_ctx* ctx, const double* b, double* x, int n_rhs, double re
     if (rel > rel_tol)
         return fail(ctx, KEMCU_ENOTCONVERGED, "GMRES stopped at relative residual %.3e > %.3e after %d iterations", rel,
                     rel_tol, iters);
+    return KEMCU_OK;
+}
+
+unsigned long long kemcu_launch_count(const kemcu_ctx* ctx)
+{
+    return ctx ? ctx->launches : 0ULL;
+}
+
+int kemcu_band_histogram(kemcu_ctx* ctx, const double* P, size_t n, long long* counts)
+{
+    int rc = check_ready(ctx, false);
+    if (rc)
+        return rc;
+    if (!P || !counts || n == 0 || n > (size_t) 0x7fffffff)
+        return fail(ctx, KEMCU_EINVAL, "invalid histogram arguments");
+    KC(cudaSetDevice(ctx->device));
+    void *dp, *dc;
+    if ((rc = ensure(ctx, sPts, n * 3 * sizeof(double), &dp)) || (rc = ensure(ctx, sOut, 12 * sizeof(long long), &dc)))
+        return rc;
+    KC(cudaMemcpyAsync(dp, P, n * 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    KC(cudaMemsetAsync(dc, 0, 12 * sizeof(long long), ctx->stream));
+    band_histogram_kernel<<<(unsigned) ((n + 127) / 128), 128, 0, ctx->stream>>>(ctx->d_rec, (int) ctx->n,
+                                                                               (const double*) dp, (int) n,
+                                                                               (unsigned long long*) dc);
+    KCHECK_LAUNCH();
+    KC(cudaMemcpyAsync(counts, dc, 12 * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+    KC(cudaStreamSynchronize(ctx->stream));
+    return KEMCU_OK;
+}
+
+int kemcu_fma_peak(kemcu_ctx* ctx, double* fp64_tflops, double* fp32_tflops)
+{
+    if (!ctx || !ctx->stream)
+        return ctx ? fail(ctx, KEMCU_ESTATE, "context has no device") : KEMCU_EINVAL;
+    KC(cudaSetDevice(ctx->device));
+    void* d;
+    int rc;
+    if ((rc = ensure(ctx, sMisc, 1 << 22, &d)))
+        return rc;
+    const int blocks = ctx->num_sms * 8, threads = 256, iters = 4096;
+    for (int pass = 0; pass < 2; pass++) {
+        for (int rep = 0; rep < 2; rep++) {  // first repetition warms up
+            cudaEventRecord(ctx->ev0, ctx->stream);
+            if (pass == 0)
+                fma_probe_kernel<double><<<blocks, threads, 0, ctx->stream>>>((double*) d, iters);
+            else
+                fma_probe_kernel<float><<<blocks, threads, 0, ctx->stream>>>((float*) d, iters);
+            KCHECK_LAUNCH();
+            cudaEventRecord(ctx->ev1, ctx->stream);
+            KC(cudaEventSynchronize(ctx->ev1));
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        const double flops = 2.0 * kProbeChains * (double) iters * blocks * threads;
+        const double tf = flops / (ms * 1e-3) / 1e12;
+        if (pass == 0 && fp64_tflops)
+            *fp64_tflops = tf;
+        if (pass == 1 && fp32_tflops)
+            *fp32_tflops = tf;
+    }
     return KEMCU_OK;
 }
 

@@ -11,10 +11,11 @@
 // Layout: a CTA owns kTrackSlots slots (one per thread). All slots of a CTA advance in lock
 // step, stage by stage, so every stage's 128 field evaluations share one pass of the element
 // records through shared memory. The 13 stage derivatives of each slot live in shared memory.
-// A slot whose track ends (electrode hit, leaving the volume, step limit, non-finite state)
-// writes it back and takes the next track index from a global work counter, so tracks of very
-// different lengths keep every slot busy; a launch runs at most `budget` steps per slot, after
-// which unfinished tracks are written back as still active for the next launch.
+// A slot whose track ends (electrode hit, leaving the volume, step limit, non-finite state) or
+// has taken `budget` steps in this launch writes it back and takes the next track index from a
+// global work counter, so tracks of very different lengths keep every slot busy and one launch
+// advances every listed track by at most `budget` steps; unfinished tracks stay active for the
+// next launch.
 #pragma once
 
 #include "kemcu_kernels.cuh"
@@ -82,11 +83,12 @@ __global__ void __launch_bounds__(kTrackSlots) rk8_tracker_kernel(const double* 
     const int tid = threadIdx.x;
     auto K = [&](int st, int c) -> double& { return s_k[(st * 7 + c) * kTrackSlots + tid]; };
 
-    int track = -1;
+    int track = -1, tsteps = 0;
     double y[8];
     int nstep = 0;
-    // grab the first track
-    {
+    auto pull = [&]() {
+        track = -1;
+        tsteps = 0;
         const unsigned w = atomicAdd(next, 1u);
         if (w < (unsigned) prm.n_list) {
             track = list[w];
@@ -94,11 +96,11 @@ __global__ void __launch_bounds__(kTrackSlots) rk8_tracker_kernel(const double* 
                 y[c] = state[(size_t) track * 8 + c];
             nstep = steps[track];
         }
-    }
+    };
+    pull();
     unsigned long long my_steps = 0;
-    for (int it = 0; it < prm.budget; it++) {
-        if (!__syncthreads_or(track >= 0))
-            break;
+    // every iteration is one RK8 step of all busy slots; ends when the list is exhausted
+    while (__syncthreads_or(track >= 0)) {
         for (int st = 0; st < kStages; st++) {
             // stage position and momentum: value_{st-1} = y0 + dt sum_k a[st-1][k] k_k
             V3 X = v3(y[2], y[3], y[4]), Pm = v3(y[5], y[6], y[7]);
@@ -177,26 +179,16 @@ __global__ void __launch_bounds__(kTrackSlots) rk8_tracker_kernel(const double* 
                 stat = 3;
             else if (nstep >= prm.max_steps)
                 stat = 2;
-            if (stat != 0) {
+            tsteps++;
+            if (stat != 0 || tsteps >= prm.budget) {
                 for (int c = 0; c < 8; c++)
                     state[(size_t) track * 8 + c] = y[c];
                 steps[track] = nstep;
-                status[track] = stat;
-                track = -1;
-                const unsigned w = atomicAdd(next, 1u);
-                if (w < (unsigned) prm.n_list) {
-                    track = list[w];
-                    for (int c = 0; c < 8; c++)
-                        y[c] = state[(size_t) track * 8 + c];
-                    nstep = steps[track];
-                }
+                if (stat != 0)
+                    status[track] = stat;
+                pull();
             }
         }
-    }
-    if (track >= 0) {
-        for (int c = 0; c < 8; c++)
-            state[(size_t) track * 8 + c] = y[c];
-        steps[track] = nstep;
     }
     atomicAdd(done_steps, my_steps);
 }

@@ -29,6 +29,7 @@
 #include "KElectrostaticBoundaryIntegratorFactory.hh"
 #include "KElectrostaticCubatureRectangleIntegrator.hh"
 #include "KElectrostaticCubatureTriangleIntegrator.hh"
+#include "KElectrostaticQuadratureLineSegmentIntegrator.hh"
 #include "KElectrostaticIntegratingFieldSolver.hh"
 #include "KGeneralizedMinimalResidual.hh"
 #include "KRobinHood.hh"
@@ -358,6 +359,17 @@ extern "C" int kemref_rule_nodes(int which, double* out)
     double Q[99];
     const double* w = nullptr;
     int n = 0;
+    if (which == 6 || which == 7) {  // Gauss-Legendre half rules (x, w, 0) of the line segments
+        const double* x = which == 6 ? gQuadx4 : gQuadx16;
+        const double* wq = which == 6 ? gQuadw4 : gQuadw16;
+        n = which == 6 ? 2 : 8;
+        for (int k = 0; k < n; k++) {
+            out[3 * k] = x[k];
+            out[3 * k + 1] = wq[k];
+            out[3 * k + 2] = 0.;
+        }
+        return n;
+    }
     switch (which) {
         case 0:
             KElectrostaticCubatureTriangleIntegrator::GaussPoints_Tri7P(data, Q);

@@ -49,3 +49,58 @@ def test_reference_container_order_is_grouped_by_type():
     q = ref.RefProblem(m2)
     A2 = q.matrix()
     np.testing.assert_allclose(A2, mx["A"][np.ix_(perm, perm)], rtol=1e-15, atol=0)
+
+
+# ---------------------------------------------------------------- the C restatement, pinned
+from oracle import port  # noqa: E402
+
+needs_port = pytest.mark.skipif(not port.available(), reason="oracle/libkemoracle.so not built")
+
+
+@needs_port
+@pytest.mark.parametrize("shape", ["rect", "tri"])
+def test_port_single_element_special_points(shape):
+    fx = golden.load("integrators")
+    p = port.PortProblem(golden.mesh_from(fx, shape + "_"))
+    out = p.element_field(0, fx[shape + "_points"])
+    ref_ = fx[shape + "_field"]
+    assert np.max(np.abs(out - ref_) / np.max(np.abs(ref_), axis=0)) < 1e-11
+
+
+@needs_port
+def test_port_lines():
+    fx = golden.load("lines")
+    m = golden.mesh_from(fx)
+    p = port.PortProblem(m)
+    for k in range(m.n):
+        ref_ = fx["element_field"][k]
+        ok = np.all(np.isfinite(ref_), axis=1) & (np.abs(ref_).max(axis=1) < 1e15)
+        out = p.element_field(k, fx["points"][ok])
+        assert np.max(np.abs(out - ref_[ok]) / np.max(np.abs(ref_[ok]), axis=0)) < 1e-12
+
+
+@needs_port
+def test_port_field_matrix_and_solve():
+    fx = golden.load("icosphere_L2")
+    p = port.PortProblem(golden.mesh_from(fx))
+    p.set_sigma(fx["sigma"])
+    out = p.field(fx["points"])
+    assert np.max(np.abs(out - fx["field"]) / np.abs(fx["field"]).max(axis=0)) < 1e-13
+    mx = golden.load("mixed_small")
+    q = port.PortProblem(golden.mesh_from(mx))
+    A, b = q.matrix()
+    assert np.max(np.abs(A - mx["A"]) / np.abs(mx["A"]).max(axis=1, keepdims=True)) < 1e-13
+    np.testing.assert_array_equal(b, mx["b"])
+    x, it, r = q.gmres(1e-13)
+    assert np.max(np.abs(x - mx["x_direct"])) / np.max(np.abs(mx["x_direct"])) < 1e-10
+
+
+@needs_port
+def test_port_rk8():
+    fx = golden.load("icosphere_L2")
+    rk = golden.load("rk8")
+    p = port.PortProblem(golden.mesh_from(fx))
+    p.set_sigma(fx["sigma"] * float(rk["sigma_scale"]))
+    st, traj = p.rk8_track(rk["state0"][0], float(rk["dt"]), 10, float(rk["charge"]), float(rk["mass"]))
+    ref_ = rk["traj"][0, :10]
+    assert np.max(np.abs(traj[:, 2:8] - ref_[:, 2:8]) / np.abs(ref_[:, 2:8]).max(axis=0)) < 1e-12
