@@ -1,0 +1,256 @@
+// kemfield_cuda.hh -- C++ adaptors that plug the B200 backend (include/kemcu.h) into KEMField
+// beside its CPU and OpenCL backends, against the reference's unchanged interfaces:
+//
+//   KCUDASurfaceContainer        flattens a KSurfaceContainer in container order (the matrix
+//                                order, KSurfaceContainer.cc:58-72) onto the device and writes
+//                                charge densities back into each KElectrostaticBasis, like
+//                                KOpenCLSurfaceContainer (KOpenCLSurfaceContainer.cc:10-266)
+//   KCUDAIntegratingFieldSolver  Potential / ElectricField / ElectricFieldAndPotential of
+//                                KIntegratingFieldSolver (KElectrostaticIntegratingFieldSolver.hh:261-339),
+//                                plus a batched ElectricFieldAndPotential over many points
+//   KCUDABoundaryIntegralMatrix  a KSquareMatrix whose virtual Multiply (KMatrix.hh:87-99) and
+//                                operator()(i, j) (KBoundaryIntegralMatrix.hh:31-55) run on the GPU
+//   KCUDAChargeDensitySolver     the whole GMRES charge-density solve on the device
+//                                (KSimpleIterativeKrylovSolver<double, KGeneralizedMinimalResidual>)
+//
+// Header-only; include after the reference's KEMField headers and link with -lkemcu. Errors
+// surface as KEMSimpleException, as elsewhere in KEMField.
+#pragma once
+
+#include "KElectrostaticBasis.hh"
+#include "KEMConstants.hh"
+#include "KEMSimpleException.hh"
+#include "KSquareMatrix.hh"
+#include "KSurfaceContainer.hh"
+#include "KSurfaceTypes.hh"
+#include "kemcu.h"
+
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace KEMField
+{
+
+class ElectrostaticCUDA;  // backend Kind tag, next to ElectrostaticSingleThread / ElectrostaticOpenCL
+
+inline void KCUDACheck(kemcu_ctx* ctx, int rc)
+{
+    if (rc != KEMCU_OK)
+        throw KEMSimpleException(std::string("kemcu: ") + kemcu_last_error(ctx));
+}
+
+class KCUDASurfaceContainer
+{
+  public:
+    explicit KCUDASurfaceContainer(KSurfaceContainer& container, int device = 0) : fContainer(container)
+    {
+        kemcu_config cfg;
+        kemcu_default_config(&cfg);
+        cfg.device = device;
+        cfg.one_over_four_pi_eps0 = KEMConstants::OneOverFourPiEps0;
+        cfg.eps0 = KEMConstants::Eps0;
+        const int rc = kemcu_create(&fCtx, &cfg);
+        if (rc != KEMCU_OK) {
+            const std::string msg = fCtx ? kemcu_last_error(fCtx) : "context creation failed";
+            kemcu_destroy(fCtx);
+            throw KEMSimpleException("kemcu: " + msg);
+        }
+        Flatten();
+    }
+    ~KCUDASurfaceContainer()
+    {
+        kemcu_destroy(fCtx);
+    }
+    KCUDASurfaceContainer(const KCUDASurfaceContainer&) = delete;
+    KCUDASurfaceContainer& operator=(const KCUDASurfaceContainer&) = delete;
+
+    kemcu_ctx* Context() const
+    {
+        return fCtx;
+    }
+    unsigned int size() const
+    {
+        return fContainer.size();
+    }
+
+    // sigma from each KElectrostaticBasis onto the device
+    void WriteBasisData()
+    {
+        std::vector<double> s(size());
+        for (unsigned i = 0; i < size(); i++)
+            s[i] = Basis(i)->GetSolution();
+        KCUDACheck(fCtx, kemcu_set_sigma(fCtx, s.data()));
+    }
+    // device sigma back into each KElectrostaticBasis (KOpenCLSurfaceContainer::ReadBasisData)
+    void ReadBasisData()
+    {
+        std::vector<double> s(size());
+        KCUDACheck(fCtx, kemcu_get_sigma(fCtx, s.data()));
+        for (unsigned i = 0; i < size(); i++)
+            Basis(i)->GetSolution() = s[i];
+    }
+
+  private:
+    KElectrostaticBasis* Basis(unsigned i) const
+    {
+        auto* b = dynamic_cast<KElectrostaticBasis*>(fContainer[i]->GetBasis());
+        if (!b)
+            throw KEMSimpleException("kemcu: element without an electrostatic basis");
+        return b;
+    }
+
+    void Flatten()
+    {
+        const unsigned n = size();
+        std::vector<int32_t> shape(n), boundary(n);
+        std::vector<double> geom(11 * (size_t) n, 0.), value(n);
+        for (unsigned i = 0; i < n; i++) {
+            KSurfacePrimitive* s = fContainer[i];
+            double* g = &geom[11 * (size_t) i];
+            if (auto* t = dynamic_cast<KTriangle*>(s->GetShape())) {
+                shape[i] = KEMCU_TRIANGLE;
+                Planar(*t, g);
+            }
+            else if (auto* r = dynamic_cast<KRectangle*>(s->GetShape())) {
+                shape[i] = KEMCU_RECTANGLE;
+                Planar(*r, g);
+            }
+            else if (auto* l = dynamic_cast<KLineSegment*>(s->GetShape())) {
+                shape[i] = KEMCU_LINE_SEGMENT;
+                for (int c = 0; c < 3; c++) {
+                    g[c] = l->GetP0()[c];
+                    g[3 + c] = l->GetP1()[c];
+                }
+                g[6] = l->GetDiameter();
+            }
+            else
+                throw KEMSimpleException("kemcu: only triangles, rectangles and line segments are supported");
+            if (auto* d = dynamic_cast<KBoundaryType<KElectrostaticBasis, KDirichletBoundary>*>(s->GetBoundary())) {
+                boundary[i] = KEMCU_DIRICHLET;
+                value[i] = d->GetBoundaryValue();
+            }
+            else if (auto* nb = dynamic_cast<KBoundaryType<KElectrostaticBasis, KNeumannBoundary>*>(s->GetBoundary())) {
+                boundary[i] = KEMCU_NEUMANN;
+                value[i] = nb->GetNormalBoundaryFlux();
+            }
+            else
+                throw KEMSimpleException("kemcu: unsupported boundary type");
+        }
+        KCUDACheck(fCtx, kemcu_set_geometry(fCtx, n, shape.data(), boundary.data(), geom.data(), value.data()));
+    }
+
+    template<class S> static void Planar(const S& s, double* g)
+    {
+        g[0] = s.GetA();
+        g[1] = s.GetB();
+        for (int c = 0; c < 3; c++) {
+            g[2 + c] = s.GetP0()[c];
+            g[5 + c] = s.GetN1()[c];
+            g[8 + c] = s.GetN2()[c];
+        }
+    }
+
+    KSurfaceContainer& fContainer;
+    kemcu_ctx* fCtx = nullptr;
+};
+
+class KCUDAIntegratingFieldSolver
+{
+  public:
+    explicit KCUDAIntegratingFieldSolver(KCUDASurfaceContainer& container, int precision = KEMCU_FP64) :
+        fContainer(container),
+        fPrecision(precision)
+    {}
+    double Potential(const KPosition& P) const
+    {
+        double o[4];
+        Eval(&P[0], 1, o, KEMCU_POTENTIAL);
+        return o[3];
+    }
+    KFieldVector ElectricField(const KPosition& P) const
+    {
+        double o[4];
+        Eval(&P[0], 1, o, KEMCU_FIELD);
+        return KFieldVector(o[0], o[1], o[2]);
+    }
+    std::pair<KFieldVector, double> ElectricFieldAndPotential(const KPosition& P) const
+    {
+        double o[4];
+        Eval(&P[0], 1, o, KEMCU_FIELD_AND_POTENTIAL);
+        return std::make_pair(KFieldVector(o[0], o[1], o[2]), o[3]);
+    }
+    // batched extension: P n x 3, out n x 4 (Ex, Ey, Ez, phi)
+    void ElectricFieldAndPotential(const double* P, size_t n, double* out) const
+    {
+        Eval(P, n, out, KEMCU_FIELD_AND_POTENTIAL);
+    }
+
+  private:
+    void Eval(const double* P, size_t n, double* out, int what) const
+    {
+        KCUDACheck(fContainer.Context(), kemcu_field(fContainer.Context(), P, n, out, fPrecision, what));
+    }
+    KCUDASurfaceContainer& fContainer;
+    int fPrecision;
+};
+
+class KCUDABoundaryIntegralMatrix : public KSquareMatrix<double>
+{
+  public:
+    explicit KCUDABoundaryIntegralMatrix(KCUDASurfaceContainer& container, bool assembled = false) :
+        fContainer(container),
+        fAssembled(assembled)
+    {}
+    unsigned int Dimension() const override
+    {
+        return fContainer.size();
+    }
+    const double& operator()(unsigned int i, unsigned int j) const override
+    {
+        KCUDACheck(fContainer.Context(), kemcu_matrix_element(fContainer.Context(), i, j, &fEntry));
+        return fEntry;
+    }
+    void Multiply(const KVector<double>& x, KVector<double>& y) const override
+    {
+        const unsigned n = Dimension();
+        std::vector<double> xs(n), ys(n);
+        for (unsigned i = 0; i < n; i++)
+            xs[i] = x(i);
+        KCUDACheck(fContainer.Context(),
+                   kemcu_matvec(fContainer.Context(), xs.data(), ys.data(), 1, KEMCU_FP64, fAssembled ? 1 : 0));
+        for (unsigned i = 0; i < n; i++)
+            y[i] = ys[i];
+    }
+
+  private:
+    KCUDASurfaceContainer& fContainer;
+    bool fAssembled;
+    mutable double fEntry = 0.;
+};
+
+class KCUDAChargeDensitySolver
+{
+  public:
+    KCUDAChargeDensitySolver(double tolerance = 1e-10, int max_iterations = 500, int mode = KEMCU_SOLVE_PLAIN) :
+        fTolerance(tolerance),
+        fMaxIterations(max_iterations),
+        fMode(mode)
+    {}
+    // solves A sigma = b for the boundary values and writes sigma into the container
+    kemcu_solve_stats Solve(KCUDASurfaceContainer& container) const
+    {
+        std::vector<double> x(container.size());
+        kemcu_solve_stats st{};
+        KCUDACheck(container.Context(),
+                   kemcu_gmres(container.Context(), nullptr, x.data(), 1, fTolerance, fMaxIterations, fMode, &st));
+        container.ReadBasisData();
+        return st;
+    }
+
+  private:
+    double fTolerance;
+    int fMaxIterations, fMode;
+};
+
+}  // namespace KEMField

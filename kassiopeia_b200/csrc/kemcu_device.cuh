@@ -184,15 +184,17 @@ __device__ __forceinline__ double rsqrt_newton(double x)
     return fma(y, h, y);
 }
 
-template<bool POT, bool FIELD, bool FAST = false>
-__device__ __forceinline__ Out4 cub64(const double* e, V3 P, int off, int n)
+// The rule (offset OFF, N nodes) is a compile-time constant: the loop is fully unrolled and
+// every node's (s, t, w) is a constant-bank operand of the FP64 instructions.
+template<int OFF, int N, bool POT, bool FIELD, bool FAST>
+__device__ __forceinline__ Out4 cub64(const double* e, V3 P)
 {
     const V3 d0 = P - ld3(e + rP0);
     const V3 a = ld3(e + rEa), b = ld3(e + rEb);
     double sx = 0., sy = 0., sz = 0., sp = 0.;
-#pragma unroll 4
-    for (int k = 0; k < n; k++) {
-        const double s = c_rules[3 * (off + k)], t = c_rules[3 * (off + k) + 1], w = c_rules[3 * (off + k) + 2];
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        const double s = c_rules[3 * (OFF + k)], t = c_rules[3 * (OFF + k) + 1], w = c_rules[3 * (OFF + k) + 2];
         const double qx = d0.x - s * a.x - t * b.x;
         const double qy = d0.y - s * a.y - t * b.y;
         const double qz = d0.z - s * a.z - t * b.z;
@@ -222,9 +224,10 @@ __device__ __forceinline__ Out4 cub64(const double* e, V3 P, int off, int n)
 // The large terms W/R and W d/R^3 are FP64; f and g are formed in FP32 without
 // cancellation (absolute error ~1e-7 |f|), so the per-element relative error is about
 // 1e-7 |o|/R: ~2e-8 at the inner edge of the 33-point band, < 3e-9 beyond the 12-point cut.
-template<bool POT, bool FIELD>
-__device__ __forceinline__ Out4 cub_mixed(const double* e, V3 P, int off, int n)
+template<int OFF, int N, bool POT, bool FIELD>
+__device__ __forceinline__ Out4 cub_mixed(const double* e, V3 P)
 {
+    constexpr int off = OFF, n = N;
     const V3 d = P - ld3(e + rCen);
     const double R2 = dot(d, d);
     const double iR = rsqrt(R2);
@@ -235,7 +238,7 @@ __device__ __forceinline__ Out4 cub_mixed(const double* e, V3 P, int off, int n)
     const float ax = (float) e[rEa], ay = (float) e[rEa + 1], az = (float) e[rEa + 2];
     const float bx = (float) e[rEb], by = (float) e[rEb + 1], bz = (float) e[rEb + 2];
     float sf = 0.f, sg = 0.f, sox = 0.f, soy = 0.f, soz = 0.f;
-#pragma unroll 4
+#pragma unroll
     for (int k = 0; k < n; k++) {
         const float4 r = *reinterpret_cast<const float4*>(&c_rules_f[4 * (off + k)]);
         const float ox = r.x * ax + r.y * bx, oy = r.x * ay + r.y * by, oz = r.x * az + r.y * bz;
@@ -572,16 +575,22 @@ template<bool MIXED, bool POT, bool FIELD> __device__ __forceinline__ Out4 epi(c
     }
     if (band == 0)
         return type == kTriangle ? rwg64<3, POT, FIELD>(e, P) : rwg64<4, POT, FIELD>(e, P);
-    int n;
-    const int off = rule_offset(type, band, n);
-    if (MIXED) {
-        // 33-point band: FP64 nodes with the Newton reciprocal square root; 12- and 7-point
-        // bands (|o|/R < 0.02): FP64 centroid term + FP32 node correction
+    // MIXED: 33-point band as FP64 nodes with the Newton reciprocal square root; 12- and
+    // 7-point bands (|o|/R < 0.02) as FP64 centroid term + FP32 node correction
+    if (type == kTriangle) {
         if (band == 1)
-            return cub64<POT, FIELD, true>(e, P, off, n);
-        return cub_mixed<POT, FIELD>(e, P, off, n);
+            return cub64<kTri33, 33, POT, FIELD, MIXED>(e, P);
+        if constexpr (MIXED)
+            return band == 2 ? cub_mixed<kTri12, 12, POT, FIELD>(e, P) : cub_mixed<kTri7, 7, POT, FIELD>(e, P);
+        else
+            return band == 2 ? cub64<kTri12, 12, POT, FIELD, false>(e, P) : cub64<kTri7, 7, POT, FIELD, false>(e, P);
     }
-    return cub64<POT, FIELD>(e, P, off, n);
+    if (band == 1)
+        return cub64<kRect33, 33, POT, FIELD, MIXED>(e, P);
+    if constexpr (MIXED)
+        return band == 2 ? cub_mixed<kRect12, 12, POT, FIELD>(e, P) : cub_mixed<kRect7, 7, POT, FIELD>(e, P);
+    else
+        return band == 2 ? cub64<kRect12, 12, POT, FIELD, false>(e, P) : cub64<kRect7, 7, POT, FIELD, false>(e, P);
 }
 
 }  // namespace kemcu

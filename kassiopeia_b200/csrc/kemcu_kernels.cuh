@@ -18,6 +18,11 @@ namespace kemcu
 
 constexpr int kThreads = 128;
 constexpr int kTile = 32;
+// resident CTAs per SM the direct-sum kernels are compiled for (bounds their registers)
+#ifndef KEMCU_MIN_BLOCKS
+#define KEMCU_MIN_BLOCKS 2
+#endif
+constexpr int kMinBlocks = KEMCU_MIN_BLOCKS;
 
 struct Kahan
 {
@@ -44,7 +49,7 @@ __device__ __forceinline__ void load_tile(double* sm, const double* __restrict__
 // K1: field and/or potential at points. out layout per point: (Ex, Ey, Ez, phi).
 // nsplit == gridDim.y; partial != nullptr when nsplit > 1 (then out is untouched).
 template<bool MIXED, bool POT, bool FIELD>
-__global__ void __launch_bounds__(kThreads) field_kernel(const double* __restrict__ rec, const double* __restrict__ sigma,
+__global__ void __launch_bounds__(kThreads, kMinBlocks) field_kernel(const double* __restrict__ rec, const double* __restrict__ sigma,
                                                          int n_elem, const double* __restrict__ pts, int n_pts,
                                                          double* __restrict__ out, double* __restrict__ partial)
 {
@@ -132,7 +137,7 @@ template<bool MIXED> __device__ __forceinline__ double entry(const double* e, co
 // KMatrix.hh:92-99, KBoundaryIntegralMatrix.hh:31-55).
 constexpr int kMaxRhs = 8;
 template<bool MIXED>
-__global__ void __launch_bounds__(kThreads) matvec_kernel(const double* __restrict__ rec, const TargetRec* __restrict__ tgt,
+__global__ void __launch_bounds__(kThreads, kMinBlocks) matvec_kernel(const double* __restrict__ rec, const TargetRec* __restrict__ tgt,
                                                           int n, const double* __restrict__ x, int nrhs,
                                                           double* __restrict__ y, double* __restrict__ partial)
 {
@@ -180,7 +185,7 @@ __global__ void __launch_bounds__(kThreads) matvec_kernel(const double* __restri
 // operator assembly: column-major dense A (A[j * n + i] = A(i, j)) for columns [j0, j1),
 // written in FP64 and, when a32 != nullptr, also rounded to FP32
 template<bool MIXED>
-__global__ void __launch_bounds__(kThreads) assemble_kernel(const double* __restrict__ rec, const TargetRec* __restrict__ tgt,
+__global__ void __launch_bounds__(kThreads, kMinBlocks) assemble_kernel(const double* __restrict__ rec, const TargetRec* __restrict__ tgt,
                                                             int n, int j0, int j1, double* __restrict__ a64,
                                                             float* __restrict__ a32)
 {

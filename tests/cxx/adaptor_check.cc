@@ -1,0 +1,138 @@
+// Drop-in check of include/kemfield_cuda.hh against the reference's unchanged KEMField classes:
+// the same KSurfaceContainer is solved on the GPU through KCUDAChargeDensitySolver, then the
+// reference's CPU KIntegratingFieldSolver / KBoundaryIntegralMatrix and the CUDA adaptors are
+// evaluated side by side; the reference's own GMRES driver also runs on the CUDA matrix.
+// Exit status 0 when every comparison is within tolerance.
+#include "KBoundaryIntegralMatrix.hh"
+#include "KBoundaryIntegralSolutionVector.hh"
+#include "KBoundaryIntegralVector.hh"
+#include "KElectrostaticBoundaryIntegratorFactory.hh"
+#include "KElectrostaticIntegratingFieldSolver.hh"
+#include "KGeneralizedMinimalResidual.hh"
+#include "KSimpleIterativeKrylovSolver.hh"
+#include "KSurface.hh"
+#include "KSurfaceContainer.hh"
+#include "kemfield_cuda.hh"
+
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <map>
+#include <vector>
+
+using namespace KEMField;
+using V = std::array<double, 3>;
+
+static V unit(V a)
+{
+    const double r = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    return {a[0] / r, a[1] / r, a[2] / r};
+}
+
+static void icosphere(int level, KSurfaceContainer& c)
+{
+    const double t = (1. + std::sqrt(5.)) / 2.;
+    std::vector<V> v = {{-1, t, 0}, {1, t, 0}, {-1, -t, 0}, {1, -t, 0}, {0, -1, t}, {0, 1, t},
+                        {0, -1, -t}, {0, 1, -t}, {t, 0, -1}, {t, 0, 1}, {-t, 0, -1}, {-t, 0, 1}};
+    for (auto& x : v)
+        x = unit(x);
+    std::vector<std::array<int, 3>> f = {{0, 11, 5}, {0, 5, 1}, {0, 1, 7}, {0, 7, 10}, {0, 10, 11}, {1, 5, 9}, {5, 11, 4},
+                                         {11, 10, 2}, {10, 7, 6}, {7, 1, 8}, {3, 9, 4}, {3, 4, 2}, {3, 2, 6}, {3, 6, 8},
+                                         {3, 8, 9}, {4, 9, 5}, {2, 4, 11}, {6, 2, 10}, {8, 6, 7}, {9, 8, 1}};
+    for (int s = 0; s < level; s++) {
+        std::map<std::pair<int, int>, int> mid;
+        std::vector<std::array<int, 3>> g;
+        auto M = [&](int a, int b) {
+            auto k = std::make_pair(std::min(a, b), std::max(a, b));
+            auto it = mid.find(k);
+            if (it != mid.end())
+                return it->second;
+            v.push_back(unit({v[a][0] + v[b][0], v[a][1] + v[b][1], v[a][2] + v[b][2]}));
+            return mid[k] = (int) v.size() - 1;
+        };
+        for (auto& q : f) {
+            const int a = M(q[0], q[1]), b = M(q[1], q[2]), d = M(q[2], q[0]);
+            g.push_back({q[0], a, d});
+            g.push_back({q[1], b, a});
+            g.push_back({q[2], d, b});
+            g.push_back({a, b, d});
+        }
+        f = g;
+    }
+    for (auto& q : f) {
+        auto* T = new KSurface<KElectrostaticBasis, KDirichletBoundary, KTriangle>();
+        T->SetValues(KPosition(v[q[0]][0], v[q[0]][1], v[q[0]][2]), KPosition(v[q[1]][0], v[q[1]][1], v[q[1]][2]),
+                     KPosition(v[q[2]][0], v[q[2]][1], v[q[2]][2]));
+        T->SetBoundaryValue(1.);
+        c.push_back(T);
+    }
+}
+
+int main()
+{
+    KSurfaceContainer container;
+    icosphere(2, container);
+    KElectrostaticBoundaryIntegrator integrator = KEBIFactory::MakeNumeric();
+    int failures = 0;
+    try {
+        KCUDASurfaceContainer gpu(container);
+        kemcu_solve_stats st = KCUDAChargeDensitySolver(1e-12, 200, KEMCU_SOLVE_PLAIN).Solve(gpu);
+        std::printf("gpu solve: %d iterations, relative residual %.3e\n", st.iterations, st.rel_residual);
+
+        // field: reference CPU direct sum vs the CUDA field solver on the same sigma
+        KIntegratingFieldSolver<KElectrostaticBoundaryIntegrator> cpu(container, integrator);
+        KCUDAIntegratingFieldSolver cuda(gpu);
+        double worst = 0.;
+        for (int i = 0; i < 24; i++) {
+            const double r = 1.05 + 0.08 * i, th = 0.7 * i, ph = 1.3 * i;
+            KPosition P(r * std::sin(th) * std::cos(ph), r * std::sin(th) * std::sin(ph), r * std::cos(th));
+            auto a = cpu.ElectricFieldAndPotential(P);
+            auto b = cuda.ElectricFieldAndPotential(P);
+            worst = std::max(worst, std::fabs(a.second - b.second) / std::fabs(a.second));
+            worst = std::max(worst, (a.first - b.first).Magnitude() / a.first.Magnitude());
+        }
+        std::printf("field: max relative difference CPU vs CUDA %.3e\n", worst);
+        failures += !(worst < 1e-12);
+
+        // matrix entries and the virtual Multiply
+        KBoundaryIntegralMatrix<KElectrostaticBoundaryIntegrator> Aref(container, integrator);
+        KCUDABoundaryIntegralMatrix Acuda(gpu);
+        double wm = 0.;
+        for (unsigned k = 0; k < 40; k++) {
+            const unsigned i = (k * 37) % Aref.Dimension(), j = (k * 91 + 5) % Aref.Dimension();
+            wm = std::max(wm, std::fabs(Aref(i, j) - Acuda(i, j)) / std::fabs(Aref(i, i)));
+        }
+        std::printf("matrix entries: max relative difference %.3e\n", wm);
+        failures += !(wm < 1e-12);
+        KSimpleVector<double> x(Aref.Dimension()), y1(Aref.Dimension()), y2(Aref.Dimension());
+        for (unsigned i = 0; i < x.Dimension(); i++)
+            x[i] = std::sin(0.1 * i);
+        Aref.Multiply(x, y1);
+        Acuda.Multiply(x, y2);
+        double wy = 0., ny = 0.;
+        for (unsigned i = 0; i < x.Dimension(); i++) {
+            wy = std::max(wy, std::fabs(y1(i) - y2(i)));
+            ny = std::max(ny, std::fabs(y1(i)));
+        }
+        std::printf("Multiply: max relative difference %.3e\n", wy / ny);
+        failures += !(wy / ny < 1e-12);
+
+        // the reference's own GMRES driver on the CUDA matrix (drop-in behind KMatrix::Multiply)
+        KBoundaryIntegralVector<KElectrostaticBoundaryIntegrator> b(container, integrator);
+        KSimpleVector<double> xs(Aref.Dimension());
+        for (unsigned i = 0; i < xs.Dimension(); i++)
+            xs[i] = 0.;
+        KSimpleIterativeKrylovSolver<double, KGeneralizedMinimalResidual> S;
+        S.SetTolerance(1e-10);
+        S.Solve(Acuda, xs, b);
+        std::printf("reference GMRES on the CUDA matrix: %u iterations, estimate %.3e\n", S.GetIteration(),
+                    S.ResidualNorm());
+        failures += !(S.ResidualNorm() < 1e-10);
+    }
+    catch (std::exception& e) {
+        std::printf("exception: %s\n", e.what());
+        return 2;
+    }
+    std::printf("%s\n", failures ? "FAILED" : "OK");
+    return failures ? 1 : 0;
+}

@@ -76,3 +76,16 @@ def test_gauss_legendre_rules():
 def test_invalid_rule_index():
     out = np.zeros((33, 3))
     assert N.lib().kemcu_rule_nodes(8, out.ctypes.data_as(C.POINTER(C.c_double))) == N.EINVAL
+
+
+def test_kemfield_adaptor_builds_against_reference():
+    """include/kemfield_cuda.hh compiles against the reference's unchanged KEMField headers and
+    links with the reference's objects and libkemcu (the drop-in the integration notes describe)."""
+    import os
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if not os.path.isdir(os.path.join(root, "oracle", "_ref", "obj")):
+        pytest.skip("the reference's objects were not built here (make -C oracle ref)")
+    r = subprocess.run(["make", "-s", "-C", os.path.join(root, "oracle"), "adaptor"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert os.path.exists(os.path.join(root, "oracle", "_ref", "adaptor_check"))
