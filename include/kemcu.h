@@ -121,6 +121,21 @@ int kemcu_field(kemcu_ctx* ctx, const double* P, size_t n, double* out4, int pre
 /* same with device pointers, ordered on the context stream, synchronous on return */
 int kemcu_field_dev(kemcu_ctx* ctx, const double* dP, size_t n, double* dout4, int precision, int what);
 
+/* ---- direct summation that allocates no device memory (no counterpart in the reference) ----
+   For callers that cannot call cudaMalloc while they evaluate fields: a host framework that has
+   given all device memory to its own pool allocator, or a loop that must not incur the implicit
+   device synchronisation a cudaMalloc / cudaFree can cause while other work runs on the GPU.
+   Same result as kemcu_field_dev (points evaluated in the caller's order, not re-sorted). The
+   element-split partial sums live in one file-scope device array of
+   KEMCU_NOALLOC_SCRATCH_BYTES (8 MiB, held by every GPU that loads the library until the
+   process exits); its device address is looked up once per context in kemcu_create. n may be
+   at most KEMCU_NOALLOC_MAX_POINTS; larger n returns KEMCU_EINVAL. All calls share the array,
+   so calls that overlap on the GPU (several contexts or threads on one device at once) race;
+   calls in sequence do not, every call overwrites the part it reads. */
+#define KEMCU_NOALLOC_SCRATCH_BYTES (8u << 20)
+#define KEMCU_NOALLOC_MAX_POINTS (KEMCU_NOALLOC_SCRATCH_BYTES / 32u)
+int kemcu_field_dev_noalloc(kemcu_ctx* ctx, const double* dP, size_t n, double* dout4, int precision, int what);
+
 /* ---- boundary-integral matrix (KBoundaryIntegralMatrix, KBoundaryIntegralMatrix.hh:16-99) ---- */
 /* single entry A(i, j) = BoundaryIntegral(source j, target i) (KBoundaryIntegralMatrix.hh:31-55) */
 int kemcu_matrix_element(kemcu_ctx* ctx, size_t i, size_t j, double* a);

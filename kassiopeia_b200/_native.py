@@ -88,6 +88,7 @@ def lib():
     L.kemcu_rhs.argtypes = [vp, _dp]
     L.kemcu_field.argtypes = [vp, _dp, C.c_size_t, _dp, C.c_int, C.c_int]
     L.kemcu_field_dev.argtypes = [vp, C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.c_int]
+    L.kemcu_field_dev_noalloc.argtypes = [vp, C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.c_int]
     L.kemcu_matrix_element.argtypes = [vp, C.c_size_t, C.c_size_t, _dp]
     L.kemcu_matvec.argtypes = [vp, _dp, _dp, C.c_int, C.c_int, C.c_int]
     L.kemcu_gmres.argtypes = [vp, _dp, _dp, C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(SolveStats)]

@@ -25,6 +25,11 @@
 
 using namespace kemcu;
 
+// Scratch of kemcu_field_dev_noalloc: a fixed device array instead of cudaMalloc'd memory. In
+// host code this name is only a host-side stand-in; the device address is obtained with
+// cudaGetSymbolAddress in kemcu_create (kemcu_ctx::noalloc_scratch).
+static __device__ __align__(256) double g_noalloc_scratch[KEMCU_NOALLOC_SCRATCH_BYTES / sizeof(double)];
+
 // ------------------------------------------------------------------------------- context
 struct DevBuf
 {
@@ -59,6 +64,7 @@ struct kemcu_ctx
     DevBuf scratch[9];
     unsigned* d_counter = nullptr;
     int* d_flag = nullptr;
+    double* noalloc_scratch = nullptr;  // device address of g_noalloc_scratch on this context's device
     kemcu_iteration_callback cb = nullptr;
     void* cb_user = nullptr;
     unsigned long long launches = 0;
@@ -618,6 +624,9 @@ int kemcu_create(kemcu_ctx** out, const kemcu_config* cfg)
     KC(cudaMalloc(&ctx->d_counter, 64 * sizeof(unsigned)));
     KC(cudaMemset(ctx->d_counter, 0, 64 * sizeof(unsigned)));
     KC(cudaMalloc(&ctx->d_flag, sizeof(int)));
+    // set-up of kemcu_field_dev_noalloc: the static scratch array's device address on this
+    // device (host code may not use the symbol itself as a device pointer)
+    KC(cudaGetSymbolAddress((void**) &ctx->noalloc_scratch, g_noalloc_scratch));
     // rule tables
     std::vector<double> rules(kNumNodes * 3), gl(20), wsum(kNumNodes, 0.);
     std::vector<float> rf(kNumNodes * 4, 0.f);
@@ -813,6 +822,61 @@ int kemcu_field_dev(kemcu_ctx* ctx, const double* dP, size_t n, double* dout4, i
         if ((rc = launch_field(ctx, ps, n, os, precision, what)))
             return rc;
         scatter_out_kernel<<<(unsigned) ((n + 255) / 256), 256, 0, ctx->stream>>>(os, i1, (int) n, dout4);
+        KCHECK_LAUNCH();
+    }
+    t.stop();
+    return check_finite(ctx, dout4, n * 4, "field result");
+}
+
+// Allocation-free direct sum (declared in kemcu.h): the element-split partial sums go to the
+// file-scope g_noalloc_scratch instead of a grow-only cudaMalloc'd buffer. Every split writes
+// its whole slice before reduce_splits reads it, so nothing needs clearing between calls.
+int kemcu_field_dev_noalloc(kemcu_ctx* ctx, const double* dP, size_t n, double* dout4, int precision, int what)
+{
+    int rc = check_ready(ctx, true);
+    if (rc)
+        return rc;
+    if (n == 0)
+        return KEMCU_OK;
+    if (!dP || !dout4 || (precision != KEMCU_FP64 && precision != KEMCU_MIXED) || what < 0 || what > 2)
+        return fail(ctx, KEMCU_EINVAL, "invalid field arguments");
+    if (n > (size_t) KEMCU_NOALLOC_MAX_POINTS)
+        return fail(ctx, KEMCU_EINVAL, "kemcu_field_dev_noalloc takes at most %u points (got %zu): its scratch is "
+                                       "a fixed %u-byte device array", (unsigned) KEMCU_NOALLOC_MAX_POINTS, n,
+                    (unsigned) KEMCU_NOALLOC_SCRATCH_BYTES);
+    if (!ctx->noalloc_scratch)
+        return fail(ctx, KEMCU_ESTATE, "no-allocation scratch not set up");
+    KC(cudaSetDevice(ctx->device));
+    Timer t(ctx);
+    const size_t cap = KEMCU_NOALLOC_SCRATCH_BYTES / sizeof(double);
+    const int split = (int) std::min((size_t) grid_split(ctx, n, ctx->n), std::max((size_t) 1, cap / (4 * n)));
+    double* partial = split > 1 ? ctx->noalloc_scratch : nullptr;
+    dim3 grid((unsigned) ((n + kThreads - 1) / kThreads), (unsigned) split);
+    const double* sg = ctx->d_sigma;
+    const int ne = (int) ctx->n, np = (int) n;
+    const bool mixed = precision == KEMCU_MIXED;
+    if (what == KEMCU_POTENTIAL) {
+        if (mixed)
+            field_kernel<true, true, false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial);
+        else
+            field_kernel<false, true, false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial);
+    }
+    else if (what == KEMCU_FIELD) {
+        if (mixed)
+            field_kernel<true, false, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial);
+        else
+            field_kernel<false, false, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial);
+    }
+    else {
+        if (mixed)
+            field_kernel<true, true, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial);
+        else
+            field_kernel<false, true, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial);
+    }
+    KCHECK_LAUNCH();
+    if (split > 1) {
+        const size_t m = n * 4;
+        reduce_splits<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(partial, split, m, dout4);
         KCHECK_LAUNCH();
     }
     t.stop();
