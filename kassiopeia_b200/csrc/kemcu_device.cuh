@@ -184,10 +184,10 @@ __device__ __forceinline__ double rsqrt_newton(double x)
     return fma(y, h, y);
 }
 
-// The rule (offset OFF, N nodes) is a compile-time constant: the loop is fully unrolled and
-// every node's (s, t, w) is a constant-bank operand of the FP64 instructions.
-template<int OFF, int N, bool POT, bool FIELD, bool FAST>
-__device__ __forceinline__ Out4 cub64(const double* e, V3 P)
+// The node count N is a compile-time constant, so the loop is fully unrolled; the rule's
+// (s, t, w) triples are read from constant memory at offsets relative to the rule start OFF.
+template<int N, bool POT, bool FIELD, bool FAST>
+__device__ __forceinline__ Out4 cub64(const double* e, V3 P, const int OFF)
 {
     const V3 d0 = P - ld3(e + rP0);
     const V3 a = ld3(e + rEa), b = ld3(e + rEb);
@@ -224,10 +224,10 @@ __device__ __forceinline__ Out4 cub64(const double* e, V3 P)
 // The large terms W/R and W d/R^3 are FP64; f and g are formed in FP32 without
 // cancellation (absolute error ~1e-7 |f|), so the per-element relative error is about
 // 1e-7 |o|/R: ~2e-8 at the inner edge of the 33-point band, < 3e-9 beyond the 12-point cut.
-template<int OFF, int N, bool POT, bool FIELD>
-__device__ __forceinline__ Out4 cub_mixed(const double* e, V3 P)
+template<int N, bool POT, bool FIELD>
+__device__ __forceinline__ Out4 cub_mixed(const double* e, V3 P, const int off)
 {
-    constexpr int off = OFF, n = N;
+    constexpr int n = N;
     const V3 d = P - ld3(e + rCen);
     const double R2 = dot(d, d);
     const double iR = rsqrt(R2);
@@ -577,20 +577,15 @@ template<bool MIXED, bool POT, bool FIELD> __device__ __forceinline__ Out4 epi(c
         return type == kTriangle ? rwg64<3, POT, FIELD>(e, P) : rwg64<4, POT, FIELD>(e, P);
     // MIXED: 33-point band as FP64 nodes with the Newton reciprocal square root; 12- and
     // 7-point bands (|o|/R < 0.02) as FP64 centroid term + FP32 node correction
-    if (type == kTriangle) {
-        if (band == 1)
-            return cub64<kTri33, 33, POT, FIELD, MIXED>(e, P);
-        if constexpr (MIXED)
-            return band == 2 ? cub_mixed<kTri12, 12, POT, FIELD>(e, P) : cub_mixed<kTri7, 7, POT, FIELD>(e, P);
-        else
-            return band == 2 ? cub64<kTri12, 12, POT, FIELD, false>(e, P) : cub64<kTri7, 7, POT, FIELD, false>(e, P);
-    }
+    // one code path for both shapes: rectangle rules sit kRect7 - kTri7 entries after the
+    // triangle rules with the same node counts
+    const int off = type == kTriangle ? 0 : kRect7 - kTri7;
     if (band == 1)
-        return cub64<kRect33, 33, POT, FIELD, MIXED>(e, P);
+        return cub64<33, POT, FIELD, MIXED>(e, P, kTri33 + off);
     if constexpr (MIXED)
-        return band == 2 ? cub_mixed<kRect12, 12, POT, FIELD>(e, P) : cub_mixed<kRect7, 7, POT, FIELD>(e, P);
+        return band == 2 ? cub_mixed<12, POT, FIELD>(e, P, kTri12 + off) : cub_mixed<7, POT, FIELD>(e, P, kTri7 + off);
     else
-        return band == 2 ? cub64<kRect12, 12, POT, FIELD, false>(e, P) : cub64<kRect7, 7, POT, FIELD, false>(e, P);
+        return band == 2 ? cub64<12, POT, FIELD, false>(e, P, kTri12 + off) : cub64<7, POT, FIELD, false>(e, P, kTri7 + off);
 }
 
 }  // namespace kemcu

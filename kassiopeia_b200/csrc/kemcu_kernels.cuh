@@ -17,10 +17,14 @@ namespace kemcu
 {
 
 constexpr int kThreads = 128;
-constexpr int kTile = 32;
+// elements per shared-memory tile (records of 256 B: kTile * 256 B of shared memory)
+#ifndef KEMCU_TILE
+#define KEMCU_TILE 128
+#endif
+constexpr int kTile = KEMCU_TILE;
 // resident CTAs per SM the direct-sum kernels are compiled for (bounds their registers)
 #ifndef KEMCU_MIN_BLOCKS
-#define KEMCU_MIN_BLOCKS 2
+#define KEMCU_MIN_BLOCKS 4
 #endif
 constexpr int kMinBlocks = KEMCU_MIN_BLOCKS;
 

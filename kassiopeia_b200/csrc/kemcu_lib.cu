@@ -230,10 +230,11 @@ void build_record(const double* g, int shape, int boundary, double value, const 
 
 int grid_split(const kemcu_ctx* ctx, size_t n_pts, size_t n_elem)
 {
+    // enough CTAs for four waves of the resident CTAs per SM, each split keeping >= 32 elements
     const size_t blocks = (n_pts + kThreads - 1) / kThreads;
-    const size_t want = (size_t) ctx->num_sms * 8;
+    const size_t want = (size_t) ctx->num_sms * kMinBlocks * 4;
     size_t split = blocks >= want ? 1 : (want + blocks - 1) / blocks;
-    split = std::min(split, std::max((size_t) 1, n_elem / 64));
+    split = std::min(split, std::max((size_t) 1, n_elem / 32));
     split = std::min(split, (size_t) 65535);
     return (int) std::max((size_t) 1, split);
 }
@@ -431,6 +432,9 @@ int assemble(kemcu_ctx* ctx, bool want32)
 // twice (CGS2), which is as accurate as the reference's modified Gram-Schmidt and reads the
 // basis with two batched passes instead of j sequential ones. The j x j triangular solve
 // uses back-substitution (KGeneralizedMinimalResidual::UseBackSubstitution).
+// basis entries (n x (j+1)) up to which one CTA per RHS orthogonalises (arnoldi_small_kernel)
+constexpr size_t kArnoldiSmall = (size_t) 1 << 20;
+
 int gmres_core(kemcu_ctx* ctx, int op, const double* d_b, double* d_x, int nrhs, double tol, int max_iter,
                int& iters, double& est, int& matvecs)
 {
@@ -486,31 +490,46 @@ int gmres_core(kemcu_ctx* ctx, int op, const double* d_b, double* d_x, int nrhs,
         if ((rc = apply_op(ctx, op, vj, w, nrhs)))
             return rc;
         matvecs++;
-        for (int pass = 0; pass < 2; pass++) {
-            double* hh = pass == 0 ? h : h2;
-            for (int k0 = 0; k0 <= j; k0 += 64) {
-                const int nk = std::min(64, j + 1 - k0);
-                multi_dot_kernel<<<dim3(kDotBlocks, nrhs), kDotThreads, 0, ctx->stream>>>(V, w, n, nrhs, k0, nk, part,
-                                                                                         ctx->d_counter, hh, hs);
-                KCHECK_LAUNCH();
-            }
-            for (int k0 = 0; k0 <= j; k0 += 64) {
-                const int nk = std::min(64, j + 1 - k0);
-                gs_update_kernel<<<vg, 256, 0, ctx->stream>>>(V, w, n, nrhs, k0, nk, hh, hs, nullptr);
-                KCHECK_LAUNCH();
+        std::vector<double> b2(nrhs * (size_t) hs);
+        if ((size_t) n * (size_t) (j + 1) <= kArnoldiSmall) {
+            // one CTA per RHS: both Gram-Schmidt passes, the norm and the new basis vector
+            arnoldi_small_kernel<<<nrhs, kArnoldiThreads, 0, ctx->stream>>>(V, w, n, nrhs, j, h, hs);
+            KCHECK_LAUNCH();
+            KC(cudaMemcpyAsync(hcol.data(), h, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+            KC(cudaStreamSynchronize(ctx->stream));
+            for (int r = 0; r < nrhs; r++) {
+                const double beta = hcol[(size_t) r * hs + hs - 1];
+                b2[(size_t) r * hs] = beta * beta;
+                for (int k = 0; k <= j; k++)
+                    hcol2[(size_t) r * hs + k] = 0.;
             }
         }
-        // beta^2 into h2[r][j+1]
-        multi_dot_kernel<<<dim3(kDotBlocks, nrhs), kDotThreads, 0, ctx->stream>>>(w - 0, w, n, nrhs, 0, 1, part, ctx->d_counter,
-                                                                                 yv, hs);
-        KCHECK_LAUNCH();
-        scale_kernel<<<vg, 256, 0, ctx->stream>>>(w, vn, n, yv, hs, 0);
-        KCHECK_LAUNCH();
-        KC(cudaMemcpyAsync(hcol.data(), h, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        KC(cudaMemcpyAsync(hcol2.data(), h2, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        std::vector<double> b2(nrhs * (size_t) hs);
-        KC(cudaMemcpyAsync(b2.data(), yv, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        KC(cudaStreamSynchronize(ctx->stream));
+        else {
+            for (int pass = 0; pass < 2; pass++) {
+                double* hh = pass == 0 ? h : h2;
+                for (int k0 = 0; k0 <= j; k0 += 64) {
+                    const int nk = std::min(64, j + 1 - k0);
+                    multi_dot_kernel<<<dim3(kDotBlocks, nrhs), kDotThreads, 0, ctx->stream>>>(V, w, n, nrhs, k0, nk,
+                                                                                             part, ctx->d_counter, hh, hs);
+                    KCHECK_LAUNCH();
+                }
+                for (int k0 = 0; k0 <= j; k0 += 64) {
+                    const int nk = std::min(64, j + 1 - k0);
+                    gs_update_kernel<<<vg, 256, 0, ctx->stream>>>(V, w, n, nrhs, k0, nk, hh, hs, nullptr);
+                    KCHECK_LAUNCH();
+                }
+            }
+            // beta^2 into yv[r][0]
+            multi_dot_kernel<<<dim3(kDotBlocks, nrhs), kDotThreads, 0, ctx->stream>>>(w, w, n, nrhs, 0, 1, part,
+                                                                                     ctx->d_counter, yv, hs);
+            KCHECK_LAUNCH();
+            scale_kernel<<<vg, 256, 0, ctx->stream>>>(w, vn, n, yv, hs, 0);
+            KCHECK_LAUNCH();
+            KC(cudaMemcpyAsync(hcol.data(), h, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+            KC(cudaMemcpyAsync(hcol2.data(), h2, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+            KC(cudaMemcpyAsync(b2.data(), yv, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+            KC(cudaStreamSynchronize(ctx->stream));
+        }
         iters = j + 1;
         double worst = 0.;
         for (int r = 0; r < nrhs; r++) {

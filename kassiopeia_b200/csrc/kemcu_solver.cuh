@@ -128,6 +128,56 @@ __global__ void axpy_kernel(double a, const double* __restrict__ x, double* __re
         y[i] += a * x[i];
 }
 
+// One Arnoldi step for small systems in a single CTA per right-hand side: w = A v_j is given;
+// modified Gram-Schmidt against V[0..j] (as KGeneralizedMinimalResidual.hh:219-231) applied twice,
+// h[r][0..j] = sum of both passes' projections,
+// beta[r] = |w| written to h[r][hs - 1], and V[j+1] = w / beta. One launch replaces the five of
+// the multi-CTA path when n is small enough for one CTA to stream the basis.
+constexpr int kArnoldiThreads = 1024;
+__global__ void __launch_bounds__(kArnoldiThreads) arnoldi_small_kernel(double* __restrict__ V, double* __restrict__ w,
+                                                                       int n, int nrhs, int j, double* __restrict__ h,
+                                                                       int hs)
+{
+    __shared__ double sh[32];
+    __shared__ double s_h[2];
+    const int r = blockIdx.x;
+    double* wr = w + (size_t) r * n;
+    for (int k = 0; k <= j; k++)
+        if (threadIdx.x == 0)
+            h[(size_t) r * hs + k] = 0.;
+    for (int pass = 0; pass < 2; pass++) {
+        for (int k = 0; k <= j; k++) {
+            const double* vk = V + ((size_t) k * nrhs + r) * n;
+            double s = 0.;
+            for (int i = threadIdx.x; i < n; i += blockDim.x)
+                s += vk[i] * wr[i];
+            s = block_sum(s, sh);
+            if (threadIdx.x == 0) {
+                s_h[0] = s;
+                h[(size_t) r * hs + k] += s;
+            }
+            __syncthreads();
+            const double hk = s_h[0];
+            for (int i = threadIdx.x; i < n; i += blockDim.x)
+                wr[i] -= hk * vk[i];
+            __syncthreads();
+        }
+    }
+    double s = 0.;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        s += wr[i] * wr[i];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) {
+        s_h[1] = sqrt(s);
+        h[(size_t) r * hs + hs - 1] = s_h[1];
+    }
+    __syncthreads();
+    const double beta = s_h[1];
+    double* vn = V + ((size_t) (j + 1) * nrhs + r) * n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        vn[i] = beta > 0. ? wr[i] * (1. / beta) : 0.;
+}
+
 // non-finite check: flag[0] |= 1 when any value is NaN or Inf
 __global__ void finite_kernel(const double* __restrict__ v, size_t n, int* __restrict__ flag)
 {

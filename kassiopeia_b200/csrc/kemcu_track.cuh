@@ -25,6 +25,7 @@ namespace kemcu
 
 constexpr int kTrackSlots = 128;
 constexpr int kStages = 13;
+constexpr int kTrackTile = 32;  // element records per tile (the stage derivatives take most shared memory)
 
 // Butcher coefficients a[s][k] (row s gives stage value s from derivatives 0..s; row 12 is
 // the final combination), the 13-stage eighth-order scheme of KSMathRK8.h:139-226
@@ -77,9 +78,9 @@ __global__ void __launch_bounds__(kTrackSlots) rk8_tracker_kernel(const double* 
                                                                   TrackParams prm)
 {
     extern __shared__ __align__(16) double smem[];
-    double* s_rec = smem;                               // kTile * rRecSize
-    double* s_sig = s_rec + kTile * rRecSize;           // kTile
-    double* s_k = s_sig + kTile;                        // [kStages][7][kTrackSlots]: v(3), F(3), |v|
+    double* s_rec = smem;                               // kTrackTile * rRecSize
+    double* s_sig = s_rec + kTrackTile * rRecSize;      // kTrackTile
+    double* s_k = s_sig + kTrackTile;                        // [kStages][7][kTrackSlots]: v(3), F(3), |v|
     const int tid = threadIdx.x;
     auto K = [&](int st, int c) -> double& { return s_k[(st * 7 + c) * kTrackSlots + tid]; };
 
@@ -120,8 +121,8 @@ __global__ void __launch_bounds__(kTrackSlots) rk8_tracker_kernel(const double* 
             }
             // E(X): lock-step pass of all elements through shared memory
             Kahan ex, ey, ez;
-            for (int t0 = 0; t0 < n_elem; t0 += kTile) {
-                const int cnt = min(kTile, n_elem - t0);
+            for (int t0 = 0; t0 < n_elem; t0 += kTrackTile) {
+                const int cnt = min(kTrackTile, n_elem - t0);
                 __syncthreads();
                 load_tile(s_rec, rec, t0, cnt);
                 if (tid < cnt)
