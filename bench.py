@@ -331,7 +331,7 @@ def main():
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f64+f32 (mixed form: FP64 near field and centroid terms, FP32 far-field node corrections)",
+            "dtype": "f64 (mixed form: FP32-class hardware rsqrt estimate + FP64 Newton step per cubature node; FP64 elsewhere)",
             "data": "synthetic (seeded coax mesh and gap points)",
             "config": {"workload": "coax: 40,000 rectangles + 4,000 cap triangles, 1,000,000 gap points per GPU, "
                                    "GMRES to 1e-10", "elements": 44000, "points_per_gpu": N_POINTS,

@@ -43,8 +43,9 @@ enum kemcu_boundary { KEMCU_DIRICHLET = 0, KEMCU_NEUMANN = 1 };
 /* arithmetic form of the element integrals */
 enum kemcu_precision {
     KEMCU_FP64 = 0,  /* every node in FP64: the plain form */
-    KEMCU_MIXED = 1  /* FP64 near field (RWG / analytic), FP64 centroid term + FP32 node
-                        correction for the cubature bands, FP64 compensated accumulation */
+    KEMCU_MIXED = 1  /* cubature nodes with the FP32-class hardware reciprocal square root
+                        refined by one FP64 Newton step (~1e-13 relative); RWG / analytic
+                        near field and the compensated accumulation as in FP64 */
 };
 /* which quantities a field evaluation produces (out4 = Ex, Ey, Ez, phi) */
 enum kemcu_what { KEMCU_FIELD_AND_POTENTIAL = 0, KEMCU_POTENTIAL = 1, KEMCU_FIELD = 2 };

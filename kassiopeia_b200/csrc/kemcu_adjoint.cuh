@@ -43,9 +43,10 @@ __device__ void record_from_vertices(const double* e, V3 v0, V3 v1, V3 v2, doubl
     const V3 ea = A * n1, eb = B * n2;
     r[rEa] = ea.x; r[rEa + 1] = ea.y; r[rEa + 2] = ea.z;
     r[rEb] = eb.x; r[rEb + 1] = eb.y; r[rEb + 2] = eb.z;
-    const V3 c = cross(n1, n2);
-    const double cm = norm(c);
-    r[rN3] = c.x / cm; r[rN3 + 1] = c.y / cm; r[rN3 + 2] = c.z / cm;
+    const double cm = norm(cross(n1, n2));
+    r[rAA] = dot(ea, ea);
+    r[rAB2] = 2. * dot(ea, eb);
+    r[rBB] = dot(eb, eb);
     if (type == kTriangle) {
         const V3 cen = v0 + (1. / 3.) * (ea + eb);
         r[rCen] = r[rCen2] = cen.x;

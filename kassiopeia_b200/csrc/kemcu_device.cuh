@@ -13,13 +13,16 @@
 // The band test is evaluated with the same FP64 operations and rounding (no FMA
 // contraction) as the reference so that band boundaries agree bit for bit.
 //
-// Two arithmetic forms of the cubature bands are provided:
-//   * FP64   -- node by node in double precision with IEEE-accurate rsqrt (the plain form);
-//   * MIXED  -- 33-point band: FP64 nodes with an FP32 hardware rsqrt estimate refined by one
-//               FP64 Newton step (<= 4e-13 relative); 12- and 7-point bands: an FP64 centroid
-//               term plus an FP32 node correction written without cancellation (cub_mixed,
-//               ~1e-7 |o|/R < 2e-9 relative per element there).
-// RWG near-field integrals and the analytic line segment are always FP64.
+// Cubature bands are evaluated in FP64 in a quadratic form (cubq below): with the element's
+// centroid c, d = P - c and node offsets o_k = s'_k (A N1) + t'_k (B N2) (s', t' relative to
+// the rule's centroid), |P - Q_k|^2 = R^2 + s' C1 + t' C2 + s'^2 |A N1|^2 + 2 s't' (A N1).(B N2)
+// + t'^2 |B N2|^2 with per-pair C1 = -2 d.(A N1), C2 = -2 d.(B N2): five FMAs per node instead of
+// forming the node and the difference vector, and the field sum collapses to
+// d S0 - (A N1) Ss - (B N2) St with three scalar node sums. Two reciprocal square roots:
+//   * FP64  -- IEEE-accurate double rsqrt (the plain form);
+//   * MIXED -- the FP32-class hardware estimate (rsqrt.approx.f64, ~2^-23 relative) refined by
+//              one FP64 Newton step (~1e-13 relative).
+// RWG near-field integrals and the analytic line segment are FP64 in both forms.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -48,7 +51,9 @@ enum Rec : int
     rEa = 11,      // A * N1 (line: P1 - P0)
     rEb = 14,      // B * N2
     rCen = 17,     // centroid (reference formula)
-    rN3 = 20,      // unit normal N1 x N2 / |N1 x N2| (line: unused)
+    rAA = 20,      // |A N1|^2      (quadratic-form coefficients of the cubature node
+    rAB2 = 21,     // 2 (A N1).(B N2) distances; lines: unused)
+    rBB = 22,      // |B N2|^2
     rInvSize = 23, // 1 / size for the distance ratio
     rPrefac = 24,  // area / (4 pi eps0)   (line: diameter / (4 eps0))
     rType = 25,    // shape as double
@@ -72,10 +77,12 @@ struct Constants
 // Line Gauss-Legendre half rules (x, w) pairs: gl4 [0,2), gl16 [2,10).
 constexpr int kTri7 = 0, kTri12 = 7, kTri33 = 19, kRect7 = 52, kRect12 = 59, kRect33 = 71, kNumNodes = 104;
 __constant__ double c_rules[kNumNodes * 3];
-__constant__ float c_rules_f[kNumNodes * 4];  // s - s_c, t - t_c, w, 0 (centroid-relative)
+// per node, relative to the rule centroid (1/3, 1/3) or (1/2, 1/2):
+//   s', t', s'^2, s't', t'^2, w, w s', w t'
+constexpr int kQ = 8;
+__constant__ double c_q[kNumNodes * kQ];
 __constant__ double c_gl[10 * 2];
 __constant__ Constants c_k;
-__constant__ double c_wsum[kNumNodes];  // FP64 sum of the rule's weights, indexed by rule offset
 
 // ------------------------------------------------------------------------- helpers
 struct V3
@@ -171,105 +178,71 @@ __device__ __forceinline__ int rule_offset(int type, int band, int& n)
     return band == 1 ? kRect33 : band == 2 ? kRect12 : kRect7;
 }
 
-// ------------------------------------------------------------------------- FP64 cubature
+// ------------------------------------------------------------------------- cubature
 // Sum over nodes of w (P-Q)/|P-Q|^3 and w/|P-Q| times area/(4 pi eps0)
 // (Potential_TriNP / ElectricField_TriNP, KElectrostaticCubatureTriangleIntegrator.cc:271-450;
-// the rectangle versions are identical in form).
-// FP64 reciprocal square root from the FP32 hardware estimate plus one Newton step in FP64:
-// relative error <= ~4e-13 (the estimate's 2^-22 squared), used by the MIXED form only.
-__device__ __forceinline__ double rsqrt_newton(double x)
+// the rectangle versions are identical in form), in the quadratic form described at the top.
+//
+// FP64 reciprocal square root from the hardware approximation plus one Newton-Raphson step
+// y1 = y0 (3 - x y0^2) / 2 (quadratic convergence: relative error ~1.5 e0^2), MIXED form only.
+__device__ __forceinline__ double rsqrt_fast(double x)
 {
-    const double y = (double) rsqrtf((float) x);
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
     const double h = fma(-0.5 * x * y, y, 0.5);
     return fma(y, h, y);
 }
 
-// The node count N is a compile-time constant, so the loop is fully unrolled; the rule's
-// (s, t, w) triples are read from constant memory at offsets relative to the rule start OFF.
-template<int N, bool POT, bool FIELD, bool FAST>
-__device__ __forceinline__ Out4 cub64(const double* e, V3 P, const int OFF)
-{
-    const V3 d0 = P - ld3(e + rP0);
-    const V3 a = ld3(e + rEa), b = ld3(e + rEb);
-    double sx = 0., sy = 0., sz = 0., sp = 0.;
-#pragma unroll
-    for (int k = 0; k < N; k++) {
-        const double s = c_rules[3 * (OFF + k)], t = c_rules[3 * (OFF + k) + 1], w = c_rules[3 * (OFF + k) + 2];
-        const double qx = d0.x - s * a.x - t * b.x;
-        const double qy = d0.y - s * a.y - t * b.y;
-        const double qz = d0.z - s * a.z - t * b.z;
-        const double q2 = qx * qx + qy * qy + qz * qz;
-        const double ir = FAST ? rsqrt_newton(q2) : rsqrt(q2);
-        const double wi = w * ir;
-        if (POT)
-            sp += wi;
-        if (FIELD) {
-            const double wi3 = wi * ir * ir;
-            sx += wi3 * qx;
-            sy += wi3 * qy;
-            sz += wi3 * qz;
-        }
-    }
-    const double pf = e[rPrefac];
-    return Out4{pf * sx, pf * sy, pf * sz, pf * sp};
-}
+// Nodes per unrolled group of the node loop (rules whose size it divides are run as a loop
+// over groups, the others fully unrolled). The reciprocal square root of the MIXED form is
+// straight-line code, so a fully unrolled 33-point rule lets the compiler interleave all 33
+// nodes and spill; a loop over groups bounds that window.
+#ifndef KEMCU_GROUP
+#define KEMCU_GROUP 11
+#endif
 
-// ------------------------------------------------------------------------- mixed cubature
-// Split of each node term around the centroid c: with d = P - c (FP64), R = |d| and the node
-// offset o = Q - c, |P - Q|^2 = R^2 (1 - eps), eps = (2 d.o - o.o) / R^2, so
-//   1/|P-Q|   = (1/R)   (1 + f),  f = (1-eps)^(-1/2) - 1 = eps y / (1 + (1-eps) y)
-//   1/|P-Q|^3 = (1/R^3) (1 + g),  g = (1-eps)^(-3/2) - 1 = f (y^2 + y + 1)
-// with y = rsqrt(1 - eps). The rule weights sum to W, so the element sums are
-//   phi = pf/R (W + sum w f),  E = pf/R^3 (d (W + sum w g) - sum w (1+g) o).
-// The large terms W/R and W d/R^3 are FP64; f and g are formed in FP32 without
-// cancellation (absolute error ~1e-7 |f|), so the per-element relative error is about
-// 1e-7 |o|/R: ~2e-8 at the inner edge of the 33-point band, < 3e-9 beyond the 12-point cut.
-template<int N, bool POT, bool FIELD>
-__device__ __forceinline__ Out4 cub_mixed(const double* e, V3 P, const int off)
+// N nodes of the rule starting at node OFF (both compile-time, so the rule constants are
+// constant-bank operands with fixed offsets within a group)
+template<int N, int OFF, bool POT, bool FIELD, bool FAST>
+__device__ __forceinline__ Out4 cubq(const double* e, V3 P)
 {
-    constexpr int n = N;
     const V3 d = P - ld3(e + rCen);
+    const V3 a = ld3(e + rEa), b = ld3(e + rEb);
     const double R2 = dot(d, d);
-    const double iR = rsqrt(R2);
-    const double iR2 = iR * iR;
-    // scaled direction u = 2 d / R^2 and v = 1 / R^2 in FP32
-    const float ux = (float) (2. * d.x * iR2), uy = (float) (2. * d.y * iR2), uz = (float) (2. * d.z * iR2);
-    const float v = (float) iR2;
-    const float ax = (float) e[rEa], ay = (float) e[rEa + 1], az = (float) e[rEa + 2];
-    const float bx = (float) e[rEb], by = (float) e[rEb + 1], bz = (float) e[rEb + 2];
-    float sf = 0.f, sg = 0.f, sox = 0.f, soy = 0.f, soz = 0.f;
+    const double C1 = -2. * dot(d, a), C2 = -2. * dot(d, b);
+    const double aa = e[rAA], ab2 = e[rAB2], bb = e[rBB];
+    double sp = 0., s0 = 0., ss = 0., st = 0.;
+    constexpr int G = N % KEMCU_GROUP == 0 ? KEMCU_GROUP : N;
+#pragma unroll 1
+    for (int g = 0; g < N / G; g++) {
+        const double* cg = c_q + kQ * (OFF + g * G);
 #pragma unroll
-    for (int k = 0; k < n; k++) {
-        const float4 r = *reinterpret_cast<const float4*>(&c_rules_f[4 * (off + k)]);
-        const float ox = r.x * ax + r.y * bx, oy = r.x * ay + r.y * by, oz = r.x * az + r.y * bz;
-        const float oo = ox * ox + oy * oy + oz * oz;
-        const float eps = ux * ox + uy * oy + uz * oz - v * oo;
-        const float om = 1.f - eps;
-        const float y0 = rsqrtf(om);
-        const float y = fmaf(y0, fmaf(-0.5f * om * y0, y0, 0.5f), y0);
-        const float f = eps * y * __fdividef(1.f, 1.f + om * y);
-        if (POT)
-            sf += r.z * f;
-        if (FIELD) {
-            const float g = f * (y * y + y + 1.f);
-            sg += r.z * g;
-            const float wy3 = r.z * (1.f + g);
-            sox += wy3 * ox;
-            soy += wy3 * oy;
-            soz += wy3 * oz;
+        for (int k = 0; k < G; k++) {
+            const double* c = cg + kQ * k;
+            double q2 = fma(c[0], C1, R2);
+            q2 = fma(c[1], C2, q2);
+            q2 = fma(c[2], aa, q2);
+            q2 = fma(c[3], ab2, q2);
+            q2 = fma(c[4], bb, q2);
+            const double ir = FAST ? rsqrt_fast(q2) : rsqrt(q2);
+            if (POT)
+                sp = fma(c[5], ir, sp);
+            if (FIELD) {
+                const double ir3 = ir * ir * ir;
+                s0 = fma(c[5], ir3, s0);
+                ss = fma(c[6], ir3, ss);
+                st = fma(c[7], ir3, st);
+            }
         }
     }
     const double pf = e[rPrefac];
     Out4 o{0., 0., 0., 0.};
-    const double Wd = c_wsum[off];
     if (POT)
-        o.phi = pf * iR * (Wd + (double) sf);
+        o.phi = pf * sp;
     if (FIELD) {
-        const double iR3 = iR * iR2;
-        const double s = Wd + (double) sg;
-        o.ex = pf * iR3 * (d.x * s - (double) sox);
-        o.ey = pf * iR3 * (d.y * s - (double) soy);
-        o.ez = pf * iR3 * (d.z * s - (double) soz);
+        o.ex = pf * (d.x * s0 - a.x * ss - b.x * st);
+        o.ey = pf * (d.y * s0 - a.y * ss - b.y * st);
+        o.ez = pf * (d.z * s0 - a.z * ss - b.z * st);
     }
     return o;
 }
@@ -563,7 +536,9 @@ template<bool POT, bool FIELD> __device__ __noinline__ Out4 line_analytic(const 
 }
 
 // ------------------------------------------------------------------------- one EPI
-// MIXED selects the FP32-split form for the cubature bands; everything else is FP64.
+// MIXED selects the Newton-refined hardware reciprocal square root for the cubature bands;
+// everything else is the same FP64 code. Triangles and rectangles have separate unrolled
+// cubature code (the element type is uniform across a warp, which evaluates one element).
 template<bool MIXED, bool POT, bool FIELD> __device__ __forceinline__ Out4 epi(const double* e, V3 P)
 {
     const int band = band_of(e, P);
@@ -575,17 +550,14 @@ template<bool MIXED, bool POT, bool FIELD> __device__ __forceinline__ Out4 epi(c
     }
     if (band == 0)
         return type == kTriangle ? rwg64<3, POT, FIELD>(e, P) : rwg64<4, POT, FIELD>(e, P);
-    // MIXED: 33-point band as FP64 nodes with the Newton reciprocal square root; 12- and
-    // 7-point bands (|o|/R < 0.02) as FP64 centroid term + FP32 node correction
-    // one code path for both shapes: rectangle rules sit kRect7 - kTri7 entries after the
-    // triangle rules with the same node counts
-    const int off = type == kTriangle ? 0 : kRect7 - kTri7;
+    if (type == kTriangle) {
+        if (band == 1)
+            return cubq<33, kTri33, POT, FIELD, MIXED>(e, P);
+        return band == 2 ? cubq<12, kTri12, POT, FIELD, MIXED>(e, P) : cubq<7, kTri7, POT, FIELD, MIXED>(e, P);
+    }
     if (band == 1)
-        return cub64<33, POT, FIELD, MIXED>(e, P, kTri33 + off);
-    if constexpr (MIXED)
-        return band == 2 ? cub_mixed<12, POT, FIELD>(e, P, kTri12 + off) : cub_mixed<7, POT, FIELD>(e, P, kTri7 + off);
-    else
-        return band == 2 ? cub64<12, POT, FIELD, false>(e, P, kTri12 + off) : cub64<7, POT, FIELD, false>(e, P, kTri7 + off);
+        return cubq<33, kRect33, POT, FIELD, MIXED>(e, P);
+    return band == 2 ? cubq<12, kRect12, POT, FIELD, MIXED>(e, P) : cubq<7, kRect7, POT, FIELD, MIXED>(e, P);
 }
 
 }  // namespace kemcu

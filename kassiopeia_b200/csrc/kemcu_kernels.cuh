@@ -50,36 +50,150 @@ __device__ __forceinline__ void load_tile(double* sm, const double* __restrict__
         dst[i] = __ldg(src + i);
 }
 
+// ------------------------------------------------------------------------- element pipeline
+// K1 streams element records through a ring of kPipe shared-memory stages of kFieldTile
+// records each. A stage is filled by one bulk copy (cp.async.bulk, completion counted on the
+// stage's mbarrier together with the 32 arrivals of the filling warp, whose lanes also store
+// the tile's charge densities). Warps consume stages at their own pace; each warp counts its
+// release of a stage in a shared counter, and the warp that releases it last refills it with
+// the tile kPipe ahead. A warp therefore waits only for data, never for the other warps
+// (which a __syncthreads per tile would impose), so warps that meet near-field elements and
+// warps that meet far-field ones drift apart by up to kPipe - 1 tiles.
+#ifndef KEMCU_FIELD_TILE
+#define KEMCU_FIELD_TILE 32
+#endif
+#ifndef KEMCU_PIPE
+#define KEMCU_PIPE 4
+#endif
+constexpr int kFieldTile = KEMCU_FIELD_TILE;
+constexpr int kPipe = KEMCU_PIPE;
+static_assert(kFieldTile <= 32 && kFieldTile % 2 == 0, "one lane of the filling warp per element");
+
+__device__ __forceinline__ unsigned smem_u32(const void* p)
+{
+    return (unsigned) __cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(unsigned long long* bar, unsigned bytes)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0u;
+}
+// bounded wait for the completion of the phase with the given parity: false after ~2^31
+// cycles (about a second), which only a defect can cause
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity)
+{
+    if (mbar_try_wait(bar, parity))
+        return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > (1ll << 31))
+            return false;
+    return true;
+}
+__device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// global -> shared bulk copy; addresses 16 B aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// element slice [e0, e1) of split blockIdx.y: slices are whole tiles, so every tile starts on
+// a record boundary that is a multiple of kFieldTile
+__device__ __forceinline__ void split_range(int n_elem, int& e0, int& e1)
+{
+    const int per = ((n_elem + (int) gridDim.y - 1) / (int) gridDim.y + kFieldTile - 1) / kFieldTile * kFieldTile;
+    e0 = min(n_elem, (int) blockIdx.y * per);
+    e1 = min(n_elem, e0 + per);
+}
+
 // K1: field and/or potential at points. out layout per point: (Ex, Ey, Ez, phi).
 // nsplit == gridDim.y; partial != nullptr when nsplit > 1 (then out is untouched).
+// flag |= 2 if a pipeline wait timed out (the outputs are then incomplete).
 template<bool MIXED, bool POT, bool FIELD>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) field_kernel(const double* __restrict__ rec, const double* __restrict__ sigma,
                                                          int n_elem, const double* __restrict__ pts, int n_pts,
-                                                         double* __restrict__ out, double* __restrict__ partial)
+                                                         double* __restrict__ out, double* __restrict__ partial,
+                                                         int* __restrict__ flag)
 {
-    __shared__ __align__(16) double s_rec[kTile * rRecSize];
-    __shared__ double s_sig[kTile];
+    __shared__ __align__(128) double s_rec[kPipe][kFieldTile * rRecSize];
+    __shared__ double s_sig[kPipe][kFieldTile];
+    __shared__ __align__(8) unsigned long long s_full[kPipe];
+    __shared__ unsigned s_rel[kPipe], s_used[kPipe];
+    const int lane = threadIdx.x & 31;
+    const unsigned nwarps = blockDim.x >> 5;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = p < n_pts;
     V3 P = v3(0., 0., 0.);
     if (active)
         P = v3(pts[3 * p], pts[3 * p + 1], pts[3 * p + 2]);
-    const int per = (n_elem + gridDim.y - 1) / gridDim.y;
-    const int e0 = blockIdx.y * per;
-    const int e1 = min(n_elem, e0 + per);
+    int e0, e1;
+    split_range(n_elem, e0, e1);
+    const int ntiles = (e1 - e0 + kFieldTile - 1) / kFieldTile;
+    if (threadIdx.x < kPipe) {
+        mbar_init(&s_full[threadIdx.x], 32);
+        s_rel[threadIdx.x] = 0u;
+        s_used[threadIdx.x] = 0u;
+        mbar_init_fence();
+    }
+    __syncthreads();
+    // fill stage i % kPipe with tile i; called by all 32 lanes of one warp
+    auto fill = [&](int i) {
+        const int s = i % kPipe, t0 = e0 + i * kFieldTile, cnt = min(kFieldTile, e1 - t0);
+        if (lane < cnt)
+            s_sig[s][lane] = sigma[t0 + lane];
+        if (lane == 0) {
+            s_used[s]++;
+            fence_proxy_async();
+            const unsigned bytes = (unsigned) (cnt * rRecSize * sizeof(double));
+            mbar_arrive_tx(&s_full[s], bytes);
+            bulk_g2s(s_rec[s], rec + (size_t) t0 * rRecSize, bytes, &s_full[s]);
+        }
+        else
+            mbar_arrive(&s_full[s]);
+    };
+    if (threadIdx.x < 32)
+        for (int i = 0; i < min(kPipe, ntiles); i++)
+            fill(i);
     Kahan kx, ky, kz, kp;
-    for (int t0 = e0; t0 < e1; t0 += kTile) {
-        const int cnt = min(kTile, e1 - t0);
-        __syncthreads();
-        load_tile(s_rec, rec, t0, cnt);
-        if (threadIdx.x < cnt)
-            s_sig[threadIdx.x] = sigma[t0 + threadIdx.x];
-        __syncthreads();
+    bool ok = true;
+    for (int i = 0; i < ntiles; i++) {
+        const int s = i % kPipe;
+        if (!mbar_wait(&s_full[s], (unsigned) (i / kPipe) & 1u)) {
+            ok = false;
+            break;
+        }
         if (active) {
+            const int cnt = min(kFieldTile, e1 - (e0 + i * kFieldTile));
             for (int j = 0; j < cnt; j++) {
-                const double* e = s_rec + j * rRecSize;
-                const Out4 r = epi<MIXED, POT, FIELD>(e, P);
-                const double sg = s_sig[j];
+                const Out4 r = epi<MIXED, POT, FIELD>(s_rec[s] + j * rRecSize, P);
+                const double sg = s_sig[s][j];
                 if (FIELD) {
                     kx.add(r.ex * sg);
                     ky.add(r.ey * sg);
@@ -89,7 +203,25 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) field_kernel(const doubl
                     kp.add(r.phi * sg);
             }
         }
+        // release the stage; the warp that releases it last refills it
+        __syncwarp();
+        unsigned last = 0u;
+        if (lane == 0) {
+            __threadfence_block();
+            last = atomicAdd(&s_rel[s], 1u) % nwarps == nwarps - 1u;
+        }
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (last && i + kPipe < ntiles) {
+            __threadfence_block();
+            fill(i + kPipe);
+        }
     }
+    if (!ok && lane == 0)
+        atomicOr(flag, 2);
+    __syncthreads();
+    // copies still in flight on the error path: wait for each stage's last fill (bounded)
+    if (threadIdx.x < kPipe && s_used[threadIdx.x] > 0u)
+        mbar_wait(&s_full[threadIdx.x], (s_used[threadIdx.x] - 1u) & 1u);
     if (!active)
         return;
     double* o = partial ? partial + ((size_t) blockIdx.y * n_pts + p) * 4 : out + (size_t) p * 4;

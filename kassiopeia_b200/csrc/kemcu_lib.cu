@@ -180,9 +180,11 @@ void build_record(const double* g, int shape, int boundary, double value, const 
         }
         const double cx = g[6] * g[10] - g[7] * g[9], cy = g[7] * g[8] - g[5] * g[10], cz = g[5] * g[9] - g[6] * g[8];
         const double cm = std::sqrt((cx * cx) + (cy * cy) + (cz * cz));
-        r[rN3] = cx * (1. / cm);
-        r[rN3 + 1] = cy * (1. / cm);
-        r[rN3 + 2] = cz * (1. / cm);
+        const double n3[3] = {cx * (1. / cm), cy * (1. / cm), cz * (1. / cm)};
+        // quadratic-form coefficients of the squared node distances
+        r[rAA] = r[rEa] * r[rEa] + r[rEa + 1] * r[rEa + 1] + r[rEa + 2] * r[rEa + 2];
+        r[rAB2] = 2. * (r[rEa] * r[rEb] + r[rEa + 1] * r[rEb + 1] + r[rEa + 2] * r[rEb + 2]);
+        r[rBB] = r[rEb] * r[rEb] + r[rEb + 1] * r[rEb + 1] + r[rEb + 2] * r[rEb + 2];
         if (shape == kTriangle) {
             double p1[3], p2[3];
             for (int c = 0; c < 3; c++) {
@@ -197,7 +199,7 @@ void build_record(const double* g, int shape, int boundary, double value, const 
             r[rInvSize] = 1. / size;
             r[rPrefac] = 0.5 * A * B * cm * K.one_over_four_pi_eps0;
             for (int c = 0; c < 3; c++)
-                t.normal[c] = r[rN3 + c];
+                t.normal[c] = n3[c];
         }
         else {
             for (int c = 0; c < 3; c++) {
@@ -252,26 +254,27 @@ int launch_field(kemcu_ctx* ctx, const double* d_pts, size_t n, double* d_out, i
         partial = (double*) p;
     }
     dim3 grid((unsigned) ((n + kThreads - 1) / kThreads), (unsigned) split);
+    KC(cudaMemsetAsync(ctx->d_flag + 1, 0, sizeof(int), ctx->stream));
     const bool mixed = precision == KEMCU_MIXED;
     const double* sg = ctx->d_sigma;
     const int ne = (int) ctx->n;
     if (what == KEMCU_POTENTIAL) {
         if (mixed)
-            field_kernel<true, true, false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial);
+            field_kernel<true, true, false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial, ctx->d_flag + 1);
         else
-            field_kernel<false, true, false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial);
+            field_kernel<false, true, false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial, ctx->d_flag + 1);
     }
     else if (what == KEMCU_FIELD) {
         if (mixed)
-            field_kernel<true, false, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial);
+            field_kernel<true, false, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial, ctx->d_flag + 1);
         else
-            field_kernel<false, false, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial);
+            field_kernel<false, false, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial, ctx->d_flag + 1);
     }
     else {
         if (mixed)
-            field_kernel<true, true, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial);
+            field_kernel<true, true, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial, ctx->d_flag + 1);
         else
-            field_kernel<false, true, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial);
+            field_kernel<false, true, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial, ctx->d_flag + 1);
     }
     KCHECK_LAUNCH();
     if (split > 1) {
@@ -297,10 +300,12 @@ int check_finite(kemcu_ctx* ctx, const double* d, size_t m, const char* what)
     KC(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
     finite_kernel<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(d, m, ctx->d_flag);
     KCHECK_LAUNCH();
-    int flag = 0;
-    KC(cudaMemcpyAsync(&flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    int flag[2] = {0, 0};
+    KC(cudaMemcpyAsync(flag, ctx->d_flag, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     KC(cudaStreamSynchronize(ctx->stream));
-    if (flag)
+    if (flag[1])
+        return fail(ctx, KEMCU_ETIMEOUT, "element pipeline wait timed out while computing the %s", what);
+    if (flag[0])
         return fail(ctx, KEMCU_ENONFINITE, "%s contains NaN or Inf", what);
     return KEMCU_OK;
 }
@@ -642,30 +647,25 @@ int kemcu_create(kemcu_ctx** out, const kemcu_config* cfg)
     KC(cudaEventCreate(&ctx->ev1));
     KC(cudaMalloc(&ctx->d_counter, 64 * sizeof(unsigned)));
     KC(cudaMemset(ctx->d_counter, 0, 64 * sizeof(unsigned)));
-    KC(cudaMalloc(&ctx->d_flag, sizeof(int)));
+    // [0]: non-finite values seen; [1]: a direct-sum pipeline wait timed out
+    KC(cudaMalloc(&ctx->d_flag, 2 * sizeof(int)));
+    KC(cudaMemset(ctx->d_flag, 0, 2 * sizeof(int)));
     // set-up of kemcu_field_dev_noalloc: the static scratch array's device address on this
     // device (host code may not use the symbol itself as a device pointer)
     KC(cudaGetSymbolAddress((void**) &ctx->noalloc_scratch, g_noalloc_scratch));
     // rule tables
-    std::vector<double> rules(kNumNodes * 3), gl(20), wsum(kNumNodes, 0.);
-    std::vector<float> rf(kNumNodes * 4, 0.f);
+    std::vector<double> rules(kNumNodes * 3), gl(20), q(kNumNodes * kQ);
     tables::build(rules.data(), gl.data());
-    const int offs[7] = {kTri7, kTri12, kTri33, kRect7, kRect12, kRect33, kNumNodes};
-    for (int q = 0; q < 6; q++) {
-        const double sc = q < 3 ? 1. / 3. : 0.5;
-        double ws = 0.;
-        for (int k = offs[q]; k < offs[q + 1]; k++) {
-            rf[4 * k] = (float) (rules[3 * k] - sc);
-            rf[4 * k + 1] = (float) (rules[3 * k + 1] - sc);
-            rf[4 * k + 2] = (float) rules[3 * k + 2];
-            ws += rules[3 * k + 2];
-        }
-        wsum[offs[q]] = ws;
+    for (int k = 0; k < kNumNodes; k++) {
+        const double sc = k < kRect7 ? 1. / 3. : 0.5;  // rule centroid
+        const double s = rules[3 * k] - sc, t = rules[3 * k + 1] - sc, w = rules[3 * k + 2];
+        const double v[kQ] = {s, t, s * s, s * t, t * t, w, w * s, w * t};
+        for (int c = 0; c < kQ; c++)
+            q[kQ * k + c] = v[c];
     }
     KC(cudaMemcpyToSymbol(c_rules, rules.data(), rules.size() * sizeof(double)));
-    KC(cudaMemcpyToSymbol(c_rules_f, rf.data(), rf.size() * sizeof(float)));
+    KC(cudaMemcpyToSymbol(c_q, q.data(), q.size() * sizeof(double)));
     KC(cudaMemcpyToSymbol(c_gl, gl.data(), gl.size() * sizeof(double)));
-    KC(cudaMemcpyToSymbol(c_wsum, wsum.data(), wsum.size() * sizeof(double)));
     KC(cudaMemcpyToSymbol(c_k, &ctx->k, sizeof(Constants)));
     double rk[kStages][kStages];
     rk8_table(rk);
@@ -871,26 +871,27 @@ int kemcu_field_dev_noalloc(kemcu_ctx* ctx, const double* dP, size_t n, double* 
     const int split = (int) std::min((size_t) grid_split(ctx, n, ctx->n), std::max((size_t) 1, cap / (4 * n)));
     double* partial = split > 1 ? ctx->noalloc_scratch : nullptr;
     dim3 grid((unsigned) ((n + kThreads - 1) / kThreads), (unsigned) split);
+    KC(cudaMemsetAsync(ctx->d_flag + 1, 0, sizeof(int), ctx->stream));
     const double* sg = ctx->d_sigma;
     const int ne = (int) ctx->n, np = (int) n;
     const bool mixed = precision == KEMCU_MIXED;
     if (what == KEMCU_POTENTIAL) {
         if (mixed)
-            field_kernel<true, true, false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial);
+            field_kernel<true, true, false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial, ctx->d_flag + 1);
         else
-            field_kernel<false, true, false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial);
+            field_kernel<false, true, false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial, ctx->d_flag + 1);
     }
     else if (what == KEMCU_FIELD) {
         if (mixed)
-            field_kernel<true, false, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial);
+            field_kernel<true, false, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial, ctx->d_flag + 1);
         else
-            field_kernel<false, false, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial);
+            field_kernel<false, false, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial, ctx->d_flag + 1);
     }
     else {
         if (mixed)
-            field_kernel<true, true, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial);
+            field_kernel<true, true, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial, ctx->d_flag + 1);
         else
-            field_kernel<false, true, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial);
+            field_kernel<false, true, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial, ctx->d_flag + 1);
     }
     KCHECK_LAUNCH();
     if (split > 1) {
