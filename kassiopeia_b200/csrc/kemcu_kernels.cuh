@@ -2,9 +2,9 @@
 // boundary-integral matvec (K2), operator assembly and the dense (assembled) matvec.
 //
 // Layout: one thread owns one evaluation point (a field point, or a target centroid for the
-// matvec); a CTA of kThreads points streams a contiguous slice of the element records through
-// shared memory in tiles of kTile elements (256 B records, copied with 16 B vector loads), and
-// every thread sums the tile's contributions with Kahan compensation, as the reference's
+// matvec); a CTA of kThreads points streams its slice of the element records (256 B each)
+// through a ring of shared-memory stages filled by bulk copies (ElementRing), and every
+// thread sums the contributions with Kahan compensation, as the reference's
 // KIntegratingFieldSolver does (KElectrostaticIntegratingFieldSolver.hh:261-339). When there
 // are too few points to fill the GPU the element list is split over gridDim.y; each split
 // writes a partial sum to scratch and reduce_splits adds the splits in a fixed order, so the
@@ -17,11 +17,6 @@ namespace kemcu
 {
 
 constexpr int kThreads = 128;
-// elements per shared-memory tile (records of 256 B: kTile * 256 B of shared memory)
-#ifndef KEMCU_TILE
-#define KEMCU_TILE 128
-#endif
-constexpr int kTile = KEMCU_TILE;
 // resident CTAs per SM the direct-sum kernels are compiled for (bounds their registers)
 #ifndef KEMCU_MIN_BLOCKS
 #define KEMCU_MIN_BLOCKS 4
@@ -40,7 +35,7 @@ struct Kahan
     }
 };
 
-// cooperative copy of `count` element records (256 B each) into shared memory
+// cooperative copy of `count` element records (256 B each) into shared memory (tracker)
 __device__ __forceinline__ void load_tile(double* sm, const double* __restrict__ rec, int first, int count)
 {
     const double2* src = reinterpret_cast<const double2*>(rec + (size_t) first * rRecSize);
@@ -124,14 +119,116 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                  : "memory");
 }
 
-// element slice [e0, e1) of split blockIdx.y: slices are whole tiles, so every tile starts on
-// a record boundary that is a multiple of kFieldTile
-__device__ __forceinline__ void split_range(int n_elem, int& e0, int& e1)
+// element slice [e0, e1) of [first, last) for split blockIdx.y, in whole tiles
+__device__ __forceinline__ void split_range(int first, int last, int& e0, int& e1)
 {
-    const int per = ((n_elem + (int) gridDim.y - 1) / (int) gridDim.y + kFieldTile - 1) / kFieldTile * kFieldTile;
-    e0 = min(n_elem, (int) blockIdx.y * per);
-    e1 = min(n_elem, e0 + per);
+    const int span = last - first;
+    const int per = ((span + (int) gridDim.y - 1) / (int) gridDim.y + kFieldTile - 1) / kFieldTile * kFieldTile;
+    e0 = min(last, first + (int) blockIdx.y * per);
+    e1 = min(last, e0 + per);
 }
+
+// The ring: kPipe stages of kFieldTile element records plus SIDE doubles of per-element side
+// data (charge densities, matvec operands) per element, stored by the filling warp's lanes.
+// RingStorage lives in shared memory; ElementRing (registers) holds the CTA's element slice
+// and a reference to it.
+template<int SIDE> struct RingStorage
+{
+    double rec[kPipe][kFieldTile * rRecSize];
+    double side[kPipe][SIDE > 0 ? SIDE : 1][kFieldTile];
+    unsigned long long full[kPipe];
+    unsigned rel[kPipe], used[kPipe];
+};
+
+template<int SIDE> struct ElementRing
+{
+    RingStorage<SIDE>& S;
+    int e0, e1;  // this CTA's element slice
+
+    __device__ __forceinline__ ElementRing(RingStorage<SIDE>& storage, int first, int last) : S(storage)
+    {
+        split_range(first, last, e0, e1);
+        if (threadIdx.x < kPipe) {
+            mbar_init(&S.full[threadIdx.x], 32);
+            S.rel[threadIdx.x] = 0u;
+            S.used[threadIdx.x] = 0u;
+            mbar_init_fence();
+        }
+        __syncthreads();
+    }
+    __device__ __forceinline__ int tiles() const
+    {
+        return (e1 - e0 + kFieldTile - 1) / kFieldTile;
+    }
+    __device__ __forceinline__ int first(int i) const
+    {
+        return e0 + i * kFieldTile;
+    }
+    __device__ __forceinline__ int count(int i) const
+    {
+        return min(kFieldTile, e1 - first(i));
+    }
+    __device__ __forceinline__ const double* element(int i, int j) const
+    {
+        return S.rec[i % kPipe] + j * rRecSize;
+    }
+    __device__ __forceinline__ double side(int i, int k, int j) const
+    {
+        return S.side[i % kPipe][k][j];
+    }
+    // fill stage i % kPipe with tile i: called by all 32 lanes of one warp;
+    // side_fn(double (*side)[kFieldTile], int t0, int cnt, int lane) stores the side data
+    template<class F> __device__ __forceinline__ void fill(const double* __restrict__ src, int i, F side_fn)
+    {
+        const int s = i % kPipe, t0 = first(i), cnt = count(i), lane = threadIdx.x & 31;
+        side_fn(S.side[s], t0, cnt, lane);
+        if (lane == 0) {
+            S.used[s]++;
+            fence_proxy_async();
+            const unsigned bytes = (unsigned) (cnt * rRecSize * sizeof(double));
+            mbar_arrive_tx(&S.full[s], bytes);
+            bulk_g2s(S.rec[s], src + (size_t) t0 * rRecSize, bytes, &S.full[s]);
+        }
+        else
+            mbar_arrive(&S.full[s]);
+    }
+    template<class F> __device__ __forceinline__ void prologue(const double* __restrict__ src, F side_fn)
+    {
+        if (threadIdx.x < 32)
+            for (int i = 0; i < min(kPipe, tiles()); i++)
+                fill(src, i, side_fn);
+    }
+    __device__ __forceinline__ bool wait(int i)
+    {
+        return mbar_wait(&S.full[i % kPipe], (unsigned) (i / kPipe) & 1u);
+    }
+    // whole warp: release tile i; the warp that releases a stage last refills it
+    template<class F> __device__ __forceinline__ void release(const double* __restrict__ src, int i, F side_fn)
+    {
+        const int s = i % kPipe;
+        __syncwarp();
+        unsigned last = 0u;
+        if ((threadIdx.x & 31) == 0) {
+            __threadfence_block();
+            last = atomicAdd(&S.rel[s], 1u) % (blockDim.x >> 5) == (blockDim.x >> 5) - 1u;
+        }
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (last && i + kPipe < tiles()) {
+            __threadfence_block();
+            fill(src, i + kPipe, side_fn);
+        }
+    }
+    // after the tile loop (all threads): report a timed-out wait in flag (|= 2) and wait,
+    // bounded, for copies still in flight
+    __device__ __forceinline__ void finish(bool ok, int* flag)
+    {
+        if (!ok && (threadIdx.x & 31) == 0)
+            atomicOr(flag, 2);
+        __syncthreads();
+        if (threadIdx.x < kPipe && S.used[threadIdx.x] > 0u)
+            mbar_wait(&S.full[threadIdx.x], (S.used[threadIdx.x] - 1u) & 1u);
+    }
+};
 
 // K1: field and/or potential at points. out layout per point: (Ex, Ey, Ez, phi).
 // nsplit == gridDim.y; partial != nullptr when nsplit > 1 (then out is untouched).
@@ -142,58 +239,31 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) field_kernel(const doubl
                                                          double* __restrict__ out, double* __restrict__ partial,
                                                          int* __restrict__ flag)
 {
-    __shared__ __align__(128) double s_rec[kPipe][kFieldTile * rRecSize];
-    __shared__ double s_sig[kPipe][kFieldTile];
-    __shared__ __align__(8) unsigned long long s_full[kPipe];
-    __shared__ unsigned s_rel[kPipe], s_used[kPipe];
-    const int lane = threadIdx.x & 31;
-    const unsigned nwarps = blockDim.x >> 5;
+    __shared__ __align__(128) RingStorage<1> S;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = p < n_pts;
     V3 P = v3(0., 0., 0.);
     if (active)
         P = v3(pts[3 * p], pts[3 * p + 1], pts[3 * p + 2]);
-    int e0, e1;
-    split_range(n_elem, e0, e1);
-    const int ntiles = (e1 - e0 + kFieldTile - 1) / kFieldTile;
-    if (threadIdx.x < kPipe) {
-        mbar_init(&s_full[threadIdx.x], 32);
-        s_rel[threadIdx.x] = 0u;
-        s_used[threadIdx.x] = 0u;
-        mbar_init_fence();
-    }
-    __syncthreads();
-    // fill stage i % kPipe with tile i; called by all 32 lanes of one warp
-    auto fill = [&](int i) {
-        const int s = i % kPipe, t0 = e0 + i * kFieldTile, cnt = min(kFieldTile, e1 - t0);
+    ElementRing<1> R(S, 0, n_elem);
+    auto side = [&](double (*sd)[kFieldTile], int t0, int cnt, int lane) {
         if (lane < cnt)
-            s_sig[s][lane] = sigma[t0 + lane];
-        if (lane == 0) {
-            s_used[s]++;
-            fence_proxy_async();
-            const unsigned bytes = (unsigned) (cnt * rRecSize * sizeof(double));
-            mbar_arrive_tx(&s_full[s], bytes);
-            bulk_g2s(s_rec[s], rec + (size_t) t0 * rRecSize, bytes, &s_full[s]);
-        }
-        else
-            mbar_arrive(&s_full[s]);
+            sd[0][lane] = sigma[t0 + lane];
     };
-    if (threadIdx.x < 32)
-        for (int i = 0; i < min(kPipe, ntiles); i++)
-            fill(i);
+    R.prologue(rec, side);
+    const int ntiles = R.tiles();
     Kahan kx, ky, kz, kp;
     bool ok = true;
     for (int i = 0; i < ntiles; i++) {
-        const int s = i % kPipe;
-        if (!mbar_wait(&s_full[s], (unsigned) (i / kPipe) & 1u)) {
+        if (!R.wait(i)) {
             ok = false;
             break;
         }
         if (active) {
-            const int cnt = min(kFieldTile, e1 - (e0 + i * kFieldTile));
+            const int cnt = R.count(i);
             for (int j = 0; j < cnt; j++) {
-                const Out4 r = epi<MIXED, POT, FIELD>(s_rec[s] + j * rRecSize, P);
-                const double sg = s_sig[s][j];
+                const Out4 r = epi<MIXED, POT, FIELD>(R.element(i, j), P);
+                const double sg = R.side(i, 0, j);
                 if (FIELD) {
                     kx.add(r.ex * sg);
                     ky.add(r.ey * sg);
@@ -203,25 +273,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) field_kernel(const doubl
                     kp.add(r.phi * sg);
             }
         }
-        // release the stage; the warp that releases it last refills it
-        __syncwarp();
-        unsigned last = 0u;
-        if (lane == 0) {
-            __threadfence_block();
-            last = atomicAdd(&s_rel[s], 1u) % nwarps == nwarps - 1u;
-        }
-        last = __shfl_sync(0xffffffffu, last, 0);
-        if (last && i + kPipe < ntiles) {
-            __threadfence_block();
-            fill(i + kPipe);
-        }
+        R.release(rec, i, side);
     }
-    if (!ok && lane == 0)
-        atomicOr(flag, 2);
-    __syncthreads();
-    // copies still in flight on the error path: wait for each stage's last fill (bounded)
-    if (threadIdx.x < kPipe && s_used[threadIdx.x] > 0u)
-        mbar_wait(&s_full[threadIdx.x], (s_used[threadIdx.x] - 1u) & 1u);
+    R.finish(ok, flag);
     if (!active)
         return;
     double* o = partial ? partial + ((size_t) blockIdx.y * n_pts + p) * 4 : out + (size_t) p * 4;
@@ -268,17 +322,18 @@ template<bool MIXED> __device__ __forceinline__ double entry(const double* e, co
     return t.diag;
 }
 
-// K2: y[r][i] = sum_j A(i, j) x[r][j] for r < nrhs (nrhs <= kMaxRhs), entries recomputed
-// on the fly (KMatrix::Multiply over KBoundaryIntegralMatrix::operator(),
-// KMatrix.hh:92-99, KBoundaryIntegralMatrix.hh:31-55).
+// K2: y[r][i] = sum_j A(i, j) x[r][j] for r < nrhs (nrhs <= NR <= kMaxRhs), entries
+// recomputed on the fly (KMatrix::Multiply over KBoundaryIntegralMatrix::operator(),
+// KMatrix.hh:92-99, KBoundaryIntegralMatrix.hh:31-55). Same element ring as K1, with the
+// operand values of the tile as side data.
 constexpr int kMaxRhs = 8;
-template<bool MIXED>
+template<bool MIXED, int NR>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) matvec_kernel(const double* __restrict__ rec, const TargetRec* __restrict__ tgt,
                                                           int n, const double* __restrict__ x, int nrhs,
-                                                          double* __restrict__ y, double* __restrict__ partial)
+                                                          double* __restrict__ y, double* __restrict__ partial,
+                                                          int* __restrict__ flag)
 {
-    __shared__ __align__(16) double s_rec[kTile * rRecSize];
-    __shared__ double s_x[kMaxRhs][kTile];
+    __shared__ __align__(128) RingStorage<NR> S;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = i < n;
     TargetRec t{};
@@ -287,27 +342,34 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) matvec_kernel(const doub
         t = tgt[i];
         C = v3(t.cen[0], t.cen[1], t.cen[2]);
     }
-    const int per = (n + gridDim.y - 1) / gridDim.y;
-    const int e0 = blockIdx.y * per;
-    const int e1 = min(n, e0 + per);
-    Kahan acc[kMaxRhs];
-    for (int t0 = e0; t0 < e1; t0 += kTile) {
-        const int cnt = min(kTile, e1 - t0);
-        __syncthreads();
-        load_tile(s_rec, rec, t0, cnt);
-        for (int q = threadIdx.x; q < cnt * nrhs; q += blockDim.x)
-            s_x[q / cnt][q % cnt] = x[(size_t) (q / cnt) * n + t0 + q % cnt];
-        __syncthreads();
+    ElementRing<NR> R(S, 0, n);
+    auto side = [&](double (*sd)[kFieldTile], int t0, int cnt, int lane) {
+        if (lane < cnt)
+            for (int r = 0; r < nrhs; r++)
+                sd[r][lane] = x[(size_t) r * n + t0 + lane];
+    };
+    R.prologue(rec, side);
+    const int ntiles = R.tiles();
+    Kahan acc[NR];
+    bool ok = true;
+    for (int q = 0; q < ntiles; q++) {
+        if (!R.wait(q)) {
+            ok = false;
+            break;
+        }
         if (active) {
+            const int cnt = R.count(q);
             for (int j = 0; j < cnt; j++) {
-                const double a = entry<MIXED>(s_rec + j * rRecSize, t, C);
+                const double a = entry<MIXED>(R.element(q, j), t, C);
 #pragma unroll
-                for (int r = 0; r < kMaxRhs; r++)
+                for (int r = 0; r < NR; r++)
                     if (r < nrhs)
-                        acc[r].add(a * s_x[r][j]);
+                        acc[r].add(a * R.side(q, r, j));
             }
         }
+        R.release(rec, q, side);
     }
+    R.finish(ok, flag);
     if (!active)
         return;
     for (int r = 0; r < nrhs; r++) {
@@ -323,9 +385,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) matvec_kernel(const doub
 template<bool MIXED>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) assemble_kernel(const double* __restrict__ rec, const TargetRec* __restrict__ tgt,
                                                             int n, int j0, int j1, double* __restrict__ a64,
-                                                            float* __restrict__ a32)
+                                                            float* __restrict__ a32, int* __restrict__ flag)
 {
-    __shared__ __align__(16) double s_rec[kTile * rRecSize];
+    __shared__ __align__(128) RingStorage<0> S;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = i < n;
     TargetRec t{};
@@ -334,18 +396,20 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) assemble_kernel(const do
         t = tgt[i];
         C = v3(t.cen[0], t.cen[1], t.cen[2]);
     }
-    const int span = j1 - j0;
-    const int per = (span + gridDim.y - 1) / gridDim.y;
-    const int e0 = j0 + blockIdx.y * per;
-    const int e1 = min(j1, e0 + per);
-    for (int t0 = e0; t0 < e1; t0 += kTile) {
-        const int cnt = min(kTile, e1 - t0);
-        __syncthreads();
-        load_tile(s_rec, rec, t0, cnt);
-        __syncthreads();
+    ElementRing<0> R(S, j0, j1);
+    auto side = [](double (*)[kFieldTile], int, int, int) {};
+    R.prologue(rec, side);
+    const int ntiles = R.tiles();
+    bool ok = true;
+    for (int q = 0; q < ntiles; q++) {
+        if (!R.wait(q)) {
+            ok = false;
+            break;
+        }
         if (active) {
+            const int t0 = R.first(q), cnt = R.count(q);
             for (int j = 0; j < cnt; j++) {
-                const double a = entry<MIXED>(s_rec + j * rRecSize, t, C);
+                const double a = entry<MIXED>(R.element(q, j), t, C);
                 const size_t idx = (size_t) (t0 + j - j0) * n + i;
                 if (a64)
                     a64[idx] = a;
@@ -353,7 +417,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) assemble_kernel(const do
                     a32[idx] = (float) a;
             }
         }
+        R.release(rec, q, side);
     }
+    R.finish(ok, flag);
 }
 
 // dense matvec on the assembled column-major operator: y[r][i] = sum_j A[j*n+i] x[r][j].

@@ -230,6 +230,24 @@ void build_record(const double* g, int shape, int boundary, double value, const 
     rhs = boundary == KEMCU_NEUMANN ? 0. : value;
 }
 
+// the direct-sum kernels OR 2 into d_flag[1] when an element-pipeline wait times out; a
+// public call clears the word before its first such launch and reads it when it is done
+int clear_pipe_flag(kemcu_ctx* ctx)
+{
+    KC(cudaMemsetAsync(ctx->d_flag + 1, 0, sizeof(int), ctx->stream));
+    return KEMCU_OK;
+}
+
+int pipe_status(kemcu_ctx* ctx, const char* what)
+{
+    int f = 0;
+    KC(cudaMemcpyAsync(&f, ctx->d_flag + 1, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    KC(cudaStreamSynchronize(ctx->stream));
+    if (f)
+        return fail(ctx, KEMCU_ETIMEOUT, "element pipeline wait timed out while computing the %s", what);
+    return KEMCU_OK;
+}
+
 int grid_split(const kemcu_ctx* ctx, size_t n_pts, size_t n_elem)
 {
     // enough CTAs for four waves of the resident CTAs per SM, each split keeping >= 32 elements
@@ -254,7 +272,8 @@ int launch_field(kemcu_ctx* ctx, const double* d_pts, size_t n, double* d_out, i
         partial = (double*) p;
     }
     dim3 grid((unsigned) ((n + kThreads - 1) / kThreads), (unsigned) split);
-    KC(cudaMemsetAsync(ctx->d_flag + 1, 0, sizeof(int), ctx->stream));
+    if (int rc = clear_pipe_flag(ctx))
+        return rc;
     const bool mixed = precision == KEMCU_MIXED;
     const double* sg = ctx->d_sigma;
     const int ne = (int) ctx->n;
@@ -361,10 +380,21 @@ int apply_op(kemcu_ctx* ctx, int op, const double* d_x, double* d_y, int nrhs)
             partial = (double*) p;
         }
         dim3 grid((n + kThreads - 1) / kThreads, split);
-        if (op == kFree64)
-            matvec_kernel<false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, ctx->d_tgt, n, d_x, nrhs, d_y, partial);
-        else
-            matvec_kernel<true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, ctx->d_tgt, n, d_x, nrhs, d_y, partial);
+        int* fl = ctx->d_flag + 1;
+        if (op == kFree64) {
+            if (nrhs == 1)
+                matvec_kernel<false, 1><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, ctx->d_tgt, n, d_x, nrhs, d_y, partial, fl);
+            else
+                matvec_kernel<false, kMaxRhs><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, ctx->d_tgt, n, d_x, nrhs, d_y,
+                                                                                  partial, fl);
+        }
+        else {
+            if (nrhs == 1)
+                matvec_kernel<true, 1><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, ctx->d_tgt, n, d_x, nrhs, d_y, partial, fl);
+            else
+                matvec_kernel<true, kMaxRhs><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, ctx->d_tgt, n, d_x, nrhs, d_y,
+                                                                                 partial, fl);
+        }
         KCHECK_LAUNCH();
         if (split > 1) {
             const size_t m = (size_t) nrhs * n;
@@ -426,7 +456,7 @@ int assemble(kemcu_ctx* ctx, bool want32)
     const int split = grid_split(ctx, n, n);
     dim3 grid((unsigned) ((n + kThreads - 1) / kThreads), (unsigned) split);
     assemble_kernel<false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, ctx->d_tgt, (int) n, 0, (int) n, ctx->d_a64,
-                                                              fill32 ? ctx->d_a32 : nullptr);
+                                                              fill32 ? ctx->d_a32 : nullptr, ctx->d_flag + 1);
     KCHECK_LAUNCH();
     return KEMCU_OK;
 }
@@ -871,7 +901,8 @@ int kemcu_field_dev_noalloc(kemcu_ctx* ctx, const double* dP, size_t n, double* 
     const int split = (int) std::min((size_t) grid_split(ctx, n, ctx->n), std::max((size_t) 1, cap / (4 * n)));
     double* partial = split > 1 ? ctx->noalloc_scratch : nullptr;
     dim3 grid((unsigned) ((n + kThreads - 1) / kThreads), (unsigned) split);
-    KC(cudaMemsetAsync(ctx->d_flag + 1, 0, sizeof(int), ctx->stream));
+    if ((rc = clear_pipe_flag(ctx)))
+        return rc;
     const double* sg = ctx->d_sigma;
     const int ne = (int) ctx->n, np = (int) n;
     const bool mixed = precision == KEMCU_MIXED;
@@ -939,11 +970,10 @@ int kemcu_matrix_element(kemcu_ctx* ctx, size_t i, size_t j, double* a)
     KC(cudaMemsetAsync(dx, 0, ctx->n * sizeof(double), ctx->stream));
     const double one = 1.;
     KC(cudaMemcpyAsync((double*) dx + j, &one, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    if ((rc = apply_op(ctx, kFree64, (const double*) dx, (double*) dy, 1)))
+    if ((rc = clear_pipe_flag(ctx)) || (rc = apply_op(ctx, kFree64, (const double*) dx, (double*) dy, 1)))
         return rc;
     KC(cudaMemcpyAsync(a, (double*) dy + i, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    KC(cudaStreamSynchronize(ctx->stream));
-    return KEMCU_OK;
+    return pipe_status(ctx, "matrix element");
 }
 
 int kemcu_matvec(kemcu_ctx* ctx, const double* x, double* y, int n_rhs, int precision, int assembled)
@@ -959,6 +989,8 @@ int kemcu_matvec(kemcu_ctx* ctx, const double* x, double* y, int n_rhs, int prec
     if ((rc = ensure(ctx, sVec0, m * sizeof(double), &dx)) || (rc = ensure(ctx, sVec1, m * sizeof(double), &dy)))
         return rc;
     KC(cudaMemcpyAsync(dx, x, m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = clear_pipe_flag(ctx)))
+        return rc;
     Timer t(ctx);
     int op = precision == KEMCU_MIXED ? kFreeMixed : kFree64;
     if (assembled) {
@@ -970,8 +1002,7 @@ int kemcu_matvec(kemcu_ctx* ctx, const double* x, double* y, int n_rhs, int prec
         return rc;
     t.stop();
     KC(cudaMemcpyAsync(y, dy, m * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    KC(cudaStreamSynchronize(ctx->stream));
-    return KEMCU_OK;
+    return pipe_status(ctx, "matvec");
 }
 
 void kemcu_set_iteration_callback(kemcu_ctx* ctx, kemcu_iteration_callback cb, void* user)
@@ -992,6 +1023,8 @@ int kemcu_gmres(kemcu_ctx* ctx, const double* b, double* x, int n_rhs, double re
         mode < 0 || mode > 2)
         return fail(ctx, KEMCU_EINVAL, "invalid gmres arguments");
     KC(cudaSetDevice(ctx->device));
+    if ((rc = clear_pipe_flag(ctx)))
+        return rc;
     const int n = (int) ctx->n;
     const size_t m = (size_t) n_rhs * n;
     // device vectors: b, x, residual/correction
