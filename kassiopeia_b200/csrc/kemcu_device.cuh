@@ -81,6 +81,12 @@ __constant__ double c_rules[kNumNodes * 3];
 //   s', t', s'^2, s't', t'^2, w, w s', w t'
 constexpr int kQ = 8;
 __constant__ double c_q[kNumNodes * kQ];
+// The rectangle rules are centrally symmetric: node pairs (o, -o) of equal weight, plus at
+// most one node at the centroid. Per pair, the values above for the + node; offsets of the
+// three rules' pairs and the centroid-node weights (rect7, rect33):
+constexpr int kPair7 = 0, kPair12 = 3, kPair33 = 9, kNumPairs = 25;
+__constant__ double c_qp[kNumPairs * kQ];
+__constant__ double c_qc[2];
 __constant__ double c_gl[10 * 2];
 __constant__ Constants c_k;
 
@@ -232,6 +238,64 @@ __device__ __forceinline__ Out4 cubq(const double* e, V3 P)
                 s0 = fma(c[5], ir3, s0);
                 ss = fma(c[6], ir3, ss);
                 st = fma(c[7], ir3, st);
+            }
+        }
+    }
+    const double pf = e[rPrefac];
+    Out4 o{0., 0., 0., 0.};
+    if (POT)
+        o.phi = pf * sp;
+    if (FIELD) {
+        o.ex = pf * (d.x * s0 - a.x * ss - b.x * st);
+        o.ey = pf * (d.y * s0 - a.y * ss - b.y * st);
+        o.ez = pf * (d.z * s0 - a.z * ss - b.z * st);
+    }
+    return o;
+}
+
+// Centrally symmetric rules (rectangles): with L = s' C1 + t' C2 and
+// Q = R^2 + s'^2 |A N1|^2 + ... the pair's squared distances are Q + L and Q - L, and the two
+// nodes' field terms combine as w (ir3+ + ir3-) into S0 and w s' (ir3+ - ir3-) into Ss, St:
+// 26 FP64 operations per pair instead of 30 for two nodes. NP pairs from pair POFF, plus the
+// centroid node of weight c_qc[CENTER] when CENTER >= 0.
+#ifndef KEMCU_PAIR_GROUP
+#define KEMCU_PAIR_GROUP 16
+#endif
+template<int NP, int POFF, int CENTER, bool POT, bool FIELD, bool FAST>
+__device__ __forceinline__ Out4 cubq_pairs(const double* e, V3 P)
+{
+    const V3 d = P - ld3(e + rCen);
+    const V3 a = ld3(e + rEa), b = ld3(e + rEb);
+    const double R2 = dot(d, d);
+    const double C1 = -2. * dot(d, a), C2 = -2. * dot(d, b);
+    const double aa = e[rAA], ab2 = e[rAB2], bb = e[rBB];
+    double sp = 0., s0 = 0., ss = 0., st = 0.;
+    if (CENTER >= 0) {
+        const double ir = FAST ? rsqrt_fast(R2) : rsqrt(R2);
+        sp = c_qc[CENTER] * ir;
+        s0 = c_qc[CENTER] * (ir * ir * ir);
+    }
+    constexpr int G = NP % KEMCU_PAIR_GROUP == 0 ? KEMCU_PAIR_GROUP : NP;
+#pragma unroll 1
+    for (int g = 0; g < NP / G; g++) {
+        const double* cg = c_qp + kQ * (POFF + g * G);
+#pragma unroll
+        for (int k = 0; k < G; k++) {
+            const double* c = cg + kQ * k;
+            const double L = fma(c[1], C2, c[0] * C1);
+            double Q = fma(c[2], aa, R2);
+            Q = fma(c[3], ab2, Q);
+            Q = fma(c[4], bb, Q);
+            const double irp = FAST ? rsqrt_fast(Q + L) : rsqrt(Q + L);
+            const double irm = FAST ? rsqrt_fast(Q - L) : rsqrt(Q - L);
+            if (POT)
+                sp = fma(c[5], irp + irm, sp);
+            if (FIELD) {
+                const double i3p = irp * irp * irp, i3m = irm * irm * irm;
+                s0 = fma(c[5], i3p + i3m, s0);
+                const double dd = i3p - i3m;
+                ss = fma(c[6], dd, ss);
+                st = fma(c[7], dd, st);
             }
         }
     }
@@ -539,25 +603,44 @@ template<bool POT, bool FIELD> __device__ __noinline__ Out4 line_analytic(const 
 // MIXED selects the Newton-refined hardware reciprocal square root for the cubature bands;
 // everything else is the same FP64 code. Triangles and rectangles have separate unrolled
 // cubature code (the element type is uniform across a warp, which evaluates one element).
-template<bool MIXED, bool POT, bool FIELD> __device__ __forceinline__ Out4 epi(const double* e, V3 P)
+//
+// epi_far evaluates the numeric bands and returns false, without evaluating, for the
+// analytic near-field band (RWG polygons, analytic wire), which epi_near evaluates. Kernels
+// that stream many elements defer the near-field pairs of a tile to a second pass, so the
+// calls of the (non-inlined) analytic integrals stay out of the numeric loop.
+template<bool MIXED, bool POT, bool FIELD> __device__ __forceinline__ bool epi_far(const double* e, V3 P, Out4& o)
 {
     const int band = band_of(e, P);
-    const int type = (int) e[rType];
-    if (type == kLineSegment) {
-        if (band == 0)
-            return line_analytic<POT, FIELD>(e, P);
-        return band == 1 ? line_gauss<POT, FIELD>(e, P, 2, 8) : line_gauss<POT, FIELD>(e, P, 0, 2);
-    }
     if (band == 0)
-        return type == kTriangle ? rwg64<3, POT, FIELD>(e, P) : rwg64<4, POT, FIELD>(e, P);
-    if (type == kTriangle) {
-        if (band == 1)
-            return cubq<33, kTri33, POT, FIELD, MIXED>(e, P);
-        return band == 2 ? cubq<12, kTri12, POT, FIELD, MIXED>(e, P) : cubq<7, kTri7, POT, FIELD, MIXED>(e, P);
-    }
-    if (band == 1)
-        return cubq<33, kRect33, POT, FIELD, MIXED>(e, P);
-    return band == 2 ? cubq<12, kRect12, POT, FIELD, MIXED>(e, P) : cubq<7, kRect7, POT, FIELD, MIXED>(e, P);
+        return false;
+    const int type = (int) e[rType];
+    if (type == kLineSegment)
+        o = band == 1 ? line_gauss<POT, FIELD>(e, P, 2, 8) : line_gauss<POT, FIELD>(e, P, 0, 2);
+    else if (type == kTriangle)
+        o = band == 1   ? cubq<33, kTri33, POT, FIELD, MIXED>(e, P)
+            : band == 2 ? cubq<12, kTri12, POT, FIELD, MIXED>(e, P)
+                        : cubq<7, kTri7, POT, FIELD, MIXED>(e, P);
+    else
+        o = band == 1   ? cubq_pairs<16, kPair33, 1, POT, FIELD, MIXED>(e, P)
+            : band == 2 ? cubq_pairs<6, kPair12, -1, POT, FIELD, MIXED>(e, P)
+                        : cubq_pairs<3, kPair7, 0, POT, FIELD, MIXED>(e, P);
+    return true;
+}
+
+template<bool POT, bool FIELD> __device__ __forceinline__ Out4 epi_near(const double* e, V3 P)
+{
+    const int type = (int) e[rType];
+    if (type == kLineSegment)
+        return line_analytic<POT, FIELD>(e, P);
+    return type == kTriangle ? rwg64<3, POT, FIELD>(e, P) : rwg64<4, POT, FIELD>(e, P);
+}
+
+template<bool MIXED, bool POT, bool FIELD> __device__ __forceinline__ Out4 epi(const double* e, V3 P)
+{
+    Out4 o;
+    if (epi_far<MIXED, POT, FIELD>(e, P, o))
+        return o;
+    return epi_near<POT, FIELD>(e, P);
 }
 
 }  // namespace kemcu

@@ -19,7 +19,7 @@ namespace kemcu
 constexpr int kThreads = 128;
 // resident CTAs per SM the direct-sum kernels are compiled for (bounds their registers)
 #ifndef KEMCU_MIN_BLOCKS
-#define KEMCU_MIN_BLOCKS 4
+#define KEMCU_MIN_BLOCKS 5
 #endif
 constexpr int kMinBlocks = KEMCU_MIN_BLOCKS;
 

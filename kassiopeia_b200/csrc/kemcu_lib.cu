@@ -695,6 +695,43 @@ int kemcu_create(kemcu_ctx** out, const kemcu_config* cfg)
     }
     KC(cudaMemcpyToSymbol(c_rules, rules.data(), rules.size() * sizeof(double)));
     KC(cudaMemcpyToSymbol(c_q, q.data(), q.size() * sizeof(double)));
+    // pair form of the centrally symmetric rectangle rules
+    std::vector<double> qp(kNumPairs * kQ, 0.);
+    double qc[2] = {0., 0.};
+    const int rule_first[3] = {kRect7, kRect12, kRect33}, rule_n[3] = {7, 12, 33};
+    const int pair_first[3] = {kPair7, kPair12, kPair33}, pair_n[3] = {3, 6, 16}, center[3] = {0, -1, 1};
+    for (int r = 0; r < 3; r++) {
+        std::vector<bool> used(rule_n[r], false);
+        int np = 0, nc = 0;
+        for (int i = 0; i < rule_n[r]; i++) {
+            if (used[i])
+                continue;
+            const double* a = &q[kQ * (rule_first[r] + i)];
+            used[i] = true;
+            if (std::fabs(a[0]) < 1e-14 && std::fabs(a[1]) < 1e-14) {
+                if (center[r] < 0 || nc++)
+                    return fail(ctx, KEMCU_ECUDA, "rectangle rule %d: unexpected centroid node", rule_n[r]);
+                qc[center[r]] = a[5];
+                continue;
+            }
+            int j = i + 1;
+            for (; j < rule_n[r]; j++) {
+                const double* b = &q[kQ * (rule_first[r] + j)];
+                if (!used[j] && std::fabs(a[0] + b[0]) < 1e-13 && std::fabs(a[1] + b[1]) < 1e-13 && std::fabs(a[5] - b[5]) <= 1e-13 * std::fabs(a[5]))
+                    break;
+            }
+            if (j == rule_n[r] || np == pair_n[r])
+                return fail(ctx, KEMCU_ECUDA, "rectangle rule %d is not centrally symmetric", rule_n[r]);
+            used[j] = true;
+            for (int c = 0; c < kQ; c++)
+                qp[kQ * (pair_first[r] + np) + c] = a[c];
+            np++;
+        }
+        if (np != pair_n[r] || nc != (center[r] >= 0 ? 1 : 0))
+            return fail(ctx, KEMCU_ECUDA, "rectangle rule %d: unexpected node pairing", rule_n[r]);
+    }
+    KC(cudaMemcpyToSymbol(c_qp, qp.data(), qp.size() * sizeof(double)));
+    KC(cudaMemcpyToSymbol(c_qc, qc, sizeof qc));
     KC(cudaMemcpyToSymbol(c_gl, gl.data(), gl.size() * sizeof(double)));
     KC(cudaMemcpyToSymbol(c_k, &ctx->k, sizeof(Constants)));
     double rk[kStages][kStages];
