@@ -23,6 +23,13 @@ constexpr int kThreads = 128;
 #endif
 constexpr int kMinBlocks = KEMCU_MIN_BLOCKS;
 
+// Leading dimension of the assembled operator: rows padded to a multiple of 4 so that every
+// column starts on a 16-byte boundary in both the FP64 and the FP32 copy.
+__host__ __device__ __forceinline__ size_t op_ld(size_t n)
+{
+    return (n + 3) / 4 * 4;
+}
+
 struct Kahan
 {
     double s = 0., c = 0.;
@@ -380,8 +387,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) matvec_kernel(const doub
     }
 }
 
-// operator assembly: column-major dense A (A[j * n + i] = A(i, j)) for columns [j0, j1),
-// written in FP64 and, when a32 != nullptr, also rounded to FP32
+// operator assembly: column-major dense A (A[j * op_ld(n) + i] = A(i, j)) for columns
+// [j0, j1), written in FP64 and, when a32 != nullptr, also rounded to FP32
 template<bool MIXED>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) assemble_kernel(const double* __restrict__ rec, const TargetRec* __restrict__ tgt,
                                                             int n, int j0, int j1, double* __restrict__ a64,
@@ -410,7 +417,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) assemble_kernel(const do
             const int t0 = R.first(q), cnt = R.count(q);
             for (int j = 0; j < cnt; j++) {
                 const double a = entry<MIXED>(R.element(q, j), t, C);
-                const size_t idx = (size_t) (t0 + j - j0) * n + i;
+                const size_t idx = (size_t) (t0 + j - j0) * op_ld(n) + i;
                 if (a64)
                     a64[idx] = a;
                 if (a32)
@@ -422,48 +429,76 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) assemble_kernel(const do
     R.finish(ok, flag);
 }
 
-// dense matvec on the assembled column-major operator: y[r][i] = sum_j A[j*n+i] x[r][j].
-// Threads own rows i (coalesced column reads); the column range is split over gridDim.y.
-template<typename T>
-__global__ void __launch_bounds__(256) dense_matvec_kernel(const T* __restrict__ A, int n, const double* __restrict__ x,
-                                                           int nrhs, double* __restrict__ y, double* __restrict__ partial)
+// dense matvec on the assembled column-major operator (leading dimension ld):
+// y[r][i] = sum_j A[j*ld+i] x[r][j] for r < nrhs <= NR. A thread owns V = 16 B / sizeof(T)
+// consecutive rows and reads them with one 16-byte load per column (512 B per warp and
+// column, streamed past L1/L2 with evict-first hints); the column range is split over
+// gridDim.y. HBM-bound: 8 or 4 B per entry per call, whatever the number of right-hand sides.
+template<typename T, int NR>
+__global__ void __launch_bounds__(256) dense_matvec_kernel(const T* __restrict__ A, int n, size_t ld,
+                                                           const double* __restrict__ x, int nrhs,
+                                                           double* __restrict__ y, double* __restrict__ partial)
 {
-    __shared__ double s_x[kMaxRhs][256];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    constexpr int V = 16 / sizeof(T);
+    constexpr int kCols = 256;
+    __shared__ double s_x[NR][kCols];
+    const int row0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
     const int per = (n + gridDim.y - 1) / gridDim.y;
     const int e0 = blockIdx.y * per;
     const int e1 = min(n, e0 + per);
-    double acc[kMaxRhs];
+    double acc[NR][V];
 #pragma unroll
-    for (int r = 0; r < kMaxRhs; r++)
-        acc[r] = 0.;
-    for (int t0 = e0; t0 < e1; t0 += 256) {
-        const int cnt = min(256, e1 - t0);
+    for (int r = 0; r < NR; r++)
+#pragma unroll
+        for (int q = 0; q < V; q++)
+            acc[r][q] = 0.;
+    for (int t0 = e0; t0 < e1; t0 += kCols) {
+        const int cnt = min(kCols, e1 - t0);
         __syncthreads();
         for (int q = threadIdx.x; q < cnt; q += blockDim.x)
             for (int r = 0; r < nrhs; r++)
                 s_x[r][q] = x[(size_t) r * n + t0 + q];
         __syncthreads();
-        if (i < n) {
-            const T* col = A + (size_t) t0 * n + i;
+        if (row0 < n) {
+            const T* col = A + (size_t) t0 * ld + row0;
 #pragma unroll 8
             for (int j = 0; j < cnt; j++) {
-                const double a = (double) __ldcs(col + (size_t) j * n);
+                T v[V];
+                if constexpr (V == 4) {
+                    const float4 w = __ldcs(reinterpret_cast<const float4*>(col + (size_t) j * ld));
+                    v[0] = w.x;
+                    v[1] = w.y;
+                    v[2] = w.z;
+                    v[3] = w.w;
+                }
+                else {
+                    const double2 w = __ldcs(reinterpret_cast<const double2*>(col + (size_t) j * ld));
+                    v[0] = w.x;
+                    v[1] = w.y;
+                }
 #pragma unroll
-                for (int r = 0; r < kMaxRhs; r++)
-                    if (r < nrhs)
-                        acc[r] += a * s_x[r][j];
+                for (int r = 0; r < NR; r++) {
+                    if (r < nrhs) {
+                        const double xr = s_x[r][j];
+#pragma unroll
+                        for (int q = 0; q < V; q++)
+                            acc[r][q] = fma((double) v[q], xr, acc[r][q]);
+                    }
+                }
             }
         }
     }
-    if (i >= n)
-        return;
-    for (int r = 0; r < nrhs; r++) {
-        if (partial)
-            partial[((size_t) blockIdx.y * nrhs + r) * n + i] = acc[r];
-        else
-            y[(size_t) r * n + i] = acc[r];
-    }
+    for (int r = 0; r < nrhs; r++)
+#pragma unroll
+        for (int q = 0; q < V; q++) {
+            const int i = row0 + q;
+            if (i >= n)
+                break;
+            if (partial)
+                partial[((size_t) blockIdx.y * nrhs + r) * n + i] = acc[r][q];
+            else
+                y[(size_t) r * n + i] = acc[r][q];
+        }
 }
 
 }  // namespace kemcu

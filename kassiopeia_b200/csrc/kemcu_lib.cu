@@ -403,8 +403,10 @@ int apply_op(kemcu_ctx* ctx, int op, const double* d_x, double* d_y, int nrhs)
         }
         return KEMCU_OK;
     }
-    const size_t rows_blocks = (n + 255) / 256;
-    size_t split = std::max((size_t) 1, (size_t) ctx->num_sms * 4 / rows_blocks);
+    // dense operator: V rows per thread, enough CTAs for ~8 per SM, columns split to match
+    const size_t V = op == kDense64 ? 2 : 4;
+    const size_t rows_blocks = (n + 256 * V - 1) / (256 * V);
+    size_t split = std::max((size_t) 1, (size_t) ctx->num_sms * 8 / rows_blocks);
     split = std::min(split, (size_t) std::max(1, n / 256));
     double* partial = nullptr;
     if (split > 1) {
@@ -415,10 +417,19 @@ int apply_op(kemcu_ctx* ctx, int op, const double* d_x, double* d_y, int nrhs)
         partial = (double*) p;
     }
     dim3 grid((unsigned) rows_blocks, (unsigned) split);
-    if (op == kDense64)
-        dense_matvec_kernel<double><<<grid, 256, 0, ctx->stream>>>(ctx->d_a64, n, d_x, nrhs, d_y, partial);
-    else
-        dense_matvec_kernel<float><<<grid, 256, 0, ctx->stream>>>(ctx->d_a32, n, d_x, nrhs, d_y, partial);
+    const size_t ld = op_ld(n);
+    if (op == kDense64) {
+        if (nrhs == 1)
+            dense_matvec_kernel<double, 1><<<grid, 256, 0, ctx->stream>>>(ctx->d_a64, n, ld, d_x, nrhs, d_y, partial);
+        else
+            dense_matvec_kernel<double, kMaxRhs><<<grid, 256, 0, ctx->stream>>>(ctx->d_a64, n, ld, d_x, nrhs, d_y, partial);
+    }
+    else {
+        if (nrhs == 1)
+            dense_matvec_kernel<float, 1><<<grid, 256, 0, ctx->stream>>>(ctx->d_a32, n, ld, d_x, nrhs, d_y, partial);
+        else
+            dense_matvec_kernel<float, kMaxRhs><<<grid, 256, 0, ctx->stream>>>(ctx->d_a32, n, ld, d_x, nrhs, d_y, partial);
+    }
     KCHECK_LAUNCH();
     if (split > 1) {
         const size_t m = (size_t) nrhs * n;
@@ -433,7 +444,8 @@ int assemble(kemcu_ctx* ctx, bool want32)
     const size_t n = ctx->n;
     if (ctx->d_a64 && (!want32 || ctx->d_a32))
         return KEMCU_OK;
-    const size_t bytes64 = n * n * sizeof(double), bytes32 = want32 ? n * n * sizeof(float) : 0;
+    const size_t ld = op_ld(n);
+    const size_t bytes64 = ld * n * sizeof(double), bytes32 = want32 ? ld * n * sizeof(float) : 0;
     size_t budget = ctx->assembled_budget;
     if (budget == 0) {
         size_t fr = 0, tot = 0;
@@ -468,7 +480,7 @@ int assemble(kemcu_ctx* ctx, bool want32)
 // basis with two batched passes instead of j sequential ones. The j x j triangular solve
 // uses back-substitution (KGeneralizedMinimalResidual::UseBackSubstitution).
 // basis entries (n x (j+1)) up to which one CTA per RHS orthogonalises (arnoldi_small_kernel)
-constexpr size_t kArnoldiSmall = (size_t) 1 << 20;
+constexpr size_t kArnoldiSmall = (size_t) 1 << 16;
 
 int gmres_core(kemcu_ctx* ctx, int op, const double* d_b, double* d_x, int nrhs, double tol, int max_iter,
                int& iters, double& est, int& matvecs)
