@@ -267,6 +267,22 @@ def run_native(args, rank, world, dist):
     return res
 
 
+def profile_operator():
+    import kassiopeia_b200 as K
+    from kassiopeia_b200 import geometry as G
+
+    ctx = K.CUDAElectrostaticContext(int(os.environ.get("LOCAL_RANK", 0)))
+    mesh = G.coax(n_phi=60, n_z=120, n_cap_rings=8)
+    ctx.SetGeometry(mesh)
+    x = np.ones(mesh.n)
+    for prec in (K.MIXED, K.MIXED, K.MIXED, K.FP64, K.FP64):
+        ctx.Multiply(x, precision=prec, assembled=True)  # the first call assembles the operator
+        entry = 4 if prec == K.MIXED else 8
+        ms = ctx.last_kernel_ms
+        print(json.dumps({"operator": "dense " + ("FP32" if prec == K.MIXED else "FP64"), "n": mesh.n, "ms": ms,
+                          "GB/s": mesh.n * mesh.n * entry / (ms * 1e-3) / 1e9}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -278,7 +294,13 @@ def main():
                     help="profiling case for ncu: no solves (fixed charge density, no assembled operator) and "
                          "--points points; prints the same JSON line")
     ap.add_argument("--points", type=int, default=N_POINTS, help="gap points per GPU (default 1,000,000)")
+    ap.add_argument("--profile-operator", action="store_true",
+                    help="profiling case for ncu: assembled operator of a 16,320-element coax (2.1 GB FP64 + "
+                         "1.1 GB FP32), three FP32 and two FP64 dense matvecs; prints one JSON line per matvec")
     args = ap.parse_args()
+    if args.profile_operator:
+        profile_operator()
+        return
     globals()["N_POINTS"] = args.points
     if args.profile:
         args.quick = True
