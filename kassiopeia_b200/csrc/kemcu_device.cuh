@@ -603,44 +603,25 @@ template<bool POT, bool FIELD> __device__ __noinline__ Out4 line_analytic(const 
 // MIXED selects the Newton-refined hardware reciprocal square root for the cubature bands;
 // everything else is the same FP64 code. Triangles and rectangles have separate unrolled
 // cubature code (the element type is uniform across a warp, which evaluates one element).
-//
-// epi_far evaluates the numeric bands and returns false, without evaluating, for the
-// analytic near-field band (RWG polygons, analytic wire), which epi_near evaluates. Kernels
-// that stream many elements defer the near-field pairs of a tile to a second pass, so the
-// calls of the (non-inlined) analytic integrals stay out of the numeric loop.
-template<bool MIXED, bool POT, bool FIELD> __device__ __forceinline__ bool epi_far(const double* e, V3 P, Out4& o)
-{
-    const int band = band_of(e, P);
-    if (band == 0)
-        return false;
-    const int type = (int) e[rType];
-    if (type == kLineSegment)
-        o = band == 1 ? line_gauss<POT, FIELD>(e, P, 2, 8) : line_gauss<POT, FIELD>(e, P, 0, 2);
-    else if (type == kTriangle)
-        o = band == 1   ? cubq<33, kTri33, POT, FIELD, MIXED>(e, P)
-            : band == 2 ? cubq<12, kTri12, POT, FIELD, MIXED>(e, P)
-                        : cubq<7, kTri7, POT, FIELD, MIXED>(e, P);
-    else
-        o = band == 1   ? cubq_pairs<16, kPair33, 1, POT, FIELD, MIXED>(e, P)
-            : band == 2 ? cubq_pairs<6, kPair12, -1, POT, FIELD, MIXED>(e, P)
-                        : cubq_pairs<3, kPair7, 0, POT, FIELD, MIXED>(e, P);
-    return true;
-}
-
-template<bool POT, bool FIELD> __device__ __forceinline__ Out4 epi_near(const double* e, V3 P)
-{
-    const int type = (int) e[rType];
-    if (type == kLineSegment)
-        return line_analytic<POT, FIELD>(e, P);
-    return type == kTriangle ? rwg64<3, POT, FIELD>(e, P) : rwg64<4, POT, FIELD>(e, P);
-}
-
 template<bool MIXED, bool POT, bool FIELD> __device__ __forceinline__ Out4 epi(const double* e, V3 P)
 {
-    Out4 o;
-    if (epi_far<MIXED, POT, FIELD>(e, P, o))
-        return o;
-    return epi_near<POT, FIELD>(e, P);
+    const int band = band_of(e, P);
+    const int type = (int) e[rType];
+    if (type == kLineSegment) {
+        if (band == 0)
+            return line_analytic<POT, FIELD>(e, P);
+        return band == 1 ? line_gauss<POT, FIELD>(e, P, 2, 8) : line_gauss<POT, FIELD>(e, P, 0, 2);
+    }
+    if (band == 0)
+        return type == kTriangle ? rwg64<3, POT, FIELD>(e, P) : rwg64<4, POT, FIELD>(e, P);
+    if (type == kTriangle) {
+        if (band == 1)
+            return cubq<33, kTri33, POT, FIELD, MIXED>(e, P);
+        return band == 2 ? cubq<12, kTri12, POT, FIELD, MIXED>(e, P) : cubq<7, kTri7, POT, FIELD, MIXED>(e, P);
+    }
+    if (band == 1)
+        return cubq_pairs<16, kPair33, 1, POT, FIELD, MIXED>(e, P);
+    return band == 2 ? cubq_pairs<6, kPair12, -1, POT, FIELD, MIXED>(e, P) : cubq_pairs<3, kPair7, 0, POT, FIELD, MIXED>(e, P);
 }
 
 }  // namespace kemcu
