@@ -404,39 +404,35 @@ int apply_op(kemcu_ctx* ctx, int op, const double* d_x, double* d_y, int nrhs)
         return KEMCU_OK;
     }
     // dense operator: V rows per thread, enough CTAs for ~8 per SM, columns split to match
+    // V rows per thread; one wave of resident CTAs, the column range split to fill it
     const size_t V = op == kDense64 ? 2 : 4;
     const size_t rows_blocks = (n + 256 * V - 1) / (256 * V);
-    size_t split = std::max((size_t) 1, (size_t) ctx->num_sms * 8 / rows_blocks);
-    split = std::min(split, (size_t) std::max(1, n / 256));
-    double* partial = nullptr;
-    if (split > 1) {
-        void* p;
-        int rc = ensure(ctx, sPartial, split * nrhs * n * sizeof(double), &p);
-        if (rc)
-            return rc;
-        partial = (double*) p;
-    }
-    dim3 grid((unsigned) rows_blocks, (unsigned) split);
-    const size_t ld = op_ld(n);
-    if (op == kDense64) {
-        if (nrhs == 1)
-            dense_matvec_kernel<double, 1><<<grid, 256, 0, ctx->stream>>>(ctx->d_a64, n, ld, d_x, nrhs, d_y, partial);
-        else
-            dense_matvec_kernel<double, kMaxRhs><<<grid, 256, 0, ctx->stream>>>(ctx->d_a64, n, ld, d_x, nrhs, d_y, partial);
-    }
-    else {
-        if (nrhs == 1)
-            dense_matvec_kernel<float, 1><<<grid, 256, 0, ctx->stream>>>(ctx->d_a32, n, ld, d_x, nrhs, d_y, partial);
-        else
-            dense_matvec_kernel<float, kMaxRhs><<<grid, 256, 0, ctx->stream>>>(ctx->d_a32, n, ld, d_x, nrhs, d_y, partial);
-    }
-    KCHECK_LAUNCH();
-    if (split > 1) {
-        const size_t m = (size_t) nrhs * n;
-        reduce_splits<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(partial, (int) split, m, d_y);
+    auto launch = [&](auto kernel, const auto* A) -> int {
+        int per_sm = 0;
+        KC(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0));
+        size_t split = std::max((size_t) 1, (size_t) ctx->num_sms * std::max(1, per_sm) / rows_blocks);
+        split = std::min(split, (size_t) std::max(1, n / 256));
+        double* partial = nullptr;
+        if (split > 1) {
+            void* p;
+            int rc = ensure(ctx, sPartial, split * nrhs * n * sizeof(double), &p);
+            if (rc)
+                return rc;
+            partial = (double*) p;
+        }
+        dim3 grid((unsigned) rows_blocks, (unsigned) split);
+        kernel<<<grid, 256, 0, ctx->stream>>>(A, n, op_ld(n), d_x, nrhs, d_y, partial);
         KCHECK_LAUNCH();
-    }
-    return KEMCU_OK;
+        if (split > 1) {
+            const size_t m = (size_t) nrhs * n;
+            reduce_splits<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(partial, (int) split, m, d_y);
+            KCHECK_LAUNCH();
+        }
+        return KEMCU_OK;
+    };
+    if (op == kDense64)
+        return nrhs == 1 ? launch(dense_matvec_kernel<double, 1>, ctx->d_a64) : launch(dense_matvec_kernel<double, kMaxRhs>, ctx->d_a64);
+    return nrhs == 1 ? launch(dense_matvec_kernel<float, 1>, ctx->d_a32) : launch(dense_matvec_kernel<float, kMaxRhs>, ctx->d_a32);
 }
 
 int assemble(kemcu_ctx* ctx, bool want32)
