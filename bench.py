@@ -283,6 +283,20 @@ def profile_operator():
                           "GB/s": mesh.n * mesh.n * entry / (ms * 1e-3) / 1e9}), flush=True)
 
 
+def profile_tracker():
+    import kassiopeia_b200 as K
+    from kassiopeia_b200 import geometry as G
+
+    ctx = K.CUDAElectrostaticContext(int(os.environ.get("LOCAL_RANK", 0)))
+    ctx.SetGeometry(G.icosphere(3))
+    ctx.Solve(tol=TOL, mode=K.SOLVE_ASSEMBLED)
+    E = G.electrons(65536, seed=99)
+    for prec, name in ((K.FP64, "FP64"), (K.MIXED, "MIXED")):
+        _, _, _, ts = ctx.TrackRK8(E, 1e-11, 10000, step_budget=8, sphere_radius=1.0, precision=prec)
+        print(json.dumps({"tracker": name, "tracks": len(E), "steps": ts["steps"], "seconds": ts["seconds"],
+                          "track_steps_per_s": ts["steps"] / ts["seconds"]}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -297,9 +311,15 @@ def main():
     ap.add_argument("--profile-operator", action="store_true",
                     help="profiling case for ncu: assembled operator of a 16,320-element coax (2.1 GB FP64 + "
                          "1.1 GB FP32), three FP32 and two FP64 dense matvecs; prints one JSON line per matvec")
+    ap.add_argument("--profile-tracker", action="store_true",
+                    help="profiling case for ncu: 65,536 electrons in the field of the 1,280-triangle sphere, "
+                         "one persistent RK8 launch of 8 steps per track, FP64 then MIXED; prints track steps/s")
     args = ap.parse_args()
     if args.profile_operator:
         profile_operator()
+        return
+    if args.profile_tracker:
+        profile_tracker()
         return
     globals()["N_POINTS"] = args.points
     if args.profile:

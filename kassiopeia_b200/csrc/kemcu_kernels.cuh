@@ -135,27 +135,28 @@ __device__ __forceinline__ void split_range(int first, int last, int& e0, int& e
     e1 = min(last, e0 + per);
 }
 
-// The ring: kPipe stages of kFieldTile element records plus SIDE doubles of per-element side
-// data (charge densities, matvec operands) per element, stored by the filling warp's lanes.
-// RingStorage lives in shared memory; ElementRing (registers) holds the CTA's element slice
-// and a reference to it.
-template<int SIDE> struct RingStorage
+// The ring: NP stages (kPipe by default) of kFieldTile element records plus SIDE doubles of
+// per-element side data (charge densities, matvec operands) per element, stored by the filling
+// warp's lanes. RingStorage lives in shared memory; ElementRing (registers) holds the CTA's
+// element slice and a reference to it. A CYCLIC ring passes over the slice again and again
+// (the tracker's stage evaluations) and keeps prefetching until finish().
+template<int SIDE, int NP = kPipe> struct RingStorage
 {
-    double rec[kPipe][kFieldTile * rRecSize];
-    double side[kPipe][SIDE > 0 ? SIDE : 1][kFieldTile];
-    unsigned long long full[kPipe];
-    unsigned rel[kPipe], used[kPipe];
+    double rec[NP][kFieldTile * rRecSize];
+    double side[NP][SIDE > 0 ? SIDE : 1][kFieldTile];
+    unsigned long long full[NP];
+    unsigned rel[NP], used[NP];
 };
 
-template<int SIDE> struct ElementRing
+template<int SIDE, int NP = kPipe, bool CYCLIC = false> struct ElementRing
 {
-    RingStorage<SIDE>& S;
+    RingStorage<SIDE, NP>& S;
     int e0, e1;  // this CTA's element slice
 
-    __device__ __forceinline__ ElementRing(RingStorage<SIDE>& storage, int first, int last) : S(storage)
+    __device__ __forceinline__ ElementRing(RingStorage<SIDE, NP>& storage, int first, int last) : S(storage)
     {
         split_range(first, last, e0, e1);
-        if (threadIdx.x < kPipe) {
+        if (threadIdx.x < NP) {
             mbar_init(&S.full[threadIdx.x], 32);
             S.rel[threadIdx.x] = 0u;
             S.used[threadIdx.x] = 0u;
@@ -167,9 +168,10 @@ template<int SIDE> struct ElementRing
     {
         return (e1 - e0 + kFieldTile - 1) / kFieldTile;
     }
+    // first element of tile i of the sequence (CYCLIC: the slice is passed over repeatedly)
     __device__ __forceinline__ int first(int i) const
     {
-        return e0 + i * kFieldTile;
+        return e0 + (CYCLIC ? i % tiles() : i) * kFieldTile;
     }
     __device__ __forceinline__ int count(int i) const
     {
@@ -177,17 +179,17 @@ template<int SIDE> struct ElementRing
     }
     __device__ __forceinline__ const double* element(int i, int j) const
     {
-        return S.rec[i % kPipe] + j * rRecSize;
+        return S.rec[i % NP] + j * rRecSize;
     }
     __device__ __forceinline__ double side(int i, int k, int j) const
     {
-        return S.side[i % kPipe][k][j];
+        return S.side[i % NP][k][j];
     }
-    // fill stage i % kPipe with tile i: called by all 32 lanes of one warp;
+    // fill stage i % NP with tile i: called by all 32 lanes of one warp;
     // side_fn(double (*side)[kFieldTile], int t0, int cnt, int lane) stores the side data
     template<class F> __device__ __forceinline__ void fill(const double* __restrict__ src, int i, F side_fn)
     {
-        const int s = i % kPipe, t0 = first(i), cnt = count(i), lane = threadIdx.x & 31;
+        const int s = i % NP, t0 = first(i), cnt = count(i), lane = threadIdx.x & 31;
         side_fn(S.side[s], t0, cnt, lane);
         if (lane == 0) {
             S.used[s]++;
@@ -202,17 +204,17 @@ template<int SIDE> struct ElementRing
     template<class F> __device__ __forceinline__ void prologue(const double* __restrict__ src, F side_fn)
     {
         if (threadIdx.x < 32)
-            for (int i = 0; i < min(kPipe, tiles()); i++)
+            for (int i = 0; i < (CYCLIC ? NP : min(NP, tiles())); i++)
                 fill(src, i, side_fn);
     }
     __device__ __forceinline__ bool wait(int i)
     {
-        return mbar_wait(&S.full[i % kPipe], (unsigned) (i / kPipe) & 1u);
+        return mbar_wait(&S.full[i % NP], (unsigned) (i / NP) & 1u);
     }
     // whole warp: release tile i; the warp that releases a stage last refills it
     template<class F> __device__ __forceinline__ void release(const double* __restrict__ src, int i, F side_fn)
     {
-        const int s = i % kPipe;
+        const int s = i % NP;
         __syncwarp();
         unsigned last = 0u;
         if ((threadIdx.x & 31) == 0) {
@@ -220,9 +222,9 @@ template<int SIDE> struct ElementRing
             last = atomicAdd(&S.rel[s], 1u) % (blockDim.x >> 5) == (blockDim.x >> 5) - 1u;
         }
         last = __shfl_sync(0xffffffffu, last, 0);
-        if (last && i + kPipe < tiles()) {
+        if (last && (CYCLIC || i + NP < tiles())) {
             __threadfence_block();
-            fill(src, i + kPipe, side_fn);
+            fill(src, i + NP, side_fn);
         }
     }
     // after the tile loop (all threads): report a timed-out wait in flag (|= 2) and wait,
@@ -232,7 +234,7 @@ template<int SIDE> struct ElementRing
         if (!ok && (threadIdx.x & 31) == 0)
             atomicOr(flag, 2);
         __syncthreads();
-        if (threadIdx.x < kPipe && S.used[threadIdx.x] > 0u)
+        if (threadIdx.x < NP && S.used[threadIdx.x] > 0u)
             mbar_wait(&S.full[threadIdx.x], (S.used[threadIdx.x] - 1u) & 1u);
     }
 };

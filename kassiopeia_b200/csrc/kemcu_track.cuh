@@ -8,14 +8,14 @@
 //   d/dt (t, s, x, p) = (1, |v|, v, q E(x)),  v = p / (m gamma),  gamma = sqrt(1 + p^2 / (m c)^2)
 // with E(x) the Kahan-summed direct sum of KIntegratingFieldSolver::ElectricField.
 //
-// Layout: a CTA owns kTrackSlots slots (one per thread). All slots of a CTA advance in lock
-// step, stage by stage, so every stage's 128 field evaluations share one pass of the element
-// records through shared memory. The 13 stage derivatives of each slot live in shared memory.
-// A slot whose track ends (electrode hit, leaving the volume, step limit, non-finite state) or
-// has taken `budget` steps in this launch writes it back and takes the next track index from a
-// global work counter, so tracks of very different lengths keep every slot busy and one launch
-// advances every listed track by at most `budget` steps; unfinished tracks stay active for the
-// next launch.
+// Layout: a CTA owns kTrackSlots slots (one per thread). Every RK stage of all slots of a CTA
+// is one pass over the element records, streamed through a cyclic shared-memory ring
+// (ElementRing, bulk copies; no CTA barrier per tile, so warps drift up to a tile apart); the
+// 13 stage derivatives of each slot live in shared memory. A slot whose track ends (electrode
+// hit, leaving the volume, step limit, non-finite state) or has taken `budget` steps in this
+// launch writes it back and takes the next track index from a global work counter, so tracks
+// of very different lengths keep every slot busy and one launch advances every listed track
+// by at most `budget` steps; unfinished tracks stay active for the next launch.
 #pragma once
 
 #include "kemcu_kernels.cuh"
@@ -25,7 +25,8 @@ namespace kemcu
 
 constexpr int kTrackSlots = 128;
 constexpr int kStages = 13;
-constexpr int kTrackTile = 32;  // element records per tile (the stage derivatives take most shared memory)
+constexpr int kTrackPipe = 3;  // ring stages (the stage derivatives take most shared memory)
+constexpr int kTrackK = 6;     // stored per stage and slot: v (3), q E (3)
 
 // Butcher coefficients a[s][k] (row s gives stage value s from derivatives 0..s; row 12 is
 // the final combination), the 13-stage eighth-order scheme of KSMathRK8.h:139-226
@@ -68,21 +69,30 @@ struct TrackParams
 };
 
 // state: n x 8; steps, status: n; list: n_list track indices to work on; next: work counter;
-// done_steps: total steps taken (for statistics)
+// done_steps: total steps taken (for statistics); flag |= 2 if a ring wait timed out.
+// Dynamic shared memory: kStages * kTrackK * kTrackSlots doubles.
 template<bool MIXED>
 __global__ void __launch_bounds__(kTrackSlots) rk8_tracker_kernel(const double* __restrict__ rec, const double* __restrict__ sigma,
                                                                   int n_elem, double* __restrict__ state,
                                                                   int* __restrict__ steps, int* __restrict__ status,
                                                                   const int* __restrict__ list, unsigned* __restrict__ next,
                                                                   unsigned long long* __restrict__ done_steps,
-                                                                  TrackParams prm)
+                                                                  TrackParams prm, int* __restrict__ flag)
 {
-    extern __shared__ __align__(16) double smem[];
-    double* s_rec = smem;                               // kTrackTile * rRecSize
-    double* s_sig = s_rec + kTrackTile * rRecSize;      // kTrackTile
-    double* s_k = s_sig + kTrackTile;                        // [kStages][7][kTrackSlots]: v(3), F(3), |v|
+    extern __shared__ __align__(16) double s_k[];  // [kStages][kTrackK][kTrackSlots]
+    __shared__ __align__(128) RingStorage<1, kTrackPipe> S;
+    __shared__ int s_abort;
     const int tid = threadIdx.x;
-    auto K = [&](int st, int c) -> double& { return s_k[(st * 7 + c) * kTrackSlots + tid]; };
+    auto K = [&](int st, int c) -> double& { return s_k[(st * kTrackK + c) * kTrackSlots + tid]; };
+    if (tid == 0)
+        s_abort = 0;
+    ElementRing<1, kTrackPipe, true> R(S, 0, n_elem);  // synchronises the CTA
+    auto side = [&](double (*sd)[kFieldTile], int t0, int cnt, int lane) {
+        if (lane < cnt)
+            sd[0][lane] = sigma[t0 + lane];
+    };
+    R.prologue(rec, side);
+    const int ntiles = R.tiles();
 
     int track = -1, tsteps = 0;
     double y[8];
@@ -100,8 +110,15 @@ __global__ void __launch_bounds__(kTrackSlots) rk8_tracker_kernel(const double* 
     };
     pull();
     unsigned long long my_steps = 0;
-    // every iteration is one RK8 step of all busy slots; ends when the list is exhausted
-    while (__syncthreads_or(track >= 0)) {
+    int gi = 0;  // position in the ring's tile sequence
+    bool ok = true;
+    // every iteration is one RK8 step of all busy slots; ends when the list is exhausted (or a
+    // ring wait of some warp timed out)
+    while (true) {
+        const int any = __syncthreads_or(track >= 0);
+        if (!any || s_abort)
+            break;
+        double ds = 0.;  // sum over stages of a[12][k] |v_k|
         for (int st = 0; st < kStages; st++) {
             // stage position and momentum: value_{st-1} = y0 + dt sum_k a[st-1][k] k_k
             V3 X = v3(y[2], y[3], y[4]), Pm = v3(y[5], y[6], y[7]);
@@ -119,45 +136,48 @@ __global__ void __launch_bounds__(kTrackSlots) rk8_tracker_kernel(const double* 
                 X = v3(y[2] + prm.dt * sx, y[3] + prm.dt * sy, y[4] + prm.dt * sz);
                 Pm = v3(y[5] + prm.dt * px, y[6] + prm.dt * py, y[7] + prm.dt * pz);
             }
-            // E(X): lock-step pass of all elements through shared memory
+            // E(X): one pass of all elements through the ring
             Kahan ex, ey, ez;
-            for (int t0 = 0; t0 < n_elem; t0 += kTrackTile) {
-                const int cnt = min(kTrackTile, n_elem - t0);
-                __syncthreads();
-                load_tile(s_rec, rec, t0, cnt);
-                if (tid < cnt)
-                    s_sig[tid] = sigma[t0 + tid];
-                __syncthreads();
-                if (track >= 0) {
-                    for (int j = 0; j < cnt; j++) {
-                        const Out4 r = epi<MIXED, false, true>(s_rec + j * rRecSize, X);
-                        const double sg = s_sig[j];
-                        ex.add(r.ex * sg);
-                        ey.add(r.ey * sg);
-                        ez.add(r.ez * sg);
+            if (ok) {
+                for (int i = 0; i < ntiles; i++, gi++) {
+                    if (!__all_sync(0xffffffffu, R.wait(gi))) {
+                        ok = false;
+                        s_abort = 1;
+                        break;
                     }
+                    if (track >= 0) {
+                        const int cnt = R.count(gi);
+                        for (int j = 0; j < cnt; j++) {
+                            const Out4 r = epi<MIXED, false, true>(R.element(gi, j), X);
+                            const double sg = R.side(gi, 0, j);
+                            ex.add(r.ex * sg);
+                            ey.add(r.ey * sg);
+                            ez.add(r.ez * sg);
+                        }
+                    }
+                    R.release(rec, gi, side);
                 }
             }
             if (track >= 0) {
                 const double p2 = dot(Pm, Pm);
                 const double gam = sqrt(1. + p2 / (prm.mass * prm.mass * prm.c2));
                 const double inv = 1. / (prm.mass * gam);
-                K(st, 0) = inv * Pm.x;
-                K(st, 1) = inv * Pm.y;
-                K(st, 2) = inv * Pm.z;
+                const double vx = inv * Pm.x, vy = inv * Pm.y, vz = inv * Pm.z;
+                K(st, 0) = vx;
+                K(st, 1) = vy;
+                K(st, 2) = vz;
                 K(st, 3) = prm.charge * ex.s;
                 K(st, 4) = prm.charge * ey.s;
                 K(st, 5) = prm.charge * ez.s;
-                K(st, 6) = sqrt(K(st, 0) * K(st, 0) + K(st, 1) * K(st, 1) + K(st, 2) * K(st, 2));
+                ds += c_rk8[kStages - 1][st] * sqrt(vx * vx + vy * vy + vz * vz);
             }
         }
-        if (track >= 0) {
+        if (track >= 0 && ok) {
             // final combination (row 12) for t (derivative 1), s (|v|), x and p
-            double dtt = 0., ds = 0., d[6] = {0., 0., 0., 0., 0., 0.};
+            double dtt = 0., d[6] = {0., 0., 0., 0., 0., 0.};
             for (int k = 0; k < kStages; k++) {
                 const double a = c_rk8[kStages - 1][k];
                 dtt += a;
-                ds += a * K(k, 6);
                 for (int c = 0; c < 6; c++)
                     d[c] += a * K(k, c);
             }
@@ -191,6 +211,7 @@ __global__ void __launch_bounds__(kTrackSlots) rk8_tracker_kernel(const double* 
             }
         }
     }
+    R.finish(ok, flag);
     atomicAdd(done_steps, my_steps);
 }
 
