@@ -152,6 +152,28 @@ int kemcu_gmres(kemcu_ctx* ctx, const double* b, double* x, int n_rhs, double re
                 kemcu_solve_stats* stats);
 void kemcu_set_iteration_callback(kemcu_ctx* ctx, kemcu_iteration_callback cb, void* user);
 
+/* ---- Robin Hood charge-density solve (KRobinHood<double, KRobinHood_SingleThread>::Solve,
+        KRobinHood.hh:61-104; KRobinHood_SingleThread.hh:59-120) ----
+   Repeatedly picks the element with the largest |residual| (first index on ties), sets its
+   charge density so that this residual vanishes (correction r_k / A(k, k)) and updates the
+   residual with column k of the operator. Every check_interval sub-iterations (0 = n, the
+   reference default) the relative residual |b - A x|_inf / |b|_inf is evaluated; the solve
+   ends when it is <= rel_tol (after finishing that sub-iteration, as the reference does).
+   b: n values or NULL for the boundary values; x: n values, in: initial guess (as the
+   reference, A x is applied when |x|_inf > 1e-16), out: solution, also stored as the
+   context's sigma. assembled != 0 reads the columns from the assembled FP64 operator (built
+   on first use), else computes them on the fly. Returns KEMCU_ENOTCONVERGED after
+   max_subiterations (0 = unlimited) or when the iteration callback asks to stop (it is
+   called after every residual check with the check count and the relative residual). */
+typedef struct {
+    long long subiterations; /* single-element corrections applied */
+    int iterations;          /* residual checks (KIterativeSolver::GetIteration) */
+    double rel_residual;     /* |b - A x|_inf / |b|_inf at the last check */
+    double seconds;          /* device time of the solve */
+} kemcu_rh_stats;
+int kemcu_robin_hood(kemcu_ctx* ctx, const double* b, double* x, double rel_tol, int check_interval,
+                     long long max_subiterations, int assembled, kemcu_rh_stats* stats);
+
 /* ---- batched exact-trajectory RK8 tracking in the electrostatic field (KSMathRK8::Integrate,
         Kassiopeia/Math/Include/KSMathRK8.h:45-226; KSTrajTermPropagation::Differentiate,
         KSTrajTermPropagation.cxx:25-35) ----

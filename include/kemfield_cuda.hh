@@ -253,4 +253,32 @@ class KCUDAChargeDensitySolver
     int fMaxIterations, fMode;
 };
 
+// KRobinHoodChargeDensitySolver analogue (KRobinHood<double>::Solve, KRobinHood.hh:61-104):
+// Robin Hood on the device, starting from the charge densities the container holds
+class KCUDARobinHoodChargeDensitySolver
+{
+  public:
+    KCUDARobinHoodChargeDensitySolver(double tolerance = 1e-8, int check_interval = 0, bool assembled = false) :
+        fTolerance(tolerance),
+        fCheckInterval(check_interval),
+        fAssembled(assembled)
+    {}
+    kemcu_rh_stats Solve(KCUDASurfaceContainer& container) const
+    {
+        std::vector<double> x(container.size(), 0.);
+        container.WriteBasisData();
+        KCUDACheck(container.Context(), kemcu_get_sigma(container.Context(), x.data()));
+        kemcu_rh_stats st{};
+        KCUDACheck(container.Context(), kemcu_robin_hood(container.Context(), nullptr, x.data(), fTolerance,
+                                                         fCheckInterval, 0, fAssembled ? 1 : 0, &st));
+        container.ReadBasisData();
+        return st;
+    }
+
+  private:
+    double fTolerance;
+    int fCheckInterval;
+    bool fAssembled;
+};
+
 }  // namespace KEMField

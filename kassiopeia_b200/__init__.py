@@ -174,6 +174,21 @@ class CUDAElectrostaticContext:
             self._check(rc)
         return x, stats
 
+    def SolveRobinHood(self, b=None, tol=1e-8, x0=None, check_interval=0, max_subiterations=0, assembled=False,
+                       raise_on_failure=True):
+        """Robin Hood charge-density solve (KRobinHood<double>::Solve); returns (x, stats dict).
+        b: None (boundary values) or [n]; x0: initial guess (zeros by default)."""
+        x = np.zeros(self.n) if x0 is None else np.ascontiguousarray(x0, np.float64).copy()
+        bp = None if b is None else _d(np.ascontiguousarray(b, np.float64))
+        st = N.RhStats()
+        rc = N.lib().kemcu_robin_hood(self._h, bp, _d(x), tol, check_interval, max_subiterations, int(bool(assembled)),
+                                      C.byref(st))
+        stats = {k: getattr(st, k) for k, _ in N.RhStats._fields_}
+        stats["status"] = rc
+        if rc != N.OK and raise_on_failure:
+            self._check(rc)
+        return x, stats
+
     # -- tracking
     def TrackRK8(self, state, dt, max_steps, steps=None, status=None, step_budget=0, charge=None, mass=None,
                  sphere_radius=0.0, max_radius=0.0, precision=FP64):

@@ -40,6 +40,11 @@ class SolveStats(C.Structure):
                 ("rel_residual", C.c_double), ("rel_residual_estimate", C.c_double), ("seconds", C.c_double)]
 
 
+class RhStats(C.Structure):
+    _fields_ = [("subiterations", C.c_longlong), ("iterations", C.c_int), ("rel_residual", C.c_double),
+                ("seconds", C.c_double)]
+
+
 class HitModel(C.Structure):
     _fields_ = [("sphere_radius", C.c_double), ("max_radius", C.c_double)]
 
@@ -93,6 +98,7 @@ def lib():
     L.kemcu_matvec.argtypes = [vp, _dp, _dp, C.c_int, C.c_int, C.c_int]
     L.kemcu_gmres.argtypes = [vp, _dp, _dp, C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(SolveStats)]
     L.kemcu_set_iteration_callback.argtypes = [vp, ITER_CB, C.c_void_p]
+    L.kemcu_robin_hood.argtypes = [vp, _dp, _dp, C.c_double, C.c_int, C.c_longlong, C.c_int, C.POINTER(RhStats)]
     L.kemcu_set_iteration_callback.restype = None
     L.kemcu_track_rk8.argtypes = [vp, _dp, _ip, _ip, C.c_size_t, C.c_double, C.c_int, C.c_int, C.c_double,
                                   C.c_double, C.POINTER(HitModel), C.c_int, C.POINTER(TrackStats)]

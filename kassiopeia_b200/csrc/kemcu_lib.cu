@@ -10,6 +10,7 @@
 #include "kemcu_tables.cuh"
 #include "kemcu_track.cuh"
 #include "kemcu_adjoint.cuh"
+#include "kemcu_robinhood.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 
@@ -1252,3 +1253,4 @@ int kemcu_rule_nodes(int which, double* out)
 
 #include "kemcu_track_host.inc"
 #include "kemcu_adjoint_host.inc"
+#include "kemcu_robinhood_host.inc"

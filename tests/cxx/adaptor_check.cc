@@ -9,6 +9,7 @@
 #include "KElectrostaticBoundaryIntegratorFactory.hh"
 #include "KElectrostaticIntegratingFieldSolver.hh"
 #include "KGeneralizedMinimalResidual.hh"
+#include "KRobinHood.hh"
 #include "KSimpleIterativeKrylovSolver.hh"
 #include "KSurface.hh"
 #include "KSurfaceContainer.hh"
@@ -128,6 +129,26 @@ int main()
         std::printf("reference GMRES on the CUDA matrix: %u iterations, estimate %.3e\n", S.GetIteration(),
                     S.ResidualNorm());
         failures += !(S.ResidualNorm() < 1e-10);
+
+        // Robin Hood: the reference's KRobinHood on its own matrix vs the CUDA solver, both from 0
+        KSimpleVector<double> xr(Aref.Dimension());
+        for (unsigned i = 0; i < xr.Dimension(); i++)
+            xr[i] = 0.;
+        KRobinHood<double> rh;
+        rh.SetTolerance(1e-8);
+        rh.Solve(Aref, xr, b);
+        for (unsigned i = 0; i < container.size(); i++)
+            dynamic_cast<KElectrostaticBasis*>(container[i]->GetBasis())->GetSolution() = 0.;
+        kemcu_rh_stats rs = KCUDARobinHoodChargeDensitySolver(1e-8).Solve(gpu);
+        double wr = 0., nr = 0.;
+        for (unsigned i = 0; i < container.size(); i++) {
+            const double g = dynamic_cast<KElectrostaticBasis*>(container[i]->GetBasis())->GetSolution();
+            wr = std::max(wr, std::fabs(g - xr(i)));
+            nr = std::max(nr, std::fabs(xr(i)));
+        }
+        std::printf("Robin Hood: reference %u checks, CUDA %d checks (%lld corrections), max relative difference "
+                    "%.3e\n", rh.GetIteration(), rs.iterations, rs.subiterations, wr / nr);
+        failures += !(wr / nr < 1e-6 && std::abs((int) rh.GetIteration() - rs.iterations) <= 1);
     }
     catch (std::exception& e) {
         std::printf("exception: %s\n", e.what());

@@ -21,6 +21,10 @@ Fixtures:
                  full boundary-integral matrix, right-hand side, GMRES solution
   coax_small     reduced coax (960 rectangles + 288 cap triangles): sigma and gap field
   rk8            4 electrons x 40 RK8 steps of 1e-11 s in the icosphere_L2 field
+  robinhood      KRobinHood<double> (default residual-check interval, tolerances 1e-8 and
+                 1e-10) on the icosphere_L2 and mixed_small meshes: sigma, iterations, residual
+
+Usage: python tests/golden/make_golden.py [fixture ...]   (default: all)
 """
 
 from __future__ import annotations
@@ -204,12 +208,25 @@ def adjoint():
          vertices=verts, **mesh_arrays(m))
 
 
+def robinhood():
+    from oracle import golden
+
+    out = {}
+    for name in ("icosphere_L2", "mixed_small"):
+        m = golden.mesh_from(golden.load(name))
+        p = ref.RefProblem(m)
+        for tol in (1e-8, 1e-10):
+            x, it, r = p.robinhood(tol)
+            key = f"{name}_{tol:.0e}"
+            out[key + "_sigma"] = x
+            out[key + "_iterations"] = np.array(it)
+            out[key + "_residual"] = np.array(r)
+    save("robinhood", **out)
+
+
+FIXTURES = {f.__name__: f for f in (rules, integrators, lines, icosphere, mixed_small, coax_small, rk8, adjoint,
+                                     robinhood)}
+
 if __name__ == "__main__":
-    rules()
-    integrators()
-    lines()
-    icosphere()
-    mixed_small()
-    coax_small()
-    rk8()
-    adjoint()
+    for name in sys.argv[1:] or list(FIXTURES):
+        FIXTURES[name]()
