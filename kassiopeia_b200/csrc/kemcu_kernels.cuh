@@ -381,7 +381,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) matvec_kernel(const doub
     R.finish(ok, flag);
     if (!active)
         return;
-    for (int r = 0; r < nrhs; r++) {
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        if (r >= nrhs)
+            break;
         if (partial)
             partial[((size_t) blockIdx.y * nrhs + r) * n + i] = acc[r].s;
         else
@@ -432,18 +435,47 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) assemble_kernel(const do
 }
 
 // dense matvec on the assembled column-major operator (leading dimension ld):
-// y[r][i] = sum_j A[j*ld+i] x[r][j] for r < nrhs <= NR. A thread owns V = 16 B / sizeof(T)
-// consecutive rows and reads them with one 16-byte load per column (512 B per warp and
-// column, streamed past L1/L2 with evict-first hints); the column range is split over
-// gridDim.y. HBM-bound: 8 or 4 B per entry per call, whatever the number of right-hand sides.
+// y[r][i] = sum_j A[j*ld+i] x[r][j] for r < nrhs <= NR. A thread owns V consecutive rows
+// (dense_rows<T, NR>: one 16-byte load per column for a single right-hand side, 8 bytes for
+// several, which keeps the NR x V accumulators in registers at full occupancy), entries are
+// streamed past L1/L2 with evict-first loads; the column range is split over gridDim.y.
+// HBM-bound: 8 or 4 B per entry per call, whatever the number of right-hand sides.
+template<typename T, int NR> __host__ __device__ constexpr int dense_rows()
+{
+    return (NR == 1 ? 16 : 8) / (int) sizeof(T);
+}
+
+template<typename T, int V> __device__ __forceinline__ void load_rows(const T* p, double* o)
+{
+    if constexpr (sizeof(T) == 4 && V == 4) {
+        const float4 w = __ldcs(reinterpret_cast<const float4*>(p));
+        o[0] = w.x;
+        o[1] = w.y;
+        o[2] = w.z;
+        o[3] = w.w;
+    }
+    else if constexpr (sizeof(T) == 4 && V == 2) {
+        const float2 w = __ldcs(reinterpret_cast<const float2*>(p));
+        o[0] = w.x;
+        o[1] = w.y;
+    }
+    else if constexpr (V == 2) {
+        const double2 w = __ldcs(reinterpret_cast<const double2*>(p));
+        o[0] = w.x;
+        o[1] = w.y;
+    }
+    else
+        o[0] = __ldcs(p);
+}
+
 template<typename T, int NR>
 __global__ void __launch_bounds__(256) dense_matvec_kernel(const T* __restrict__ A, int n, size_t ld,
                                                            const double* __restrict__ x, int nrhs,
                                                            double* __restrict__ y, double* __restrict__ partial)
 {
-    constexpr int V = 16 / sizeof(T);
+    constexpr int V = dense_rows<T, NR>();
     constexpr int kCols = 256;
-    __shared__ double s_x[NR][kCols];
+    __shared__ __align__(16) double s_x[kCols][NR];  // the operand values of one column side by side
     const int row0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
     const int per = (n + gridDim.y - 1) / gridDim.y;
     const int e0 = blockIdx.y * per;
@@ -457,40 +489,33 @@ __global__ void __launch_bounds__(256) dense_matvec_kernel(const T* __restrict__
     for (int t0 = e0; t0 < e1; t0 += kCols) {
         const int cnt = min(kCols, e1 - t0);
         __syncthreads();
-        for (int q = threadIdx.x; q < cnt; q += blockDim.x)
-            for (int r = 0; r < nrhs; r++)
-                s_x[r][q] = x[(size_t) r * n + t0 + q];
+        for (int q = threadIdx.x; q < cnt * NR; q += blockDim.x) {
+            const int j = q / NR, r = q % NR;
+            s_x[j][r] = r < nrhs ? x[(size_t) r * n + t0 + j] : 0.;
+        }
         __syncthreads();
         if (row0 < n) {
             const T* col = A + (size_t) t0 * ld + row0;
 #pragma unroll 8
             for (int j = 0; j < cnt; j++) {
-                T v[V];
-                if constexpr (V == 4) {
-                    const float4 w = __ldcs(reinterpret_cast<const float4*>(col + (size_t) j * ld));
-                    v[0] = w.x;
-                    v[1] = w.y;
-                    v[2] = w.z;
-                    v[3] = w.w;
-                }
-                else {
-                    const double2 w = __ldcs(reinterpret_cast<const double2*>(col + (size_t) j * ld));
-                    v[0] = w.x;
-                    v[1] = w.y;
-                }
+                double v[V];
+                load_rows<T, V>(col + (size_t) j * ld, v);
 #pragma unroll
                 for (int r = 0; r < NR; r++) {
-                    if (r < nrhs) {
-                        const double xr = s_x[r][j];
+                    const double xr = s_x[j][r];
 #pragma unroll
-                        for (int q = 0; q < V; q++)
-                            acc[r][q] = fma((double) v[q], xr, acc[r][q]);
-                    }
+                    for (int q = 0; q < V; q++)
+                        acc[r][q] = fma(v[q], xr, acc[r][q]);
                 }
             }
         }
     }
-    for (int r = 0; r < nrhs; r++)
+    // unrolled over NR with a guard, so acc stays in registers (a runtime index would put it
+    // in local memory)
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        if (r >= nrhs)
+            break;
 #pragma unroll
         for (int q = 0; q < V; q++) {
             const int i = row0 + q;
@@ -501,6 +526,7 @@ __global__ void __launch_bounds__(256) dense_matvec_kernel(const T* __restrict__
             else
                 y[(size_t) r * n + i] = acc[r][q];
         }
+    }
 }
 
 }  // namespace kemcu

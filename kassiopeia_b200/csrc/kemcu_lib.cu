@@ -405,10 +405,9 @@ int apply_op(kemcu_ctx* ctx, int op, const double* d_x, double* d_y, int nrhs)
         return KEMCU_OK;
     }
     // dense operator: V rows per thread, enough CTAs for ~8 per SM, columns split to match
-    // V rows per thread; one wave of resident CTAs, the column range split to fill it
-    const size_t V = op == kDense64 ? 2 : 4;
-    const size_t rows_blocks = (n + 256 * V - 1) / (256 * V);
-    auto launch = [&](auto kernel, const auto* A) -> int {
+    // rows per thread (dense_rows); one wave of resident CTAs, the column range split to fill it
+    auto launch = [&](auto kernel, const auto* A, int V) -> int {
+        const size_t rows_blocks = (n + 256 * (size_t) V - 1) / (256 * (size_t) V);
         int per_sm = 0;
         KC(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0));
         size_t split = std::max((size_t) 1, (size_t) ctx->num_sms * std::max(1, per_sm) / rows_blocks);
@@ -432,8 +431,10 @@ int apply_op(kemcu_ctx* ctx, int op, const double* d_x, double* d_y, int nrhs)
         return KEMCU_OK;
     };
     if (op == kDense64)
-        return nrhs == 1 ? launch(dense_matvec_kernel<double, 1>, ctx->d_a64) : launch(dense_matvec_kernel<double, kMaxRhs>, ctx->d_a64);
-    return nrhs == 1 ? launch(dense_matvec_kernel<float, 1>, ctx->d_a32) : launch(dense_matvec_kernel<float, kMaxRhs>, ctx->d_a32);
+        return nrhs == 1 ? launch(dense_matvec_kernel<double, 1>, ctx->d_a64, dense_rows<double, 1>())
+                         : launch(dense_matvec_kernel<double, kMaxRhs>, ctx->d_a64, dense_rows<double, kMaxRhs>());
+    return nrhs == 1 ? launch(dense_matvec_kernel<float, 1>, ctx->d_a32, dense_rows<float, 1>())
+                     : launch(dense_matvec_kernel<float, kMaxRhs>, ctx->d_a32, dense_rows<float, kMaxRhs>());
 }
 
 int assemble(kemcu_ctx* ctx, bool want32)
