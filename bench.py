@@ -143,12 +143,12 @@ def run_native(args, rank, world, dist):
     import kassiopeia_b200 as K
     from kassiopeia_b200 import _native as NN
     from kassiopeia_b200 import geometry as G
+    from kassiopeia_b200 import ranks as RK
 
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
-    # the CPU baseline pool is spawned before this process touches CUDA state it could inherit
     mesh = G.coax()
-    P = G.gap_points(N_POINTS, seed=2024 + rank)
+    P = RK.rank_points(N_POINTS, rank)
     ctx = K.CUDAElectrostaticContext(dev)
     ctx.SetGeometry(mesh)
 
@@ -166,16 +166,10 @@ def run_native(args, rank, world, dist):
     ctx.SetSigma(x_asm)
 
     def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
+        RK.barrier(dist, device=torch.device("cuda", dev))
 
     def max_over_ranks(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return RK.max_over_ranks(v, dist, device=torch.device("cuda", dev))
 
     dP = torch.from_numpy(P).cuda()
     dOut = torch.empty((N_POINTS, 4), dtype=torch.float64, device="cuda")
@@ -445,7 +439,7 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libkemref.so not built here"}))
         return
     mesh = G.coax()
-    P = G.gap_points(N_POINTS, seed=2024)
+    P = G.gap_points(N_POINTS, seed=2024)  # rank 0's block (kassiopeia_b200.ranks.rank_points)
     # charge densities from the reference's own solver would take hours at 44,000 elements
     # (N^2 matrix entries per GMRES iteration on the CPU); the reference field sum is timed
     # with a fixed smooth density instead -- the direct sum's cost does not depend on sigma
