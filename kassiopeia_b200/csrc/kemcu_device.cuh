@@ -189,15 +189,24 @@ __device__ __forceinline__ int rule_offset(int type, int band, int& n)
 // (Potential_TriNP / ElectricField_TriNP, KElectrostaticCubatureTriangleIntegrator.cc:271-450;
 // the rectangle versions are identical in form), in the quadratic form described at the top.
 //
-// FP64 reciprocal square root from the hardware approximation plus one Newton-Raphson step
-// y1 = y0 (3 - x y0^2) / 2 (quadratic convergence: relative error ~1.5 e0^2), MIXED form only.
-__device__ __forceinline__ double rsqrt_fast(double x)
+// Twice the FP64 reciprocal square root, from the hardware approximation y0 plus one
+// Newton-Raphson step written as 2 y1 = y0 (3 - x y0^2) (quadratic convergence: relative
+// error ~1.5 e0^2). Returning 2 y1 saves the halving (three FP64 operations instead of
+// four); callers fold the factors 1/2 (potential) and 1/8 (field) into their element sums.
+// MIXED form only.
+__device__ __forceinline__ double rsqrt2_fast(double x)
 {
     double y;
     asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    const double h = fma(-0.5 * x * y, y, 0.5);
-    return fma(y, h, y);
+    return y * fma(-(x * y), y, 3.);
 }
+// scale of the values returned by the reciprocal square root used in a form: 2 (MIXED), 1 (FP64)
+template<bool FAST> __device__ __forceinline__ double irsq(double x)
+{
+    return FAST ? rsqrt2_fast(x) : rsqrt(x);
+}
+template<bool FAST> constexpr double kPotScale = FAST ? 0.5 : 1.;
+template<bool FAST> constexpr double kFieldScale = FAST ? 0.125 : 1.;
 
 // Nodes per unrolled group of the node loop (rules whose size it divides are run as a loop
 // over groups, the others fully unrolled). The reciprocal square root of the MIXED form is
@@ -230,7 +239,7 @@ __device__ __forceinline__ Out4 cubq(const double* e, V3 P)
             q2 = fma(c[2], aa, q2);
             q2 = fma(c[3], ab2, q2);
             q2 = fma(c[4], bb, q2);
-            const double ir = FAST ? rsqrt_fast(q2) : rsqrt(q2);
+            const double ir = irsq<FAST>(q2);
             if (POT)
                 sp = fma(c[5], ir, sp);
             if (FIELD) {
@@ -244,11 +253,12 @@ __device__ __forceinline__ Out4 cubq(const double* e, V3 P)
     const double pf = e[rPrefac];
     Out4 o{0., 0., 0., 0.};
     if (POT)
-        o.phi = pf * sp;
+        o.phi = (kPotScale<FAST> * pf) * sp;
     if (FIELD) {
-        o.ex = pf * (d.x * s0 - a.x * ss - b.x * st);
-        o.ey = pf * (d.y * s0 - a.y * ss - b.y * st);
-        o.ez = pf * (d.z * s0 - a.z * ss - b.z * st);
+        const double pff = kFieldScale<FAST> * pf;
+        o.ex = pff * (d.x * s0 - a.x * ss - b.x * st);
+        o.ey = pff * (d.y * s0 - a.y * ss - b.y * st);
+        o.ez = pff * (d.z * s0 - a.z * ss - b.z * st);
     }
     return o;
 }
@@ -271,7 +281,7 @@ __device__ __forceinline__ Out4 cubq_pairs(const double* e, V3 P)
     const double aa = e[rAA], ab2 = e[rAB2], bb = e[rBB];
     double sp = 0., s0 = 0., ss = 0., st = 0.;
     if (CENTER >= 0) {
-        const double ir = FAST ? rsqrt_fast(R2) : rsqrt(R2);
+        const double ir = irsq<FAST>(R2);
         sp = c_qc[CENTER] * ir;
         s0 = c_qc[CENTER] * (ir * ir * ir);
     }
@@ -286,8 +296,8 @@ __device__ __forceinline__ Out4 cubq_pairs(const double* e, V3 P)
             double Q = fma(c[2], aa, R2);
             Q = fma(c[3], ab2, Q);
             Q = fma(c[4], bb, Q);
-            const double irp = FAST ? rsqrt_fast(Q + L) : rsqrt(Q + L);
-            const double irm = FAST ? rsqrt_fast(Q - L) : rsqrt(Q - L);
+            const double irp = irsq<FAST>(Q + L);
+            const double irm = irsq<FAST>(Q - L);
             if (POT)
                 sp = fma(c[5], irp + irm, sp);
             if (FIELD) {
@@ -302,11 +312,12 @@ __device__ __forceinline__ Out4 cubq_pairs(const double* e, V3 P)
     const double pf = e[rPrefac];
     Out4 o{0., 0., 0., 0.};
     if (POT)
-        o.phi = pf * sp;
+        o.phi = (kPotScale<FAST> * pf) * sp;
     if (FIELD) {
-        o.ex = pf * (d.x * s0 - a.x * ss - b.x * st);
-        o.ey = pf * (d.y * s0 - a.y * ss - b.y * st);
-        o.ez = pf * (d.z * s0 - a.z * ss - b.z * st);
+        const double pff = kFieldScale<FAST> * pf;
+        o.ex = pff * (d.x * s0 - a.x * ss - b.x * st);
+        o.ey = pff * (d.y * s0 - a.y * ss - b.y * st);
+        o.ez = pff * (d.z * s0 - a.z * ss - b.z * st);
     }
     return o;
 }
