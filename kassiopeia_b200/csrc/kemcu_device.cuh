@@ -78,7 +78,7 @@ struct Constants
 constexpr int kTri7 = 0, kTri12 = 7, kTri33 = 19, kRect7 = 52, kRect12 = 59, kRect33 = 71, kNumNodes = 104;
 __constant__ double c_rules[kNumNodes * 3];
 // per node, relative to the rule centroid (1/3, 1/3) or (1/2, 1/2):
-//   s', t', s'^2, s't', t'^2, w, w s', w t'
+//   -2 s', -2 t', s'^2, s't', t'^2, w, w s', w t'
 constexpr int kQ = 8;
 __constant__ double c_q[kNumNodes * kQ];
 // The rectangle rules are centrally symmetric: node pairs (o, -o) of equal weight, plus at
@@ -154,24 +154,35 @@ __device__ __forceinline__ int band_exact(const double* e, double r2)
     return ratio > 27.7 ? 2 : ratio > 2. ? 1 : 0;
 }
 
-__device__ __forceinline__ int band_of(const double* e, V3 P)
+// The band of (element, P); also returns d = P - centroid and r2 = |d|^2 (formed as the
+// reference forms the distance ratio), which the cubature code re-uses.
+__device__ __forceinline__ int band_of(const double* e, V3 P, V3& d, double& r2)
 {
     const double dx = __dadd_rn(e[rCen], -P.x);
     const double dy = __dadd_rn(e[rCen + 1], -P.y);
     const double dz = __dadd_rn(e[rCen + 2], -P.z);
-    const double r2 = sumsq_rn(dx, dy, dz);
+    r2 = sumsq_rn(dx, dy, dz);
+    d = v3(-dx, -dy, -dz);
+    // outside a relative 1e-12 of every cut the fast comparison is the reference's decision
+    const double lo = r2 * (1. - 1e-12), hi = r2 * (1. + 1e-12);
     int band = 0;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         const double c = e[rCut + k];
-        if (r2 > c * (1. + 1e-12))
+        if (lo > c)
             band = k + 1;
-        else if (r2 >= c * (1. - 1e-12))
+        else if (hi >= c)
             return band_exact(e, r2);
         else
             break;
     }
     return band;
+}
+__device__ __forceinline__ int band_of(const double* e, V3 P)
+{
+    V3 d;
+    double r2;
+    return band_of(e, P, d, r2);
 }
 
 __device__ __forceinline__ int rule_offset(int type, int band, int& n)
@@ -219,12 +230,10 @@ template<bool FAST> constexpr double kFieldScale = FAST ? 0.125 : 1.;
 // N nodes of the rule starting at node OFF (both compile-time, so the rule constants are
 // constant-bank operands with fixed offsets within a group)
 template<int N, int OFF, bool POT, bool FIELD, bool FAST>
-__device__ __forceinline__ Out4 cubq(const double* e, V3 P)
+__device__ __forceinline__ Out4 cubq(const double* e, V3 d, double R2)
 {
-    const V3 d = P - ld3(e + rCen);
     const V3 a = ld3(e + rEa), b = ld3(e + rEb);
-    const double R2 = dot(d, d);
-    const double C1 = -2. * dot(d, a), C2 = -2. * dot(d, b);
+    const double C1 = dot(d, a), C2 = dot(d, b);  // the rule tables carry the factor -2
     const double aa = e[rAA], ab2 = e[rAB2], bb = e[rBB];
     double sp = 0., s0 = 0., ss = 0., st = 0.;
     constexpr int G = N % KEMCU_GROUP == 0 ? KEMCU_GROUP : N;
@@ -272,12 +281,10 @@ __device__ __forceinline__ Out4 cubq(const double* e, V3 P)
 #define KEMCU_PAIR_GROUP 16
 #endif
 template<int NP, int POFF, int CENTER, bool POT, bool FIELD, bool FAST>
-__device__ __forceinline__ Out4 cubq_pairs(const double* e, V3 P)
+__device__ __forceinline__ Out4 cubq_pairs(const double* e, V3 d, double R2)
 {
-    const V3 d = P - ld3(e + rCen);
     const V3 a = ld3(e + rEa), b = ld3(e + rEb);
-    const double R2 = dot(d, d);
-    const double C1 = -2. * dot(d, a), C2 = -2. * dot(d, b);
+    const double C1 = dot(d, a), C2 = dot(d, b);  // the rule tables carry the factor -2
     const double aa = e[rAA], ab2 = e[rAB2], bb = e[rBB];
     double sp = 0., s0 = 0., ss = 0., st = 0.;
     if (CENTER >= 0) {
@@ -616,7 +623,9 @@ template<bool POT, bool FIELD> __device__ __noinline__ Out4 line_analytic(const 
 // cubature code (the element type is uniform across a warp, which evaluates one element).
 template<bool MIXED, bool POT, bool FIELD> __device__ __forceinline__ Out4 epi(const double* e, V3 P)
 {
-    const int band = band_of(e, P);
+    V3 d;
+    double r2;
+    const int band = band_of(e, P, d, r2);
     const int type = (int) e[rType];
     if (type == kLineSegment) {
         if (band == 0)
@@ -627,12 +636,12 @@ template<bool MIXED, bool POT, bool FIELD> __device__ __forceinline__ Out4 epi(c
         return type == kTriangle ? rwg64<3, POT, FIELD>(e, P) : rwg64<4, POT, FIELD>(e, P);
     if (type == kTriangle) {
         if (band == 1)
-            return cubq<33, kTri33, POT, FIELD, MIXED>(e, P);
-        return band == 2 ? cubq<12, kTri12, POT, FIELD, MIXED>(e, P) : cubq<7, kTri7, POT, FIELD, MIXED>(e, P);
+            return cubq<33, kTri33, POT, FIELD, MIXED>(e, d, r2);
+        return band == 2 ? cubq<12, kTri12, POT, FIELD, MIXED>(e, d, r2) : cubq<7, kTri7, POT, FIELD, MIXED>(e, d, r2);
     }
     if (band == 1)
-        return cubq_pairs<16, kPair33, 1, POT, FIELD, MIXED>(e, P);
-    return band == 2 ? cubq_pairs<6, kPair12, -1, POT, FIELD, MIXED>(e, P) : cubq_pairs<3, kPair7, 0, POT, FIELD, MIXED>(e, P);
+        return cubq_pairs<16, kPair33, 1, POT, FIELD, MIXED>(e, d, r2);
+    return band == 2 ? cubq_pairs<6, kPair12, -1, POT, FIELD, MIXED>(e, d, r2) : cubq_pairs<3, kPair7, 0, POT, FIELD, MIXED>(e, d, r2);
 }
 
 }  // namespace kemcu

@@ -699,7 +699,7 @@ int kemcu_create(kemcu_ctx** out, const kemcu_config* cfg)
     for (int k = 0; k < kNumNodes; k++) {
         const double sc = k < kRect7 ? 1. / 3. : 0.5;  // rule centroid
         const double s = rules[3 * k] - sc, t = rules[3 * k + 1] - sc, w = rules[3 * k + 2];
-        const double v[kQ] = {s, t, s * s, s * t, t * t, w, w * s, w * t};
+        const double v[kQ] = {-2. * s, -2. * t, s * s, s * t, t * t, w, w * s, w * t};
         for (int c = 0; c < kQ; c++)
             q[kQ * k + c] = v[c];
     }
