@@ -91,7 +91,8 @@ enum kemcu_track_status { KEMCU_TRACK_ACTIVE = 0, KEMCU_TRACK_HIT = 1, KEMCU_TRA
 
 typedef struct {
     long long steps;         /* RK8 steps taken by all tracks */
-    long long field_evals;   /* field evaluations (13 per step) */
+    long long field_evals;   /* field evaluations (12 per step: the 13-stage scheme's stage 10 has
+                                zero weight everywhere, KSMathRK8.h:139-226, and is not evaluated) */
     int hit, max_steps, left, nonfinite, active;
     double seconds;
 } kemcu_track_stats;

@@ -66,7 +66,21 @@ struct TrackParams
     double hit_r2, max_r2;        // squared radii (0 disables)
     int max_steps, budget;
     int n_list;                   // number of track indices in list
+    unsigned live;                // bit s: stage s's derivative has a nonzero weight somewhere
 };
+
+// Stages whose derivative no later stage and not the final combination uses (zero column of the
+// Butcher table; stage 10 of this scheme: a[10][10] = a[11][10] = a[12][10] = 0). Their field
+// sums cannot change the result, so the tracker does not evaluate them.
+inline unsigned rk8_live_stages(const double a[kStages][kStages])
+{
+    unsigned live = 0u;
+    for (int k = 0; k < kStages; k++)
+        for (int r = k; r < kStages; r++)
+            if (a[r][k] != 0.)
+                live |= 1u << k;
+    return live;
+}
 
 // state: n x 8; steps, status: n; list: n_list track indices to work on; next: work counter;
 // done_steps: total steps taken (for statistics); flag |= 2 if a ring wait timed out.
@@ -120,11 +134,15 @@ __global__ void __launch_bounds__(kTrackSlots) rk8_tracker_kernel(const double* 
             break;
         double ds = 0.;  // sum over stages of a[12][k] |v_k|
         for (int st = 0; st < kStages; st++) {
+            if (!((prm.live >> st) & 1u))
+                continue;  // unused derivative (its column of the table is zero): not evaluated
             // stage position and momentum: value_{st-1} = y0 + dt sum_k a[st-1][k] k_k
             V3 X = v3(y[2], y[3], y[4]), Pm = v3(y[5], y[6], y[7]);
             if (track >= 0 && st > 0) {
                 double sx = 0., sy = 0., sz = 0., px = 0., py = 0., pz = 0.;
                 for (int k = 0; k < st; k++) {
+                    if (!((prm.live >> k) & 1u))
+                        continue;
                     const double a = c_rk8[st - 1][k];
                     sx += a * K(k, 0);
                     sy += a * K(k, 1);
@@ -178,6 +196,8 @@ __global__ void __launch_bounds__(kTrackSlots) rk8_tracker_kernel(const double* 
             for (int k = 0; k < kStages; k++) {
                 const double a = c_rk8[kStages - 1][k];
                 dtt += a;
+                if (!((prm.live >> k) & 1u))
+                    continue;
                 for (int c = 0; c < 6; c++)
                     d[c] += a * K(k, c);
             }

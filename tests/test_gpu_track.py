@@ -62,7 +62,9 @@ def test_multi_step_launch_equals_single_steps(ctx):
     st, steps, status, stats = ctx.TrackRK8(rk["state0"], float(rk["dt"]), 10000, step_budget=40,
                                             charge=float(rk["charge"]), mass=float(rk["mass"]))
     np.testing.assert_allclose(st, rk["traj"][:, -1], rtol=1e-12, atol=0)
-    assert stats["steps"] == 160 and stats["field_evals"] == 13 * 160
+    # 12 field sums per step: stage 10 of the 13-stage table has zero weight everywhere
+    # (KSMathRK8.h:139-226) and is not evaluated; the trajectory above is the reference's
+    assert stats["steps"] == 160 and stats["field_evals"] == 12 * 160
 
 
 def test_uneven_tracks_terminate_with_status(ctx):
