@@ -212,7 +212,7 @@ def run_native(args, rank, world, dist):
     barrier()
     e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
 
-    # accuracy of the mixed form against the plain FP64 form (north-star bound 1e-9)
+    # accuracy of the mixed form against the plain FP64 form (the metric bound is 1e-9)
     sub = P[:20000]
     o64 = ctx.ElectricFieldAndPotential(sub, precision=K.FP64)
     o32 = ctx.ElectricFieldAndPotential(sub, precision=K.MIXED)

@@ -3,7 +3,7 @@ reference's own FP64 CPU results (golden fixtures from tests/golden/make_golden.
 
 Tolerances: the FP64 form must agree with the reference to rounding (1e-12 relative to the
 largest value of the quantity, 1e-11 at the near-singular RWG special points); the MIXED form
-must meet the north-star bound of 1e-9 relative error against the FP64 oracle.
+must stay within 1e-9 relative error of the FP64 results.
 """
 
 import numpy as np
