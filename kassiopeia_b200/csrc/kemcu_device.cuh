@@ -18,10 +18,10 @@
 // the rule's centroid), |P - Q_k|^2 = R^2 + s' C1 + t' C2 + s'^2 |A N1|^2 + 2 s't' (A N1).(B N2)
 // + t'^2 |B N2|^2 with per-pair C1 = -2 d.(A N1), C2 = -2 d.(B N2): five FMAs per node instead of
 // forming the node and the difference vector, and the field sum collapses to
-// d S0 - (A N1) Ss - (B N2) St with three scalar node sums. Two reciprocal square roots:
-//   * FP64  -- IEEE-accurate double rsqrt (the plain form);
-//   * MIXED -- the FP32-class hardware estimate (rsqrt.approx.f64, ~2^-23 relative) refined by
-//              one FP64 Newton step (~1e-13 relative).
+// d S0 - (A N1) Ss - (B N2) St with three scalar node sums. Two reciprocal square roots, both
+// from the FP32-class hardware estimate (rsqrt.approx.f64, ~2^-23 relative):
+//   * FP64  -- refined by two FP64 Newton steps (within one unit in the last place);
+//   * MIXED -- refined by one FP64 Newton step (~1e-13 relative).
 // RWG near-field integrals and the analytic line segment are FP64 in both forms.
 #pragma once
 
@@ -211,13 +211,22 @@ __device__ __forceinline__ double rsqrt2_fast(double x)
     asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
     return y * fma(-(x * y), y, 3.);
 }
-// scale of the values returned by the reciprocal square root used in a form: 2 (MIXED), 1 (FP64)
+// Twice the FP64 reciprocal square root to within about one unit in the last place: the
+// MIXED estimate refined by a second Newton step on z = 2y, 2 y2 = z + (z/8) (4 - x z^2)
+// (the correction is ~1e-13 of z, so its own rounding stays below half an ulp). FP64 form.
+__device__ __forceinline__ double rsqrt2_acc(double x)
+{
+    const double z = rsqrt2_fast(x);
+    const double e4 = fma(-(x * z), z, 4.);
+    return fma(0.125 * z, e4, z);
+}
+// the reciprocal square root of a form, returned doubled (folded back by kPotScale/kFieldScale)
 template<bool FAST> __device__ __forceinline__ double irsq(double x)
 {
-    return FAST ? rsqrt2_fast(x) : rsqrt(x);
+    return FAST ? rsqrt2_fast(x) : rsqrt2_acc(x);
 }
-template<bool FAST> constexpr double kPotScale = FAST ? 0.5 : 1.;
-template<bool FAST> constexpr double kFieldScale = FAST ? 0.125 : 1.;
+template<bool FAST> constexpr double kPotScale = 0.5;
+template<bool FAST> constexpr double kFieldScale = 0.125;
 
 // Nodes per unrolled group of the node loop (rules whose size it divides are run as a loop
 // over groups, the others fully unrolled). The reciprocal square root of the MIXED form is
