@@ -37,6 +37,10 @@ sys.path.insert(0, ROOT)
 
 N_POINTS = 1_000_000
 TOL = 1e-10
+# DRAM bytes (read + write) of one MIXED direct-sum launch over the default 1,000,000-point
+# workload, from a one-pass ncu capture (profiles/field_kernel_coax1m_dram.md); bench.py
+# cannot run ncu itself, so the figure is reported only for that workload
+FIELD_TRAFFIC_BYTES_1M = 69.49e6 + 83.10e6
 # algorithmic flops per element-point interaction (field + potential) by band:
 # cubature / Gauss with n nodes: 20 n + 30 (node sums, ratio test); analytic near field:
 # fixed counts of one pass through the non-degenerate branch (frozen here)
@@ -405,7 +409,10 @@ def main():
                     "h2d_bytes_per_step": N_POINTS * 24, "d2h_bytes_per_step": N_POINTS * 32},
             "gpu_launches": r["launches"],
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": r["fp64_peak"], "unit": "TFLOP/s",
-                         "frac": achieved / r["fp64_peak"] if r["fp64_peak"] else None, "traffic": None,
+                         "frac": achieved / r["fp64_peak"] if r["fp64_peak"] else None,
+                         "traffic": FIELD_TRAFFIC_BYTES_1M if N_POINTS == 1_000_000 else None,
+                         "traffic_unit": "bytes per launch (ncu dram read + write)",
+                         "algorithmic_bytes": N_POINTS * (24 + 32) + 44000 * (256 + 8),
                          "peak_source": "measured FP64 FMA throughput of this GPU (kemcu_fma_peak); "
                                         "MEASURED_PEAKS.json has no FP64 CUDA-core figure",
                          "flops_per_step": r["flops_per_step"], "band_counts": r["counts"]},
