@@ -212,6 +212,11 @@ unsigned long long kemcu_launch_count(const kemcu_ctx* ctx);
    counts[shape * 4 + band], band 0 = analytic (RWG / analytic wire), 1 = 33-point / 16-node,
    2 = 12-point / 4-node, 3 = 7-point; the algorithmic work of a field evaluation */
 int kemcu_band_histogram(kemcu_ctx* ctx, const double* P, size_t n, long long* counts12);
+/* self-test of the device-side timeout path (no counterpart in the reference): a kernel waits
+   on a barrier phase that completes only when `complete` is nonzero; otherwise its bounded
+   wait gives up after ~2e6 cycles and the call returns KEMCU_ETIMEOUT, as a stalled element
+   pipeline would. The context stays usable either way. */
+int kemcu_selftest_timeout(kemcu_ctx* ctx, int complete);
 /* measured FMA throughput of the context's device, FP64 and FP32 CUDA-core pipes (TFLOP/s,
    2 flops per FMA), from independent dependent-FMA chains */
 int kemcu_fma_peak(kemcu_ctx* ctx, double* fp64_tflops, double* fp32_tflops);

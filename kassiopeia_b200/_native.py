@@ -108,5 +108,6 @@ def lib():
     L.kemcu_launch_count.restype = C.c_ulonglong
     L.kemcu_band_histogram.argtypes = [vp, _dp, C.c_size_t, C.POINTER(C.c_longlong)]
     L.kemcu_fma_peak.argtypes = [vp, _dp, _dp]
+    L.kemcu_selftest_timeout.argtypes = [vp, C.c_int]
     _lib = L
     return L

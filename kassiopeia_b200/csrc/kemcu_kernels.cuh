@@ -116,6 +116,34 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
             return false;
     return true;
 }
+// same wait with a caller-chosen cycle limit (the failure-path self-test)
+__device__ __forceinline__ bool mbar_wait_limit(unsigned long long* bar, unsigned parity, long long limit)
+{
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > limit)
+            return false;
+    return true;
+}
+
+// Self-test of the timeout path: one warp waits on an mbarrier phase that completes only when
+// `complete` is set (one arrival of the expected one); otherwise the wait gives up after
+// `limit` cycles and the kernel reports it in flag (|= 2), as the element ring does.
+__global__ void wait_timeout_selftest_kernel(int* __restrict__ flag, long long limit, int complete)
+{
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (complete && threadIdx.x == 0)
+        mbar_arrive(&bar);
+    const bool ok = mbar_wait_limit(&bar, 0u, limit);
+    if (!ok && threadIdx.x == 0)
+        atomicOr(flag, 2);
+}
+
 __device__ __forceinline__ void fence_proxy_async()
 {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

@@ -1196,6 +1196,19 @@ int kemcu_band_histogram(kemcu_ctx* ctx, const double* P, size_t n, long long* c
     return KEMCU_OK;
 }
 
+int kemcu_selftest_timeout(kemcu_ctx* ctx, int complete)
+{
+    if (!ctx)
+        return KEMCU_EINVAL;
+    KC(cudaSetDevice(ctx->device));
+    int rc = clear_pipe_flag(ctx);
+    if (rc)
+        return rc;
+    wait_timeout_selftest_kernel<<<1, 32, 0, ctx->stream>>>(ctx->d_flag + 1, 2000000LL, complete ? 1 : 0);
+    KCHECK_LAUNCH();
+    return pipe_status(ctx, "self-test wait");
+}
+
 int kemcu_fma_peak(kemcu_ctx* ctx, double* fp64_tflops, double* fp32_tflops)
 {
     if (!ctx || !ctx->stream)
