@@ -240,3 +240,17 @@ def test_invalid_inputs_are_reported(ctx):
         fresh.ElectricFieldAndPotential(np.zeros((2, 3)))
     assert e.value.code == K._native.ESTATE
     fresh.close()
+
+
+def test_empty_and_boundary_sized_point_sets(ctx):
+    # n = 0 is a no-op; sizes around the Morton-ordering threshold (4,096) and a ragged last
+    # CTA give the same values as evaluating the points one block at a time
+    fx = golden.load("icosphere_L2")
+    ctx.SetGeometry(golden.mesh_from(fx))
+    ctx.SetSigma(fx["sigma"])
+    assert ctx.ElectricFieldAndPotential(np.zeros((0, 3))).shape == (0, 4)
+    P = G.shell_points(4097 + 129, seed=21)
+    ref = np.concatenate([ctx.ElectricFieldAndPotential(P[i:i + 128]) for i in range(0, len(P), 128)])
+    for n in (1, 127, 4095, 4096, 4097, 4097 + 129):
+        out = ctx.ElectricFieldAndPotential(P[:n])
+        np.testing.assert_allclose(out, ref[:n], rtol=1e-13, atol=1e-13 * np.abs(ref).max())
