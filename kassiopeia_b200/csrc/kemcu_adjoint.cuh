@@ -95,9 +95,18 @@ __global__ void __launch_bounds__(kAdjThreads) vjp_kernel(const double* __restri
 {
     __shared__ double s_p[kPtTile][3];
     __shared__ double s_w[kPtTile][4];
+    // the CTA's element records, one per thread, rows padded to 33 doubles so that the threads'
+    // reads of the same field fall in different banks (read once per point by the owner)
+    __shared__ double s_e[kAdjThreads][rRecSize + 1];
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = j < n_elem;
-    const double* e = rec + (size_t) (active ? j : 0) * rRecSize;  // re-read through L1 per point
+    {
+        const int first = blockIdx.x * blockDim.x, cnt = min((int) blockDim.x, n_elem - first);
+        for (int q = threadIdx.x; q < cnt * rRecSize; q += blockDim.x)
+            s_e[q / rRecSize][q % rRecSize] = rec[(size_t) first * rRecSize + q];
+    }
+    __syncthreads();
+    const double* e = s_e[threadIdx.x];
     const int type = active ? (int) e[rType] : 0;
     const int per = (n_pts + gridDim.y - 1) / gridDim.y;
     const int p0 = blockIdx.y * per, p1 = min(n_pts, p0 + per);
@@ -135,7 +144,7 @@ __global__ void __launch_bounds__(kAdjThreads) vjp_kernel(const double* __restri
             for (int k = 0; k < n; k++) {
                 const double s = c_rules[3 * (off + k)], t = c_rules[3 * (off + k) + 1], wk = c_rules[3 * (off + k) + 2];
                 const V3 d = d0 - s * a - t * b;
-                const double ir = rsqrt(dot(d, d));
+                const double ir = 0.5 * rsqrt2_acc(dot(d, d));
                 const double ir3 = ir * ir * ir, ir5 = ir3 * ir * ir;
                 const double c1 = pf * wk * (w[3] * ir3 + 3. * dot(wE, d) * ir5), c2 = pf * wk * ir3;
                 const V3 gk = v3(c1 * d.x - c2 * wE.x, c1 * d.y - c2 * wE.y, c1 * d.z - c2 * wE.z);
