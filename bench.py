@@ -378,6 +378,9 @@ def main():
         rate, sample = cpu_reference_rate(r["mesh"], r["sigma"], r["P"], workers)
         if rate is not None:
             cpu = {"value": rate, "unit": "points/s", "cores": workers, "kind": "reference", "sample": sample}
+            # the single-core figure beside it (one process, a ~5 s sample)
+            rate1, sample1 = cpu_reference_rate(r["mesh"], r["sigma"], r["P"], 1, seconds_target=5.0)
+            cpu["one_core"] = {"value": rate1, "sample": sample1}
         else:
             cpu = {"value": None, "unit": "points/s", "cores": 0, "kind": "reference", "sample": sample}
 
