@@ -87,6 +87,50 @@ __device__ __noinline__ void rwg_vertex_grad(const double* e, V3 P, const double
     }
 }
 
+// Node-gradient moments of one (element, point) pair for a rule of N nodes from node OFF.
+// With d = P - centroid, node offsets o_k = s'_k (A N1) + t'_k (B N2), r_k = |d - o_k| and
+//   c1_k = w_k (wphi / r^3 + 3 (wE . (d - o_k)) / r^5),  c2_k = w_k / r^3,
+// the gradient of w . F with respect to node k is pf (c1_k (d - o_k) - c2_k wE), and a vertex
+// gradient is its barycentric weight times that, summed over nodes. Both sums are linear in
+// the node moments m = (sum c1, sum s'c1, sum t'c1, sum s'^2 c1, sum s't' c1, sum t'^2 c1,
+// sum c2, sum s'c2, sum t'c2), accumulated here (9 FMAs per node, no per-node vectors).
+constexpr int kQA = 6;
+__constant__ double c_qa[kNumNodes * kQA];  // per node: w, w s', w t', w s'^2, w s't', w t'^2
+template<int N, int OFF, bool FAST>
+__device__ __forceinline__ void node_moments(const double* e, V3 d, V3 wE, double wphi, double m[9])
+{
+    const V3 a = ld3(e + rEa), b = ld3(e + rEb);
+    const double R2 = dot(d, d), Da = dot(d, a), Db = dot(d, b);
+    const double aa = e[rAA], ab2 = e[rAB2], bb = e[rBB];
+    // 3 wE.(d - o_k) = 3 wE.d + (-2 s') (1.5 wE.a) + (-2 t') (1.5 wE.b)
+    const double w3d = 3. * dot(wE, d), w3a = 1.5 * dot(wE, a), w3b = 1.5 * dot(wE, b);
+    constexpr int G = N % KEMCU_GROUP == 0 ? KEMCU_GROUP : N;
+#pragma unroll 1
+    for (int g = 0; g < N / G; g++) {
+        const double* cg = c_q + kQ * (OFF + g * G);
+        const double* ag = c_qa + kQA * (OFF + g * G);
+#pragma unroll
+        for (int k = 0; k < G; k++) {
+            const double* c = cg + kQ * k;
+            const double* w = ag + kQA * k;
+            double q2 = fma(c[0], Da, R2);
+            q2 = fma(c[1], Db, q2);
+            q2 = fma(c[2], aa, q2);
+            q2 = fma(c[3], ab2, q2);
+            q2 = fma(c[4], bb, q2);
+            const double ir = 0.5 * irsq<FAST>(q2), ir2 = ir * ir, ir3 = ir2 * ir;
+            const double wd3 = fma(c[1], w3b, fma(c[0], w3a, w3d));
+            const double c1 = ir3 * fma(wd3, ir2, wphi);
+#pragma unroll
+            for (int q = 0; q < 6; q++)
+                m[q] = fma(w[q], c1, m[q]);
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+                m[6 + q] = fma(w[q], ir3, m[6 + q]);
+        }
+    }
+}
+
 template<bool MIXED>
 __global__ void __launch_bounds__(kAdjThreads) vjp_kernel(const double* __restrict__ rec, int n_elem,
                                                           const double* __restrict__ pts, const double* __restrict__ wts,
@@ -112,6 +156,23 @@ __global__ void __launch_bounds__(kAdjThreads) vjp_kernel(const double* __restri
     const int p0 = blockIdx.y * per, p1 = min(n_pts, p0 + per);
     Kahan S;
     double g[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
+    // gradients of log(area) with respect to P1 and P2 (the element's constant part of the
+    // area term), formed once per element
+    V3 dA1 = v3(0., 0., 0.), dA2 = v3(0., 0., 0.);
+    if (active && type != kLineSegment) {
+        const V3 ea = ld3(e + rEa), eb = ld3(e + rEb);
+        if (type == kTriangle) {
+            const V3 c = cross(ea, eb);
+            const V3 ch = (1. / norm(c)) * c;
+            const double A2 = 0.5 * norm(c);
+            dA1 = (0.5 / A2) * cross(eb, ch);
+            dA2 = (0.5 / A2) * cross(ch, ea);
+        }
+        else {
+            dA1 = (1. / dot(ea, ea)) * ea;
+            dA2 = (1. / dot(eb, eb)) * eb;
+        }
+    }
     for (int t0 = p0; t0 < p1; t0 += kPtTile) {
         const int cnt = min(kPtTile, p1 - t0);
         __syncthreads();
@@ -136,40 +197,53 @@ __global__ void __launch_bounds__(kAdjThreads) vjp_kernel(const double* __restri
                 rwg_vertex_grad(e, P, w, g);
                 continue;
             }
-            int n;
-            const int off = rule_offset(type, band, n);
-            const V3 d0 = P - ld3(e + rP0), a = ld3(e + rEa), b = ld3(e + rEb);
+            // node gradients from the rule's node moments (node_moments), mapped to the vertices
+            const V3 dc = P - ld3(e + rCen), a = ld3(e + rEa), b = ld3(e + rEb);
             const V3 wE = v3(w[0], w[1], w[2]);
-            const double pf = e[rPrefac];
-            for (int k = 0; k < n; k++) {
-                const double s = c_rules[3 * (off + k)], t = c_rules[3 * (off + k) + 1], wk = c_rules[3 * (off + k) + 2];
-                const V3 d = d0 - s * a - t * b;
-                const double ir = 0.5 * rsqrt2_acc(dot(d, d));
-                const double ir3 = ir * ir * ir, ir5 = ir3 * ir * ir;
-                const double c1 = pf * wk * (w[3] * ir3 + 3. * dot(wE, d) * ir5), c2 = pf * wk * ir3;
-                const V3 gk = v3(c1 * d.x - c2 * wE.x, c1 * d.y - c2 * wE.y, c1 * d.z - c2 * wE.z);
-                const double cw[3] = {1. - s - t, s, t};
-#pragma unroll
-                for (int v = 0; v < 3; v++) {
-                    g[3 * v] += cw[v] * gk.x;
-                    g[3 * v + 1] += cw[v] * gk.y;
-                    g[3 * v + 2] += cw[v] * gk.z;
-                }
-            }
-            // area term for this point: (w . F) dA / A, added per point so the frozen band holds
-            const V3 ea = ld3(e + rEa), eb = ld3(e + rEb);
-            V3 dA1, dA2;
+            double m[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
             if (type == kTriangle) {
-                const V3 c = cross(ea, eb);
-                const V3 ch = (1. / norm(c)) * c;
-                const double A2 = 0.5 * norm(c);
-                dA1 = (0.5 / A2) * cross(eb, ch);
-                dA2 = (0.5 / A2) * cross(ch, ea);
+                if (band == 1)
+                    node_moments<33, kTri33, MIXED>(e, dc, wE, w[3], m);
+                else if (band == 2)
+                    node_moments<12, kTri12, MIXED>(e, dc, wE, w[3], m);
+                else
+                    node_moments<7, kTri7, MIXED>(e, dc, wE, w[3], m);
             }
             else {
-                dA1 = (1. / dot(ea, ea)) * ea;
-                dA2 = (1. / dot(eb, eb)) * eb;
+                if (band == 1)
+                    node_moments<33, kRect33, MIXED>(e, dc, wE, w[3], m);
+                else if (band == 2)
+                    node_moments<12, kRect12, MIXED>(e, dc, wE, w[3], m);
+                else
+                    node_moments<7, kRect7, MIXED>(e, dc, wE, w[3], m);
             }
+            {
+                // barycentric weights of the nodes: P1 weight s = s' + sc, P2 weight t = t' + sc
+                const double sc = type == kTriangle ? 1. / 3. : 0.5;
+                const double pf = e[rPrefac];
+                // sum over nodes of weight x (c1 (d - o) - c2 wE) for weights 1, s, t
+                const double T1[3] = {m[0], m[1] + sc * m[0], m[2] + sc * m[0]};           // c1 . {1, s, t}
+                const double Ts[3] = {m[1], m[3] + sc * m[1], m[4] + sc * m[1]};           // c1 s' . {1, s, t}
+                const double Tt[3] = {m[2], m[4] + sc * m[2], m[5] + sc * m[2]};           // c1 t' . {1, s, t}
+                const double T2[3] = {m[6], m[7] + sc * m[6], m[8] + sc * m[6]};           // c2 . {1, s, t}
+                V3 G[3];
+#pragma unroll
+                for (int v = 0; v < 3; v++)
+                    G[v] = v3(pf * (dc.x * T1[v] - a.x * Ts[v] - b.x * Tt[v] - wE.x * T2[v]),
+                              pf * (dc.y * T1[v] - a.y * Ts[v] - b.y * Tt[v] - wE.y * T2[v]),
+                              pf * (dc.z * T1[v] - a.z * Ts[v] - b.z * Tt[v] - wE.z * T2[v]));
+                // vertex P0 has weight 1 - s - t
+                g[0] += G[0].x - G[1].x - G[2].x;
+                g[1] += G[0].y - G[1].y - G[2].y;
+                g[2] += G[0].z - G[1].z - G[2].z;
+                g[3] += G[1].x;
+                g[4] += G[1].y;
+                g[5] += G[1].z;
+                g[6] += G[2].x;
+                g[7] += G[2].y;
+                g[8] += G[2].z;
+            }
+            // area term for this point: (w . F) dA / A, added per point so the frozen band holds
             const double wf = w[0] * F.ex + w[1] * F.ey + w[2] * F.ez + w[3] * F.phi;
             g[0] -= wf * (dA1.x + dA2.x);
             g[1] -= wf * (dA1.y + dA2.y);

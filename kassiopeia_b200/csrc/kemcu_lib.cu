@@ -705,6 +705,15 @@ int kemcu_create(kemcu_ctx** out, const kemcu_config* cfg)
     }
     KC(cudaMemcpyToSymbol(c_rules, rules.data(), rules.size() * sizeof(double)));
     KC(cudaMemcpyToSymbol(c_q, q.data(), q.size() * sizeof(double)));
+    std::vector<double> qa(kNumNodes * kQA);
+    for (int k = 0; k < kNumNodes; k++) {
+        const double sc = k < kRect7 ? 1. / 3. : 0.5;
+        const double s = rules[3 * k] - sc, t = rules[3 * k + 1] - sc, w = rules[3 * k + 2];
+        const double v[kQA] = {w, w * s, w * t, w * s * s, w * s * t, w * t * t};
+        for (int c = 0; c < kQA; c++)
+            qa[kQA * k + c] = v[c];
+    }
+    KC(cudaMemcpyToSymbol(c_qa, qa.data(), qa.size() * sizeof(double)));
     // pair form of the centrally symmetric rectangle rules
     std::vector<double> qp(kNumPairs * kQ, 0.);
     double qc[2] = {0., 0.};
