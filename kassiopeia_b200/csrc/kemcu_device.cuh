@@ -72,11 +72,11 @@ struct Constants
 };
 
 // Cubature rules in barycentric-like (s, t) form: node = P0 + s * (A N1) + t * (B N2),
-// weights normalised to 1 over the element. Offsets into c_rules (triples s, t, w):
+// weights normalised to 1 over the element (tables in kemcu_tables.cuh). Node offsets of the
+// rules in the tables below:
 //   tri7 [0,7) tri12 [7,19) tri33 [19,52) rect7 [52,59) rect12 [59,71) rect33 [71,104)
 // Line Gauss-Legendre half rules (x, w) pairs: gl4 [0,2), gl16 [2,10).
 constexpr int kTri7 = 0, kTri12 = 7, kTri33 = 19, kRect7 = 52, kRect12 = 59, kRect33 = 71, kNumNodes = 104;
-__constant__ double c_rules[kNumNodes * 3];
 // per node, relative to the rule centroid (1/3, 1/3) or (1/2, 1/2):
 //   -2 s', -2 t', s'^2, s't', t'^2, w, w s', w t'
 constexpr int kQ = 8;
@@ -183,16 +183,6 @@ __device__ __forceinline__ int band_of(const double* e, V3 P)
     V3 d;
     double r2;
     return band_of(e, P, d, r2);
-}
-
-__device__ __forceinline__ int rule_offset(int type, int band, int& n)
-{
-    if (type == kTriangle) {
-        n = band == 1 ? 33 : band == 2 ? 12 : 7;
-        return band == 1 ? kTri33 : band == 2 ? kTri12 : kTri7;
-    }
-    n = band == 1 ? 33 : band == 2 ? 12 : 7;
-    return band == 1 ? kRect33 : band == 2 ? kRect12 : kRect7;
 }
 
 // ------------------------------------------------------------------------- cubature

@@ -703,7 +703,6 @@ int kemcu_create(kemcu_ctx** out, const kemcu_config* cfg)
         for (int c = 0; c < kQ; c++)
             q[kQ * k + c] = v[c];
     }
-    KC(cudaMemcpyToSymbol(c_rules, rules.data(), rules.size() * sizeof(double)));
     KC(cudaMemcpyToSymbol(c_q, q.data(), q.size() * sizeof(double)));
     std::vector<double> qa(kNumNodes * kQA);
     for (int k = 0; k < kNumNodes; k++) {
