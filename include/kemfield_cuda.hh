@@ -12,11 +12,16 @@
 //                                operator()(i, j) (KBoundaryIntegralMatrix.hh:31-55) run on the GPU
 //   KCUDAChargeDensitySolver     the whole GMRES charge-density solve on the device
 //                                (KSimpleIterativeKrylovSolver<double, KGeneralizedMinimalResidual>)
+//   KCUDARobinHoodChargeDensitySolver  Robin Hood on the device (KRobinHood.hh:61-104)
+//                                both KChargeDensitySolver subclasses that read and write
+//                                KEMField's solution cache (KChargeDensitySolver.cc:51-280)
 //
-// Header-only; include after the reference's KEMField headers and link with -lkemcu. Errors
+// Header-only; include after the reference's KEMField headers and link with -lkemcu and the
+// KEMField libraries that hold KChargeDensitySolver and KEMFileInterface. Errors
 // surface as KEMSimpleException, as elsewhere in KEMField.
 #pragma once
 
+#include "KChargeDensitySolver.hh"
 #include "KElectrostaticBasis.hh"
 #include "KEMConstants.hh"
 #include "KEMSimpleException.hh"
@@ -229,14 +234,83 @@ class KCUDABoundaryIntegralMatrix : public KSquareMatrix<double>
     mutable double fEntry = 0.;
 };
 
-class KCUDAChargeDensitySolver
+// The charge-density solvers are KChargeDensitySolver subclasses (KChargeDensitySolver.hh:17-45),
+// so KElectrostaticBoundaryField::SetChargeDensitySolver (KElectrostaticBoundaryField.cc:29-32)
+// takes them where it takes KKrylovChargeDensitySolver or KRobinHoodChargeDensitySolver.
+// Initialize(container) keeps the reference's solution cache protocol
+// (KRobinHoodChargeDensitySolver.cc:83-216): FindSolution(tolerance) first, which loads a cached
+// solution of the same shape and boundary hashes solved to at least this tolerance (or a
+// superposition of such solutions); otherwise the solve runs on the device, sigma is written into
+// each KElectrostaticBasis and SaveSolution(tolerance) stores it through KEMFileInterface.
+// Solve(KCUDASurfaceContainer&) is the uncached device solve on an existing context.
+class KCUDAChargeDensitySolverBase : public KChargeDensitySolver
 {
   public:
-    KCUDAChargeDensitySolver(double tolerance = 1e-10, int max_iterations = 500, int mode = KEMCU_SOLVE_PLAIN) :
-        fTolerance(tolerance),
+    KCUDAChargeDensitySolverBase(double tolerance, int device) : fTolerance(tolerance), fDevice(device)
+    {
+        // the defaults KElectrostaticBoundaryField passes in before Initialize
+        // (KElectrostaticBoundaryField.cc:20-21, 79); it overrides them when it drives the solver
+        SetHashProperties(20, 1.e-14);
+    }
+    void SetTolerance(double d)
+    {
+        fTolerance = d;
+    }
+    double GetTolerance() const
+    {
+        return fTolerance;
+    }
+    void SetDevice(int device)
+    {
+        fDevice = device;
+    }
+    // true when the last Initialize took its solution from the cache, without a device solve
+    bool SolutionFromCache() const
+    {
+        return fFromCache;
+    }
+
+  protected:
+    virtual void DeviceSolve(KCUDASurfaceContainer& container) = 0;
+    double fTolerance;
+    int fDevice;
+
+  private:
+    void InitializeCore(KSurfaceContainer& container) override
+    {
+        if (container.empty())
+            throw KEMSimpleException("kemcu: charge density solver got no electrode elements");
+        fFromCache = FindSolution(fTolerance, container);
+        if (fFromCache)
+            return;
+        {
+            KCUDASurfaceContainer gpu(container, fDevice);
+            DeviceSolve(gpu);
+        }
+        SaveSolution(fTolerance, container);
+    }
+    bool fFromCache = false;
+};
+
+// KKrylovChargeDensitySolver analogue for the direct operator: the whole GMRES solve
+// (KSimpleIterativeKrylovSolver<double, KGeneralizedMinimalResidual>) on the device
+class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
+{
+  public:
+    KCUDAChargeDensitySolver(double tolerance = 1e-10, int max_iterations = 500, int mode = KEMCU_SOLVE_PLAIN,
+                             int device = 0) :
+        KCUDAChargeDensitySolverBase(tolerance, device),
         fMaxIterations(max_iterations),
         fMode(mode)
     {}
+    void SetMaxIterations(int n)
+    {
+        fMaxIterations = n;
+    }
+    void SetMode(int mode)
+    {
+        fMode = mode;
+    }
     // solves A sigma = b for the boundary values and writes sigma into the container
     kemcu_solve_stats Solve(KCUDASurfaceContainer& container) const
     {
@@ -247,22 +321,40 @@ class KCUDAChargeDensitySolver
         container.ReadBasisData();
         return st;
     }
+    const kemcu_solve_stats& LastStats() const
+    {
+        return fStats;
+    }
 
   private:
-    double fTolerance;
+    void DeviceSolve(KCUDASurfaceContainer& container) override
+    {
+        fStats = Solve(container);
+    }
     int fMaxIterations, fMode;
+    kemcu_solve_stats fStats{};
 };
 
 // KRobinHoodChargeDensitySolver analogue (KRobinHood<double>::Solve, KRobinHood.hh:61-104):
 // Robin Hood on the device, starting from the charge densities the container holds
-class KCUDARobinHoodChargeDensitySolver
+class KCUDARobinHoodChargeDensitySolver : public KCUDAChargeDensitySolverBase
 {
   public:
-    KCUDARobinHoodChargeDensitySolver(double tolerance = 1e-8, int check_interval = 0, bool assembled = false) :
-        fTolerance(tolerance),
+    KCUDARobinHoodChargeDensitySolver(double tolerance = 1e-8, int check_interval = 0, bool assembled = false,
+                                      int device = 0) :
+        KCUDAChargeDensitySolverBase(tolerance, device),
         fCheckInterval(check_interval),
         fAssembled(assembled)
     {}
+    // residual check every i corrections; 0 picks the element count
+    void SetCheckSubInterval(unsigned int i)
+    {
+        fCheckInterval = (int) i;
+    }
+    void CacheMatrixElements(bool choice)
+    {
+        fAssembled = choice;
+    }
     kemcu_rh_stats Solve(KCUDASurfaceContainer& container) const
     {
         std::vector<double> x(container.size(), 0.);
@@ -274,11 +366,19 @@ class KCUDARobinHoodChargeDensitySolver
         container.ReadBasisData();
         return st;
     }
+    const kemcu_rh_stats& LastStats() const
+    {
+        return fStats;
+    }
 
   private:
-    double fTolerance;
+    void DeviceSolve(KCUDASurfaceContainer& container) override
+    {
+        fStats = Solve(container);
+    }
     int fCheckInterval;
     bool fAssembled;
+    kemcu_rh_stats fStats{};
 };
 
 }  // namespace KEMField

@@ -1,12 +1,15 @@
 // Drop-in check of include/kemfield_cuda.hh against the reference's unchanged KEMField classes:
 // the same KSurfaceContainer is solved on the GPU through KCUDAChargeDensitySolver, then the
 // reference's CPU KIntegratingFieldSolver / KBoundaryIntegralMatrix and the CUDA adaptors are
-// evaluated side by side; the reference's own GMRES driver also runs on the CUDA matrix.
+// evaluated side by side; the reference's own GMRES driver also runs on the CUDA matrix. Last,
+// the CUDA charge-density solvers run as KChargeDensitySolver subclasses against KEMField's own
+// solution cache (SaveSolution / FindSolution through KEMFileInterface) in a scratch directory.
 // Exit status 0 when every comparison is within tolerance.
 #include "KBoundaryIntegralMatrix.hh"
 #include "KBoundaryIntegralSolutionVector.hh"
 #include "KBoundaryIntegralVector.hh"
 #include "KElectrostaticBoundaryIntegratorFactory.hh"
+#include "KEMFileInterface.hh"
 #include "KElectrostaticIntegratingFieldSolver.hh"
 #include "KGeneralizedMinimalResidual.hh"
 #include "KRobinHood.hh"
@@ -18,6 +21,8 @@
 #include <array>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
+#include <filesystem>
 #include <map>
 #include <vector>
 
@@ -30,7 +35,7 @@ static V unit(V a)
     return {a[0] / r, a[1] / r, a[2] / r};
 }
 
-static void icosphere(int level, KSurfaceContainer& c)
+static void icosphere(int level, KSurfaceContainer& c, double R = 1., double U = 1.)
 {
     const double t = (1. + std::sqrt(5.)) / 2.;
     std::vector<V> v = {{-1, t, 0}, {1, t, 0}, {-1, -t, 0}, {1, -t, 0}, {0, -1, t}, {0, 1, t},
@@ -62,11 +67,90 @@ static void icosphere(int level, KSurfaceContainer& c)
     }
     for (auto& q : f) {
         auto* T = new KSurface<KElectrostaticBasis, KDirichletBoundary, KTriangle>();
-        T->SetValues(KPosition(v[q[0]][0], v[q[0]][1], v[q[0]][2]), KPosition(v[q[1]][0], v[q[1]][1], v[q[1]][2]),
-                     KPosition(v[q[2]][0], v[q[2]][1], v[q[2]][2]));
-        T->SetBoundaryValue(1.);
+        T->SetValues(KPosition(R * v[q[0]][0], R * v[q[0]][1], R * v[q[0]][2]),
+                     KPosition(R * v[q[1]][0], R * v[q[1]][1], R * v[q[1]][2]),
+                     KPosition(R * v[q[2]][0], R * v[q[2]][1], R * v[q[2]][2]));
+        T->SetBoundaryValue(U);
         c.push_back(T);
     }
+}
+
+static double sigma_of(KSurfaceContainer& c, unsigned i)
+{
+    return dynamic_cast<KElectrostaticBasis*>(c[i]->GetBasis())->GetSolution();
+}
+
+// KEMField's solution cache with CUDA-solved charge densities, through the reference's own
+// FindSolution / SaveSolution (KChargeDensitySolver.cc:51-280):
+//  1. nothing stored: solved on the device and stored;
+//  2. same shape and boundary values: the stored sigma comes back bit for bit, no device solve.
+//     The reference takes a stored solution of matching hashes whatever tolerance it was solved
+//     to (FindByHash sets the found flag, KChargeDensitySolver.cc:108-131), so a request at a
+//     tighter tolerance is answered from the cache as well;
+//  3. same shape at 2 V: composed by the reference's superposition of stored solutions;
+//  4. another shape (radius 1.5 m): solved on the device; sigma scales as 1/R.
+static int cache_round_trip()
+{
+    char tmpl[] = "/tmp/kemcu_cacheXXXXXX";
+    if (!mkdtemp(tmpl)) {
+        std::printf("cache: no scratch directory\n");
+        return 1;
+    }
+    const std::string dir(tmpl);
+    KEMFileInterface::GetInstance()->ActiveDirectory(dir);
+    KEMFileInterface::GetInstance()->ActiveFile(dir + "/kemcu_cache.kbd");
+    int fail = 0;
+    auto rel = [](KSurfaceContainer& a, KSurfaceContainer& b, double scale) {
+        double w = 0., n = 0.;
+        for (unsigned i = 0; i < a.size(); i++) {
+            w = std::max(w, std::fabs(sigma_of(a, i) - scale * sigma_of(b, i)));
+            n = std::max(n, std::fabs(scale * sigma_of(b, i)));
+        }
+        return w / n;
+    };
+
+    KSurfaceContainer c1;
+    icosphere(2, c1);
+    KCUDAChargeDensitySolver s1(1e-10, 200, KEMCU_SOLVE_PLAIN);
+    s1.Initialize(c1);
+    const bool stored = std::filesystem::exists(dir + "/kemcu_cache.kbd");
+    std::printf("cache: first solve from cache %d, %d GMRES iterations, cache file written %d\n",
+                (int) s1.SolutionFromCache(), s1.LastStats().iterations, (int) stored);
+    fail += s1.SolutionFromCache() || s1.LastStats().iterations < 1 || !stored;
+
+    for (double tol : {1e-8, 1e-12}) {
+        KSurfaceContainer c2;
+        icosphere(2, c2);
+        KCUDARobinHoodChargeDensitySolver s2(tol);
+        s2.Initialize(c2);
+        unsigned differ = c1.size() != c2.size();
+        for (unsigned i = 0; !differ && i < c1.size(); i++)
+            differ += sigma_of(c1, i) != sigma_of(c2, i);
+        std::printf("cache: request at %.0e from cache %d, Robin Hood checks %d, elements differing %u\n", tol,
+                    (int) s2.SolutionFromCache(), s2.LastStats().iterations, differ);
+        fail += !s2.SolutionFromCache() || s2.LastStats().iterations != 0 || differ != 0;
+    }
+
+    KSurfaceContainer c3;
+    icosphere(2, c3, 1., 2.);
+    KCUDAChargeDensitySolver s3(1e-10, 200, KEMCU_SOLVE_PLAIN);
+    s3.Initialize(c3);
+    const double r3 = rel(c3, c1, 2.);
+    std::printf("cache: 2 V from cache %d (superposition), %d GMRES iterations, max relative difference to 2 sigma "
+                "%.3e\n", (int) s3.SolutionFromCache(), s3.LastStats().iterations, r3);
+    fail += !s3.SolutionFromCache() || s3.LastStats().iterations != 0 || !(r3 < 1e-12);
+
+    KSurfaceContainer c4;
+    icosphere(2, c4, 1.5);
+    KCUDAChargeDensitySolver s4(1e-10, 200, KEMCU_SOLVE_PLAIN);
+    s4.Initialize(c4);
+    const double r4 = rel(c4, c1, 1. / 1.5);
+    std::printf("cache: radius 1.5 m from cache %d, %d GMRES iterations, max relative difference to sigma / 1.5 "
+                "%.3e\n", (int) s4.SolutionFromCache(), s4.LastStats().iterations, r4);
+    fail += s4.SolutionFromCache() || s4.LastStats().iterations < 1 || !(r4 < 1e-8);
+
+    std::filesystem::remove_all(dir);
+    return fail;
 }
 
 int main()
@@ -149,6 +233,8 @@ int main()
         std::printf("Robin Hood: reference %u checks, CUDA %d checks (%lld corrections), max relative difference "
                     "%.3e\n", rh.GetIteration(), rs.iterations, rs.subiterations, wr / nr);
         failures += !(wr / nr < 1e-6 && std::abs((int) rh.GetIteration() - rs.iterations) <= 1);
+
+        failures += cache_round_trip();
     }
     catch (std::exception& e) {
         std::printf("exception: %s\n", e.what());
