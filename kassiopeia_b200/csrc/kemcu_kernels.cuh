@@ -474,10 +474,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) assemble_kernel(const do
 
 // dense matvec on the assembled column-major operator (leading dimension ld):
 // y[r][i] = sum_j A[j*ld+i] x[r][j] for r < nrhs <= NR. A thread owns V consecutive rows
-// (dense_rows<T, NR>: one 16-byte load per column for a single right-hand side, 8 bytes for
-// several, which keeps the NR x V accumulators in registers at full occupancy), entries are
-// streamed past L1/L2 with evict-first loads; the column range is split over gridDim.y.
-// HBM-bound: 8 or 4 B per entry per call, whatever the number of right-hand sides.
+// (dense_rows<T, NR>: one 16-byte load per column), entries are streamed past L1/L2 with
+// evict-first loads; the column range is split over gridDim.y. HBM-bound for one right-hand
+// side (8 or 4 B per entry per call); several right-hand sides go to dense_mma_kernel, whose
+// x operand needs no broadcast through shared memory.
 template<typename T, int NR> __host__ __device__ constexpr int dense_rows()
 {
     return (NR == 1 ? 16 : 8) / (int) sizeof(T);
@@ -563,6 +563,109 @@ __global__ void __launch_bounds__(256) dense_matvec_kernel(const T* __restrict__
                 partial[((size_t) blockIdx.y * nrhs + r) * n + i] = acc[r][q];
             else
                 y[(size_t) r * n + i] = acc[r][q];
+        }
+    }
+}
+
+// dense matvec for several right-hand sides on the FP64 tensor cores: y[r] = A x[r] for
+// r < nrhs <= 8 as a skinny GEMM, one mma.sync m8n8k4 (FP64 in, FP64 accumulate) per 8 rows x
+// 4 columns x 8 right-hand sides. The 8 right-hand sides are the n = 8 of the MMA, so each lane
+// takes its x operand straight from global memory (x is L2-resident) and no broadcast of x
+// through shared memory is needed, which is what limits the FMA form at 8 right-hand sides.
+// The MMA accumulates its k = 4 products in order, so the sums are those of a per-row FMA
+// chain over the columns.
+// Lane (g, t) = (lane / 4, lane % 4) reads column c0 + t in 16-byte loads of kPer = 16 / sizeof(T)
+// rows; load h starts at row rowbase + 8 kPer h + kPer g for FP64 entries, so the 8 lanes of one
+// column read 128 contiguous bytes per load, and at rowbase + 8 g + kPer h for FP32 entries, the
+// lane's 8 rows side by side (measured faster for FP32, slower for FP64). Entry rt
+// (h = rt / kPer, j = rt % kPer) is the A fragment of row tile rt, whose rows are those of
+// entry rt over the 8 lane groups g; the accumulator pair of tile rt holds that row for
+// right-hand sides 2t and 2t + 1.
+// A warp covers 64 rows; the column range is split over gridDim.y as in dense_matvec_kernel.
+// Entries are streamed with evict-first loads.
+__device__ __forceinline__ void mma_884(double& d0, double& d1, double a, double b)
+{
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+        : "+d"(d0), "+d"(d1)
+        : "d"(a), "d"(b));
+}
+
+constexpr int kMmaRowsPerCta = 512;  // 8 warps x 64 rows
+
+// (256, 1): ptxas then keeps more loads in flight (110 / 90 registers for FP32 / FP64 entries,
+// 2 CTAs per SM); the default heuristic gives 76 / 64 registers and ran 5 % / 25 % slower
+template<typename T>
+__global__ void __launch_bounds__(256, 1)
+    dense_mma_kernel(const T* __restrict__ A, int n, size_t ld, const double* __restrict__ x, int nrhs,
+                     double* __restrict__ y, double* __restrict__ partial)
+{
+    constexpr int kU = sizeof(T) == 4 ? 4 : 2;  // column chunks of 4 in flight: 128 bytes per lane
+    constexpr int kPer = 16 / (int) sizeof(T);     // rows per 16-byte load
+    constexpr int kLoads = 8 / kPer;
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int rowbase = blockIdx.x * kMmaRowsPerCta + (threadIdx.x >> 5) * 64;
+    const int per = (n + gridDim.y - 1) / gridDim.y;
+    const int e0 = blockIdx.y * per;
+    const int e1 = min(n, e0 + per);
+    const double* xg = x + (size_t) min(g, nrhs - 1) * n;
+    const bool rhs_ok = g < nrhs;
+    // load h starts at row r0 + step h (step a compile-time constant); a load is issued when its
+    // first row is inside the matrix: ld is a multiple of 4 and that row one of kPer, so a
+    // started group of kPer rows ends below ld
+    constexpr int kStep = sizeof(T) == 4 ? kPer : 8 * kPer;
+    const int r0 = sizeof(T) == 4 ? rowbase + 8 * g : rowbase + kPer * g;
+    double acc[8][2];
+#pragma unroll
+    for (int rt = 0; rt < 8; rt++)
+        acc[rt][0] = acc[rt][1] = 0.;
+    if (rowbase < n) {
+        for (int c0 = e0; c0 < e1; c0 += 4 * kU) {
+            T a[kU][8];
+            double b[kU];
+#pragma unroll
+            for (int u = 0; u < kU; u++) {
+                const int c = c0 + 4 * u + t;
+                const bool col_ok = c < e1;
+                const T* p = A + (size_t) (col_ok ? c : e0) * ld + (r0 < n ? r0 : 0);
+#pragma unroll
+                for (int h = 0; h < kLoads; h++) {
+                    const bool ok = col_ok && r0 + kStep * h < n;
+                    if constexpr (sizeof(T) == 4) {
+                        float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (ok)
+                            w = __ldcs(reinterpret_cast<const float4*>(p + kStep * h));
+                        a[u][4 * h] = w.x, a[u][4 * h + 1] = w.y, a[u][4 * h + 2] = w.z, a[u][4 * h + 3] = w.w;
+                    }
+                    else {
+                        double2 w = make_double2(0., 0.);
+                        if (ok)
+                            w = __ldcs(reinterpret_cast<const double2*>(p + kStep * h));
+                        a[u][2 * h] = w.x, a[u][2 * h + 1] = w.y;
+                    }
+                }
+                b[u] = (col_ok && rhs_ok) ? __ldg(xg + c) : 0.;
+            }
+#pragma unroll
+            for (int u = 0; u < kU; u++)
+#pragma unroll
+                for (int rt = 0; rt < 8; rt++)
+                    mma_884(acc[rt][0], acc[rt][1], (double) a[u][rt], b[u]);
+        }
+    }
+#pragma unroll
+    for (int rt = 0; rt < 8; rt++) {
+        const int i = r0 + kStep * (rt / kPer) + rt % kPer;  // increasing in rt
+        if (i >= n)
+            break;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int r = 2 * t + h;
+            if (r < nrhs) {
+                if (partial)
+                    partial[((size_t) blockIdx.y * nrhs + r) * n + i] = acc[rt][h];
+                else
+                    y[(size_t) r * n + i] = acc[rt][h];
+            }
         }
     }
 }

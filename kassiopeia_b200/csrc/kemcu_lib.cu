@@ -404,14 +404,25 @@ int apply_op(kemcu_ctx* ctx, int op, const double* d_x, double* d_y, int nrhs)
         }
         return KEMCU_OK;
     }
-    // dense operator: V rows per thread, enough CTAs for ~8 per SM, columns split to match
-    // rows per thread (dense_rows); one wave of resident CTAs, the column range split to fill it
+    // dense operator: 256 V rows per CTA; the column range is split S ways. Every CTA does the
+    // same work, so the time goes as waves / S with waves = ceil(rows_blocks S / resident CTAs):
+    // S is the smallest split that minimises it (up to 128 ways), which fills the GPU whether the
+    // row blocks are fewer or more than one wave
     auto launch = [&](auto kernel, const auto* A, int V) -> int {
         const size_t rows_blocks = (n + 256 * (size_t) V - 1) / (256 * (size_t) V);
         int per_sm = 0;
         KC(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0));
-        size_t split = std::max((size_t) 1, (size_t) ctx->num_sms * std::max(1, per_sm) / rows_blocks);
-        split = std::min(split, (size_t) std::max(1, n / 256));
+        const size_t resident = (size_t) ctx->num_sms * std::max(1, per_sm);
+        const size_t max_split = std::min((size_t) 128, (size_t) std::max(1, n / 256));
+        size_t split = 1;
+        double best = 1e300;
+        for (size_t s = 1; s <= max_split; s++) {
+            const double cost = (double) ((rows_blocks * s + resident - 1) / resident) / (double) s;
+            if (cost < best * (1. - 1e-9)) {
+                best = cost;
+                split = s;
+            }
+        }
         double* partial = nullptr;
         if (split > 1) {
             void* p;
@@ -430,11 +441,13 @@ int apply_op(kemcu_ctx* ctx, int op, const double* d_x, double* d_y, int nrhs)
         }
         return KEMCU_OK;
     };
+    // one right-hand side: FMA kernel, HBM-bound; several: the FP64 tensor-core kernel
+    static_assert(kMaxRhs <= 8, "dense_mma_kernel takes at most 8 right-hand sides");
     if (op == kDense64)
         return nrhs == 1 ? launch(dense_matvec_kernel<double, 1>, ctx->d_a64, dense_rows<double, 1>())
-                         : launch(dense_matvec_kernel<double, kMaxRhs>, ctx->d_a64, dense_rows<double, kMaxRhs>());
+                         : launch(dense_mma_kernel<double>, ctx->d_a64, kMmaRowsPerCta / 256);
     return nrhs == 1 ? launch(dense_matvec_kernel<float, 1>, ctx->d_a32, dense_rows<float, 1>())
-                     : launch(dense_matvec_kernel<float, kMaxRhs>, ctx->d_a32, dense_rows<float, kMaxRhs>());
+                     : launch(dense_mma_kernel<float>, ctx->d_a32, kMmaRowsPerCta / 256);
 }
 
 int assemble(kemcu_ctx* ctx, bool want32)

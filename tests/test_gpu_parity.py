@@ -154,6 +154,44 @@ def test_matrix_entries_and_matvec(ctx):
         np.testing.assert_allclose(Y[r], ctx.Multiply(X[r]), rtol=1e-13, atol=1e-12 * np.abs(Y).max())
 
 
+@pytest.mark.parametrize("nrhs", [2, 3, 8])
+def test_assembled_multi_rhs_against_reference_matrix(ctx, nrhs):
+    # the several-right-hand-side dense kernel (FP64 tensor cores) on an operator whose size is
+    # not a multiple of its 64-row warp tiles or 4-column chunks, with 2, 3 or 8 right-hand sides
+    fx = golden.load("mixed_small")
+    m = golden.mesh_from(fx)
+    ctx.SetGeometry(m)
+    rng = np.random.default_rng(5)
+    X = rng.standard_normal((nrhs, m.n))
+    ref = X @ fx["A"].T
+    scale = np.abs(X) @ np.abs(fx["A"]).T
+    Y64 = ctx.Multiply(X, assembled=True)
+    assert np.max(np.abs(Y64 - ref) / scale) < 1e-12
+    for r in range(nrhs):
+        np.testing.assert_allclose(Y64[r], ctx.Multiply(X[r], assembled=True), rtol=0,
+                                   atol=1e-14 * scale[r].max())
+    # FP32 operator copy: entries rounded to FP32 (2^-24 relative), products and sums in FP64
+    Y32 = ctx.Multiply(X, precision=K.MIXED, assembled=True)
+    assert np.max(np.abs(Y32 - ref) / scale) < 1e-7
+    A32 = fx["A"].astype(np.float32).astype(np.float64)
+    assert np.max(np.abs(Y32 - X @ A32.T) / scale) < 1e-13
+
+
+def test_assembled_multi_rhs_ragged_coax(ctx):
+    # 1,554 rectangles and triangles (1554 = 24 x 64 + 18 rows, column splits not multiples of
+    # 4): the tensor-core dense product against the matrix-free FP64 matvec, 5 right-hand sides
+    m = G.coax(n_phi=21, n_z=31, n_cap_rings=3)
+    ctx.SetGeometry(m)
+    rng = np.random.default_rng(9)
+    X = rng.standard_normal((5, m.n))
+    Yf = ctx.Multiply(X)
+    Ya = ctx.Multiply(X, assembled=True)
+    Y32 = ctx.Multiply(X, precision=K.MIXED, assembled=True)
+    norm = np.abs(Yf).max(axis=1, keepdims=True)
+    assert np.max(np.abs(Ya - Yf) / norm) < 1e-13
+    assert np.max(np.abs(Y32 - Yf) / norm) < 1e-6
+
+
 def test_gmres_plain_matches_reference(ctx):
     # oracle: the direct solution of the reference's own boundary-integral matrix. The
     # reference GMRES converges in the same number of iterations on its implicit estimate,
