@@ -301,11 +301,15 @@ def profile_operator():
     mesh = G.coax(n_phi=60, n_z=120, n_cap_rings=8)
     ctx.SetGeometry(mesh)
     x = np.ones(mesh.n)
-    for prec in (K.MIXED, K.MIXED, K.MIXED, K.FP64, K.FP64):
-        ctx.Multiply(x, precision=prec, assembled=True)  # the first call assembles the operator
+    X = np.stack([x * (r + 1) for r in range(8)])
+    # one right-hand side (dense_matvec_kernel): 3 FP32 then 2 FP64 launches; then 8 right-hand
+    # sides (dense_mma_kernel): 2 FP32 then 2 FP64 launches
+    for prec, xx in ((K.MIXED, x),) * 3 + ((K.FP64, x),) * 2 + ((K.MIXED, X),) * 2 + ((K.FP64, X),) * 2:
+        ctx.Multiply(xx, precision=prec, assembled=True)  # the first call assembles the operator
         entry = 4 if prec == K.MIXED else 8
         ms = ctx.last_kernel_ms
-        print(json.dumps({"operator": "dense " + ("FP32" if prec == K.MIXED else "FP64"), "n": mesh.n, "ms": ms,
+        print(json.dumps({"operator": "dense " + ("FP32" if prec == K.MIXED else "FP64"), "n": mesh.n,
+                          "rhs": 1 if xx.ndim == 1 else xx.shape[0], "ms": ms,
                           "GB/s": mesh.n * mesh.n * entry / (ms * 1e-3) / 1e9}), flush=True)
 
 

@@ -592,14 +592,19 @@ __device__ __forceinline__ void mma_884(double& d0, double& d1, double a, double
 
 constexpr int kMmaRowsPerCta = 512;  // 8 warps x 64 rows
 
-// (256, 1): ptxas then keeps more loads in flight (110 / 90 registers for FP32 / FP64 entries,
-// 2 CTAs per SM); the default heuristic gives 76 / 64 registers and ran 5 % / 25 % slower
+// (256, 1): ptxas then keeps more loads in flight (2 CTAs per SM for FP32 and FP64 entries);
+// its default register heuristic gave fewer registers and ran 5 % / 25 % slower
 template<typename T>
 __global__ void __launch_bounds__(256, 1)
     dense_mma_kernel(const T* __restrict__ A, int n, size_t ld, const double* __restrict__ x, int nrhs,
                      double* __restrict__ y, double* __restrict__ partial)
 {
-    constexpr int kU = sizeof(T) == 4 ? 4 : 2;  // column chunks of 4 in flight: 128 bytes per lane
+    // 2 chunks of 4 columns per stage; FP32 entries run two register stages (loads of the next
+    // stage in flight during the MMAs of this one: 8.46 -> 6.93 ms on a 100,000^2 operator with
+    // 8 right-hand sides), FP64 entries one (already at 1.07x the HBM time; two stages ran 3 %
+    // slower at 142 registers)
+    constexpr int kU = 2;
+    constexpr bool kPipelined = sizeof(T) == 4;
     constexpr int kPer = 16 / (int) sizeof(T);     // rows per 16-byte load
     constexpr int kLoads = 8 / kPer;
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
@@ -618,38 +623,60 @@ __global__ void __launch_bounds__(256, 1)
 #pragma unroll
     for (int rt = 0; rt < 8; rt++)
         acc[rt][0] = acc[rt][1] = 0.;
-    if (rowbase < n) {
-        for (int c0 = e0; c0 < e1; c0 += 4 * kU) {
-            T a[kU][8];
-            double b[kU];
+    // kU chunks of 4 columns starting at column cb: entries into a, x values into b (zeros
+    // outside the row and column ranges, with no memory access there)
+    auto load = [&](T (&a)[kU][8], double (&b)[kU], int cb) {
 #pragma unroll
-            for (int u = 0; u < kU; u++) {
-                const int c = c0 + 4 * u + t;
-                const bool col_ok = c < e1;
-                const T* p = A + (size_t) (col_ok ? c : e0) * ld + (r0 < n ? r0 : 0);
+        for (int u = 0; u < kU; u++) {
+            const int c = cb + 4 * u + t;
+            const bool col_ok = c < e1;
+            const T* p = A + (size_t) (col_ok ? c : e0) * ld + (r0 < n ? r0 : 0);
 #pragma unroll
-                for (int h = 0; h < kLoads; h++) {
-                    const bool ok = col_ok && r0 + kStep * h < n;
-                    if constexpr (sizeof(T) == 4) {
-                        float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
-                        if (ok)
-                            w = __ldcs(reinterpret_cast<const float4*>(p + kStep * h));
-                        a[u][4 * h] = w.x, a[u][4 * h + 1] = w.y, a[u][4 * h + 2] = w.z, a[u][4 * h + 3] = w.w;
-                    }
-                    else {
-                        double2 w = make_double2(0., 0.);
-                        if (ok)
-                            w = __ldcs(reinterpret_cast<const double2*>(p + kStep * h));
-                        a[u][2 * h] = w.x, a[u][2 * h + 1] = w.y;
-                    }
+            for (int h = 0; h < kLoads; h++) {
+                const bool ok = col_ok && r0 + kStep * h < n;
+                if constexpr (sizeof(T) == 4) {
+                    float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (ok)
+                        w = __ldcs(reinterpret_cast<const float4*>(p + kStep * h));
+                    a[u][4 * h] = w.x, a[u][4 * h + 1] = w.y, a[u][4 * h + 2] = w.z, a[u][4 * h + 3] = w.w;
                 }
-                b[u] = (col_ok && rhs_ok) ? __ldg(xg + c) : 0.;
+                else {
+                    double2 w = make_double2(0., 0.);
+                    if (ok)
+                        w = __ldcs(reinterpret_cast<const double2*>(p + kStep * h));
+                    a[u][2 * h] = w.x, a[u][2 * h + 1] = w.y;
+                }
             }
+            b[u] = (col_ok && rhs_ok) ? __ldg(xg + c) : 0.;
+        }
+    };
+    auto mma = [&](const T (&a)[kU][8], const double (&b)[kU]) {
 #pragma unroll
-            for (int u = 0; u < kU; u++)
+        for (int u = 0; u < kU; u++)
 #pragma unroll
-                for (int rt = 0; rt < 8; rt++)
-                    mma_884(acc[rt][0], acc[rt][1], (double) a[u][rt], b[u]);
+            for (int rt = 0; rt < 8; rt++)
+                mma_884(acc[rt][0], acc[rt][1], (double) a[u][rt], b[u]);
+    };
+    if (rowbase < n) {
+        if constexpr (kPipelined) {
+            // two register stages (a stage past e1 loads zeros and adds nothing)
+            T a0[kU][8], a1[kU][8];
+            double b0[kU], b1[kU];
+            load(a0, b0, e0);
+            for (int c0 = e0; c0 < e1; c0 += 8 * kU) {
+                load(a1, b1, c0 + 4 * kU);
+                mma(a0, b0);
+                load(a0, b0, c0 + 8 * kU);
+                mma(a1, b1);
+            }
+        }
+        else {
+            for (int c0 = e0; c0 < e1; c0 += 4 * kU) {
+                T a[kU][8];
+                double b[kU];
+                load(a, b, c0);
+                mma(a, b);
+            }
         }
     }
 #pragma unroll
