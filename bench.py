@@ -278,11 +278,12 @@ def run_native(args, rank, world, dist):
         for _ in range(2):
             c5.Multiply(B * 1e-12, precision=K.FP64)
         t8 = c5.last_kernel_ms
-        _, s5 = c5.Solve(B, tol=TOL, mode=K.SOLVE_ASSEMBLED)
+        _, s5 = c5.Solve(B, tol=TOL, mode=K.SOLVE_ASSEMBLED)  # allocates and assembles the operator
+        _, s5r = c5.Solve(B, tol=TOL, mode=K.SOLVE_ASSEMBLED)
         extra["c5_stacked_rings_100k_8rhs"] = {
             "matrix_free_fp64_matvec_ms_1rhs": t1, "matrix_free_fp64_matvec_ms_8rhs": t8,
-            "assembled_solve_s": s5["seconds"], "krylov_iterations": s5["iterations"],
-            "rel_residual": s5["rel_residual"]}
+            "assembled_solve_s": s5["seconds"], "assembled_solve_repeat_s": s5r["seconds"],
+            "krylov_iterations": s5["iterations"], "rel_residual": s5["rel_residual"]}
 
     res = dict(
         ms_mixed=ms_mixed, ms_fp64=ms_fp64, wall_mixed=wall_mixed, e2e_s=e2e_s, launches=int(launches),
