@@ -34,24 +34,59 @@ __device__ __forceinline__ double block_sum(double v, double* sh)
 
 // h[r][k0 + k] = sum_i V[k0 + k][r][i] * w[r][i] for k < nk (nk <= 64 per launch); h row stride hs.
 // grid (kDotBlocks, nrhs); partial[r][k][blk]; counter[r] must start at 0 and is reset.
+// A CTA covers one slice of the rows i. Its 8 warps take the basis vectors in groups of 8: with
+// G = ceil(nk / 8) groups, 8 / G warps share a group and stride over the rows, each lane keeping
+// 8 running sums (one w load serves 8 basis entries); warp shuffles then reduce the lanes,
+// shared memory the warps of a group, and the last CTA of a right-hand side sums the slices in
+// block order, so the result does not depend on scheduling.
 __global__ void __launch_bounds__(kDotThreads) multi_dot_kernel(const double* __restrict__ V, const double* __restrict__ w,
                                                                 int n, int nrhs, int k0, int nk, double* __restrict__ partial,
                                                                 unsigned* __restrict__ counter, double* __restrict__ h, int hs)
 {
-    __shared__ double sh[32];
+    static_assert(kDotThreads == 256, "8 warps of 8 basis vectors cover the 64 vectors of a launch");
+    __shared__ double s_red[8][8];
     __shared__ bool last;
     const int r = blockIdx.y;
     const int per = (n + gridDim.x - 1) / gridDim.x;
     const int i0 = blockIdx.x * per, i1 = min(n, i0 + per);
     const double* wr = w + (size_t) r * n;
-    for (int k = 0; k < nk; k++) {
-        const double* vk = V + ((size_t) (k0 + k) * nrhs + r) * n;
-        double s = 0.;
-        for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x)
-            s += vk[i] * wr[i];
-        s = block_sum(s, sh);
-        if (threadIdx.x == 0)
-            partial[((size_t) r * 64 + k) * gridDim.x + blockIdx.x] = s;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int groups = (nk + 7) >> 3;
+    const int wpg = max(1, 8 / groups);  // warps per group of 8 basis vectors
+    const int grp = warp / wpg, slice = warp % wpg;
+    double acc[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++)
+        acc[q] = 0.;
+    if (grp < groups) {
+        const int kb = 8 * grp, kn = min(8, nk - kb);
+        const size_t vstride = (size_t) nrhs * n;
+        const double* vb = V + ((size_t) (k0 + kb) * nrhs + r) * n;
+        for (int i = i0 + 32 * slice + lane; i < i1; i += 32 * wpg) {
+            const double wi = wr[i];
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if (q < kn)
+                    acc[q] = fma(vb[q * vstride + i], wi, acc[q]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        double v = acc[q];
+        for (int o = 16; o > 0; o >>= 1)
+            v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0)
+            s_red[warp][q] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 64) {
+        const int g2 = threadIdx.x >> 3, q = threadIdx.x & 7;
+        if (g2 < groups && 8 * g2 + q < nk) {
+            double v = 0.;
+            for (int sl = 0; sl < wpg; sl++)
+                v += s_red[g2 * wpg + sl][q];
+            partial[((size_t) r * 64 + 8 * g2 + q) * gridDim.x + blockIdx.x] = v;
+        }
     }
     __threadfence();
     __syncthreads();
