@@ -525,7 +525,7 @@ int gmres_core(kemcu_ctx* ctx, int op, const double* d_b, double* d_x, int nrhs,
     KC(cudaMemcpyAsync(hb.data(), h2, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     KC(cudaStreamSynchronize(ctx->stream));
     std::vector<double> bnorm(nrhs), p((size_t) nrhs * hs, 0.), cs((size_t) nrhs * hs), sn((size_t) nrhs * hs);
-    std::vector<std::vector<double>> H(nrhs, std::vector<double>((size_t) hs * hs, 0.));  // column-major R
+    std::vector<std::vector<double>> H(nrhs);  // column-major R, one column of hs added per iteration
     std::vector<int> kfin(nrhs, 0);
     std::vector<char> done(nrhs, 0);
     for (int r = 0; r < nrhs; r++) {
@@ -593,6 +593,7 @@ int gmres_core(kemcu_ctx* ctx, int op, const double* d_b, double* d_x, int nrhs,
         for (int r = 0; r < nrhs; r++) {
             if (done[r])
                 continue;
+            H[r].resize((size_t) (j + 1) * hs, 0.);
             double* col = H[r].data() + (size_t) j * hs;
             for (int k = 0; k <= j; k++)
                 col[k] = hcol[(size_t) r * hs + k] + hcol2[(size_t) r * hs + k];
