@@ -11,12 +11,19 @@
  *
  * Element encoding (the flattened KSurfaceContainer, KSurfaceContainer.cc:36-72; element
  * index = matrix row/column index):
- *   shape[i]    KEMCU_TRIANGLE | KEMCU_RECTANGLE | KEMCU_LINE_SEGMENT
+ *   shape[i]    KEMCU_TRIANGLE | KEMCU_RECTANGLE | KEMCU_LINE_SEGMENT, or
+ *               KEMCU_CONIC_SECTION | KEMCU_RING (axisymmetric; a context holds either kind,
+ *               not both)
  *   boundary[i] KEMCU_DIRICHLET (value = potential, KDirichletBoundary::GetBoundaryValue)
- *               KEMCU_NEUMANN   (value = normal boundary flux, KNeumannBoundary)
+ *               KEMCU_NEUMANN   (value = normal boundary flux, KNeumannBoundary; planar only)
  *   geom[11*i]  triangle / rectangle: A, B, P0(xyz), N1(xyz), N2(xyz)
  *               (KTriangle.hh:125-130, KRectangle.hh:132-137; P1 = P0 + A*N1, P2 = P0 + B*N2)
  *               line segment: P0(xyz), P1(xyz), diameter, 0, 0, 0, 0 (KLineSegment.hh:74-76)
+ *               conic section: r0, z0, r1, z1, 0... (KConicSection.hh: P0 = (r0, 0, z0),
+ *               P1 = (r1, 0, z1)); ring: r, z, 0... (KRing.hh: P = (r, 0, z)). Their integrals
+ *               are KElectrostaticAnalyticConicSectionIntegrator / ...RingIntegrator, FP64
+ *               whatever the precision argument; tracking, the adjoint, Robin Hood and the
+ *               band histogram take planar elements only (KEMCU_EINVAL otherwise).
  * Units are SI; 1/(4 pi eps0) and eps0 come from kemcu_config (KEMConstants, KEMConstants.cc:11-12).
  */
 #ifndef KEMCU_H
@@ -38,7 +45,13 @@ extern "C" {
 #define KEMCU_ENOMEM (-6)       /* device allocation failed or budget exceeded */
 #define KEMCU_ESTATE (-7)       /* call out of order (e.g. no geometry set) */
 
-enum kemcu_shape { KEMCU_TRIANGLE = 0, KEMCU_RECTANGLE = 1, KEMCU_LINE_SEGMENT = 2 };
+enum kemcu_shape {
+    KEMCU_TRIANGLE = 0,
+    KEMCU_RECTANGLE = 1,
+    KEMCU_LINE_SEGMENT = 2,
+    KEMCU_CONIC_SECTION = 3,
+    KEMCU_RING = 4
+};
 enum kemcu_boundary { KEMCU_DIRICHLET = 0, KEMCU_NEUMANN = 1 };
 /* arithmetic form of the element integrals */
 enum kemcu_precision {

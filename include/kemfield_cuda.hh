@@ -129,8 +129,21 @@ class KCUDASurfaceContainer
                 }
                 g[6] = l->GetDiameter();
             }
+            else if (auto* cs = dynamic_cast<KConicSection*>(s->GetShape())) {
+                shape[i] = KEMCU_CONIC_SECTION;
+                g[0] = cs->GetR0();
+                g[1] = cs->GetZ0();
+                g[2] = cs->GetR1();
+                g[3] = cs->GetZ1();
+            }
+            else if (auto* rg = dynamic_cast<KRing*>(s->GetShape())) {
+                shape[i] = KEMCU_RING;
+                g[0] = rg->GetR();
+                g[1] = rg->GetZ();
+            }
             else
-                throw KEMSimpleException("kemcu: only triangles, rectangles and line segments are supported");
+                throw KEMSimpleException("kemcu: only triangles, rectangles, line segments, conic sections and rings "
+                                         "are supported");
             if (auto* d = dynamic_cast<KBoundaryType<KElectrostaticBasis, KDirichletBoundary>*>(s->GetBoundary())) {
                 boundary[i] = KEMCU_DIRICHLET;
                 value[i] = d->GetBoundaryValue();

@@ -369,6 +369,14 @@ template<bool MIXED> __device__ __forceinline__ double entry(const double* e, co
     return t.diag;
 }
 
+// one entry A(i, j) (kemcu_matrix_element), the FP64 form the matvec uses
+__global__ void entry_kernel(const double* __restrict__ rec, const TargetRec* __restrict__ tgt, int i, int j,
+                             double* __restrict__ a)
+{
+    const TargetRec t = tgt[i];
+    *a = entry<false>(rec + (size_t) j * rRecSize, t, v3(t.cen[0], t.cen[1], t.cen[2]));
+}
+
 // K2: y[r][i] = sum_j A(i, j) x[r][j] for r < nrhs (nrhs <= NR <= kMaxRhs), entries
 // recomputed on the fly (KMatrix::Multiply over KBoundaryIntegralMatrix::operator(),
 // KMatrix.hh:92-99, KBoundaryIntegralMatrix.hh:31-55). Same element ring as K1, with the

@@ -6,6 +6,7 @@
 #include "kemcu.h"
 #include "kemcu_device.cuh"
 #include "kemcu_kernels.cuh"
+#include "kemcu_axisym.cuh"
 #include "kemcu_solver.cuh"
 #include "kemcu_tables.cuh"
 #include "kemcu_track.cuh"
@@ -58,6 +59,8 @@ struct kemcu_ctx
     TargetRec* d_tgt = nullptr;
     double* d_sigma = nullptr;
     bool have_sigma = false;
+    // all elements axisymmetric (conic sections, rings): records in the AxRec layout
+    bool axisym = false;
     // assembled operator (column-major)
     double* d_a64 = nullptr;
     float* d_a32 = nullptr;
@@ -134,6 +137,37 @@ int ensure(kemcu_ctx* ctx, int slot, size_t bytes, void** out)
 
 // element record and matrix-row target of one element, in the reference's FP64 operation
 // order (no FMA: the host compiler targets baseline x86-64)
+// axisymmetric element record (AxRec). Caller layout: conic section geom = (r0, z0, r1, z1),
+// ring geom = (r, z) (KConicSection.hh: P0 = (r0, 0, z0), P1 = (r1, 0, z1); KRing.hh: P = (r, 0, z)).
+// Prefactors and the centroid as KElectrostaticAnalyticConicSectionIntegrator.cc:91,
+// KElectrostaticAnalyticRingIntegrator.cc:36 and KConicSection.hh:29-32 / KRing.hh:29-32 form them.
+void build_axisym_record(const double* g, int shape, double value, const Constants& K, double* r, double& rhs)
+{
+    if (shape == KEMCU_RING) {
+        r[aType] = kAxRing;
+        r[aZa] = r[aZb] = g[1];
+        r[aRa] = r[aRb] = g[0];
+        r[aLen] = 1.;
+        r[aPre] = 1. / (g[0] * 2. * K.pi * K.pi * K.eps0);
+        r[aCx] = g[0];
+        r[aCz] = g[1];
+    }
+    else {
+        r[aType] = kAxConic;
+        r[aZa] = g[1];
+        r[aRa] = g[0];
+        r[aZb] = g[3];
+        r[aRb] = g[2];
+        const double dx = g[0] - g[2], dz = g[1] - g[3];
+        r[aLen] = sqrt(dx * dx + 0. * 0. + dz * dz);
+        r[aPre] = 1. / (K.pi * K.eps0);
+        r[aCx] = (g[0] + g[2]) * .5;
+        r[aCz] = (g[1] + g[3]) * .5;
+    }
+    r[aCy] = 0.;
+    rhs = value;
+}
+
 void build_record(const double* g, int shape, int boundary, double value, const Constants& K, double* r,
                   TargetRec& t, double& rhs)
 {
@@ -260,9 +294,29 @@ int grid_split(const kemcu_ctx* ctx, size_t n_pts, size_t n_elem)
     return (int) std::max((size_t) 1, split);
 }
 
+// axisymmetric elements: FP64 element integrals whatever the precision argument
+int launch_axisym_field(kemcu_ctx* ctx, const double* d_pts, size_t n, double* d_out, int what)
+{
+    const unsigned grid = (unsigned) ((n + kAxThreads - 1) / kAxThreads);
+    const int ne = (int) ctx->n, np = (int) n;
+    if (what == KEMCU_POTENTIAL)
+        axisym_field_kernel<true, false><<<grid, kAxThreads, 0, ctx->stream>>>(ctx->d_rec, rRecSize, ctx->d_sigma, ne,
+                                                                               d_pts, np, d_out);
+    else if (what == KEMCU_FIELD)
+        axisym_field_kernel<false, true><<<grid, kAxThreads, 0, ctx->stream>>>(ctx->d_rec, rRecSize, ctx->d_sigma, ne,
+                                                                               d_pts, np, d_out);
+    else
+        axisym_field_kernel<true, true><<<grid, kAxThreads, 0, ctx->stream>>>(ctx->d_rec, rRecSize, ctx->d_sigma, ne,
+                                                                              d_pts, np, d_out);
+    KCHECK_LAUNCH();
+    return KEMCU_OK;
+}
+
 // field at device points; d_out n x 4
 int launch_field(kemcu_ctx* ctx, const double* d_pts, size_t n, double* d_out, int precision, int what)
 {
+    if (ctx->axisym)
+        return launch_axisym_field(ctx, d_pts, n, d_out, what);
     const int split = grid_split(ctx, n, ctx->n);
     double* partial = nullptr;
     if (split > 1) {
@@ -341,6 +395,14 @@ int check_ready(kemcu_ctx* ctx, bool need_sigma)
     return KEMCU_OK;
 }
 
+// entry points whose kernels take planar elements only (triangles, rectangles, wires)
+int planar_only(kemcu_ctx* ctx, const char* what)
+{
+    if (ctx->axisym)
+        return fail(ctx, KEMCU_EINVAL, "%s is not available for axisymmetric elements (conic sections, rings)", what);
+    return KEMCU_OK;
+}
+
 struct Timer
 {
     kemcu_ctx* ctx;
@@ -370,6 +432,15 @@ enum OpKind
 int apply_op(kemcu_ctx* ctx, int op, const double* d_x, double* d_y, int nrhs)
 {
     const int n = (int) ctx->n;
+    if ((op == kFree64 || op == kFreeMixed) && ctx->axisym) {
+        const unsigned grid = (unsigned) ((n + kAxThreads - 1) / kAxThreads);
+        if (nrhs == 1)
+            axisym_matvec_kernel<1><<<grid, kAxThreads, 0, ctx->stream>>>(ctx->d_rec, rRecSize, n, d_x, nrhs, d_y);
+        else
+            axisym_matvec_kernel<kMaxRhs><<<grid, kAxThreads, 0, ctx->stream>>>(ctx->d_rec, rRecSize, n, d_x, nrhs, d_y);
+        KCHECK_LAUNCH();
+        return KEMCU_OK;
+    }
     if (op == kFree64 || op == kFreeMixed) {
         const int split = grid_split(ctx, n, n);
         double* partial = nullptr;
@@ -475,6 +546,12 @@ int assemble(kemcu_ctx* ctx, bool want32)
         cudaGetLastError();
         ctx->d_a32 = nullptr;
         return fail(ctx, KEMCU_ENOMEM, "allocation of the FP32 operator copy failed");
+    }
+    if (ctx->axisym) {
+        axisym_assemble_kernel<<<(unsigned) ((n + kAxThreads - 1) / kAxThreads), kAxThreads, 0, ctx->stream>>>(
+            ctx->d_rec, rRecSize, (int) n, 0, (int) n, ld, ctx->d_a64, fill32 ? ctx->d_a32 : nullptr);
+        KCHECK_LAUNCH();
+        return KEMCU_OK;
     }
     const int split = grid_split(ctx, n, n);
     dim3 grid((unsigned) ((n + kThreads - 1) / kThreads), (unsigned) split);
@@ -820,16 +897,29 @@ int kemcu_set_geometry(kemcu_ctx* ctx, size_t n, const int32_t* shape, const int
     if (n == 0 || n > (size_t) 0x7fffffff || !shape || !boundary || !geom11 || !value)
         return fail(ctx, KEMCU_EINVAL, "invalid geometry arguments (n = %zu)", n);
     KC(cudaSetDevice(ctx->device));
+    size_t n_axisym = 0;
     for (size_t i = 0; i < n; i++) {
-        if (shape[i] < 0 || shape[i] > 2 || (boundary[i] != 0 && boundary[i] != 1))
+        if (shape[i] < 0 || shape[i] > KEMCU_RING || (boundary[i] != 0 && boundary[i] != 1))
             return fail(ctx, KEMCU_EINVAL, "element %zu: shape %d / boundary %d not supported", i, shape[i], boundary[i]);
         for (int c = 0; c < 11; c++)
             if (!std::isfinite(geom11[11 * i + c]))
                 return fail(ctx, KEMCU_EINVAL, "element %zu: non-finite geometry", i);
         const double* g = geom11 + 11 * i;
-        if (shape[i] != kLineSegment && !(g[0] > 0. && g[1] > 0.))
+        if (shape[i] == KEMCU_CONIC_SECTION || shape[i] == KEMCU_RING) {
+            n_axisym++;
+            if (boundary[i] != KEMCU_DIRICHLET)
+                return fail(ctx, KEMCU_EINVAL, "element %zu: axisymmetric elements take Dirichlet boundaries only", i);
+            if (shape[i] == KEMCU_RING ? !(g[0] > 0.)
+                                       : !(g[0] >= 0. && g[2] >= 0. && (g[0] != g[2] || g[1] != g[3])))
+                return fail(ctx, KEMCU_EINVAL, "element %zu: radii must be non-negative (a ring's positive) and a "
+                                               "conic section's end points distinct", i);
+        }
+        else if (shape[i] != kLineSegment && !(g[0] > 0. && g[1] > 0.))
             return fail(ctx, KEMCU_EINVAL, "element %zu: side lengths must be positive", i);
     }
+    if (n_axisym != 0 && n_axisym != n)
+        return fail(ctx, KEMCU_EINVAL, "axisymmetric elements (conic sections, rings) cannot share a context with "
+                                       "triangles, rectangles or line segments");
     // release everything that depends on the old geometry
     cudaFree(ctx->d_rec);
     cudaFree(ctx->d_tgt);
@@ -847,9 +937,15 @@ int kemcu_set_geometry(kemcu_ctx* ctx, size_t n, const int32_t* shape, const int
     ctx->h_tgt.assign(n, TargetRec{});
     ctx->h_rhs.assign(n, 0.);
     ctx->h_shape.assign(shape, shape + n);
-    for (size_t i = 0; i < n; i++)
-        build_record(geom11 + 11 * i, shape[i], boundary[i], value[i], ctx->k, ctx->h_rec.data() + i * rRecSize,
-                     ctx->h_tgt[i], ctx->h_rhs[i]);
+    ctx->axisym = n_axisym != 0;
+    for (size_t i = 0; i < n; i++) {
+        if (ctx->axisym)
+            build_axisym_record(geom11 + 11 * i, shape[i], value[i], ctx->k, ctx->h_rec.data() + i * rRecSize,
+                                ctx->h_rhs[i]);
+        else
+            build_record(geom11 + 11 * i, shape[i], boundary[i], value[i], ctx->k, ctx->h_rec.data() + i * rRecSize,
+                         ctx->h_tgt[i], ctx->h_rhs[i]);
+    }
     KC(cudaMalloc(&ctx->d_rec, n * rRecSize * sizeof(double)));
     KC(cudaMalloc(&ctx->d_tgt, n * sizeof(TargetRec)));
     KC(cudaMalloc(&ctx->d_sigma, n * sizeof(double)));
@@ -966,6 +1062,12 @@ int kemcu_field_dev_noalloc(kemcu_ctx* ctx, const double* dP, size_t n, double* 
         return fail(ctx, KEMCU_ESTATE, "no-allocation scratch not set up");
     KC(cudaSetDevice(ctx->device));
     Timer t(ctx);
+    if (ctx->axisym) {
+        if ((rc = launch_axisym_field(ctx, dP, n, dout4, what)))
+            return rc;
+        t.stop();
+        return KEMCU_OK;
+    }
     const size_t cap = KEMCU_NOALLOC_SCRATCH_BYTES / sizeof(double);
     const int split = (int) std::min((size_t) grid_split(ctx, n, ctx->n), std::max((size_t) 1, cap / (4 * n)));
     double* partial = split > 1 ? ctx->noalloc_scratch : nullptr;
@@ -1032,17 +1134,18 @@ int kemcu_matrix_element(kemcu_ctx* ctx, size_t i, size_t j, double* a)
     if (i >= ctx->n || j >= ctx->n || !a)
         return fail(ctx, KEMCU_EINVAL, "matrix index out of range");
     KC(cudaSetDevice(ctx->device));
-    // one column j applied to the unit vector restricted to row i: y = A e_j, read y_i
-    void *dx, *dy;
-    if ((rc = ensure(ctx, sVec0, ctx->n * sizeof(double), &dx)) || (rc = ensure(ctx, sVec1, ctx->n * sizeof(double), &dy)))
+    // one thread computes the entry, in the FP64 form of the matvec
+    void* d;
+    if ((rc = ensure(ctx, sVec1, sizeof(double), &d)))
         return rc;
-    KC(cudaMemsetAsync(dx, 0, ctx->n * sizeof(double), ctx->stream));
-    const double one = 1.;
-    KC(cudaMemcpyAsync((double*) dx + j, &one, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    if ((rc = clear_pipe_flag(ctx)) || (rc = apply_op(ctx, kFree64, (const double*) dx, (double*) dy, 1)))
-        return rc;
-    KC(cudaMemcpyAsync(a, (double*) dy + i, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    return pipe_status(ctx, "matrix element");
+    if (ctx->axisym)
+        axisym_entry_kernel<<<1, 1, 0, ctx->stream>>>(ctx->d_rec, rRecSize, (int) i, (int) j, (double*) d);
+    else
+        entry_kernel<<<1, 1, 0, ctx->stream>>>(ctx->d_rec, ctx->d_tgt, (int) i, (int) j, (double*) d);
+    KCHECK_LAUNCH();
+    KC(cudaMemcpyAsync(a, d, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    KC(cudaStreamSynchronize(ctx->stream));
+    return KEMCU_OK;
 }
 
 int kemcu_matvec(kemcu_ctx* ctx, const double* x, double* y, int n_rhs, int precision, int assembled)
@@ -1203,7 +1306,7 @@ unsigned long long kemcu_launch_count(const kemcu_ctx* ctx)
 int kemcu_band_histogram(kemcu_ctx* ctx, const double* P, size_t n, long long* counts)
 {
     int rc = check_ready(ctx, false);
-    if (rc)
+    if (rc || (rc = planar_only(ctx, "the band histogram")))
         return rc;
     if (!P || !counts || n == 0 || n > (size_t) 0x7fffffff)
         return fail(ctx, KEMCU_EINVAL, "invalid histogram arguments");

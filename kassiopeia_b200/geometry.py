@@ -9,7 +9,11 @@ in the reference's element encoding:
   ``P1 = P0 + A*N1`` and ``P2 = P0 + B*N2`` (KTriangle::SetValues(p0, p1, p2),
   KEMField/Source/Surfaces/src/KTriangle.cc:18-28; KRectangle.hh:132-137);
 * line segment: ``geom = (P0x, P0y, P0z, P1x, P1y, P1z, diameter, 0, 0, 0, 0)``
-  (KEMField/Source/Surfaces/include/KLineSegment.hh:74-76).
+  (KEMField/Source/Surfaces/include/KLineSegment.hh:74-76);
+* conic section: ``geom = (r0, z0, r1, z1, 0, ...)``, the generator from (r0, z0) to (r1, z1)
+  turned about the z axis (KEMField/Source/Surfaces/include/KConicSection.hh);
+* ring: ``geom = (r, z, 0, ...)`` (KEMField/Source/Surfaces/include/KRing.hh).
+  A mesh holds either planar elements or axisymmetric ones.
 
 Every generator is deterministic for a given seed (numpy ``default_rng``).
 """
@@ -20,7 +24,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-TRIANGLE, RECTANGLE, LINE_SEGMENT = 0, 1, 2
+TRIANGLE, RECTANGLE, LINE_SEGMENT, CONIC_SECTION, RING = 0, 1, 2, 3, 4
 DIRICHLET, NEUMANN = 0, 1
 
 
@@ -58,6 +62,11 @@ class Mesh:
         c[tri] = g[tri, 2:5] + (g[tri, 0:1] * g[tri, 5:8] + g[tri, 1:2] * g[tri, 8:11]) / 3.0
         c[rect] = g[rect, 2:5] + 0.5 * g[rect, 0:1] * g[rect, 5:8] + 0.5 * g[rect, 1:2] * g[rect, 8:11]
         c[line] = 0.5 * (g[line, 0:3] + g[line, 3:6])
+        conic = self.shape == CONIC_SECTION
+        ring = self.shape == RING
+        c[conic] = np.stack([0.5 * (g[conic, 0] + g[conic, 2]), np.zeros(int(conic.sum())),
+                             0.5 * (g[conic, 1] + g[conic, 3])], axis=1)
+        c[ring] = np.stack([g[ring, 0], np.zeros(int(ring.sum())), g[ring, 1]], axis=1)
         return c
 
     def areas(self) -> np.ndarray:
@@ -70,7 +79,59 @@ class Mesh:
         a[tri] = 0.5 * g[tri, 0] * g[tri, 1] * np.linalg.norm(cr, axis=1)
         a[rect] = g[rect, 0] * g[rect, 1]
         a[line] = np.pi * g[line, 6] * np.linalg.norm(g[line, 3:6] - g[line, 0:3], axis=1)
+        conic = self.shape == CONIC_SECTION
+        a[conic] = np.pi * (g[conic, 0] + g[conic, 2]) * np.hypot(g[conic, 0] - g[conic, 2], g[conic, 1] - g[conic, 3])
+        a[self.shape == RING] = 2.0 * np.pi * g[self.shape == RING, 0]  # KRing::Area (KRing.cc:20-23)
         return a
+
+
+def axisymmetric(shape, r0, z0, r1=None, z1=None, value=1.0, name: str = "") -> Mesh:
+    """Conic sections (``r1``, ``z1`` given) or rings from per-element arrays, Dirichlet."""
+    r0 = np.atleast_1d(np.asarray(r0, np.float64))
+    n = r0.shape[0]
+    geom = np.zeros((n, 11))
+    geom[:, 0] = r0
+    geom[:, 1] = np.broadcast_to(np.asarray(z0, np.float64), (n,))
+    if r1 is not None:
+        geom[:, 2] = np.broadcast_to(np.asarray(r1, np.float64), (n,))
+        geom[:, 3] = np.broadcast_to(np.asarray(z1, np.float64), (n,))
+    return Mesh(np.full(n, shape, np.int32), np.full(n, DIRICHLET, np.int32), geom,
+                np.broadcast_to(np.asarray(value, np.float64), (n,)).copy(), name=name)
+
+
+def conic_sphere(n_sections: int = 200, radius: float = 1.0, potential: float = 1.0) -> Mesh:
+    """Sphere as ``n_sections`` conic sections between equally spaced polar angles (the
+    generator a chord of the meridian; the first and last sections are cones meeting the
+    axis). Its capacitance tends to 4 pi eps0 radius as the sections shrink."""
+    th = np.linspace(0.0, np.pi, n_sections + 1)
+    r, z = radius * np.sin(th), radius * np.cos(th)
+    r[0] = r[-1] = 0.0
+    m = axisymmetric(CONIC_SECTION, r[:-1], z[:-1], r[1:], z[1:], potential, name="conic-sphere")
+    m.meta = {"n_sections": n_sections, "radius": radius}
+    return m
+
+
+def conic_coax(n_z: int = 100, n_cap: int = 10, r_in: float = 0.5, r_out: float = 1.0, length: float = 4.0,
+               v_in: float = -1000.0, v_out: float = 0.0, n_rings: int = 0) -> Mesh:
+    """Axisymmetric counterpart of :func:`coax`: inner and outer cylinders of ``n_z``
+    conic sections each, annular end caps of ``n_cap`` sections at z = +-length/2, plus
+    ``n_rings`` rings (thin wires) at the inner potential spread over the gap's mid-radius."""
+    z = np.linspace(-length / 2, length / 2, n_z + 1)
+    parts = [axisymmetric(CONIC_SECTION, np.full(n_z, r_in), z[:-1], np.full(n_z, r_in), z[1:], v_in),
+             axisymmetric(CONIC_SECTION, np.full(n_z, r_out), z[:-1], np.full(n_z, r_out), z[1:], v_out)]
+    rr = np.linspace(r_in, r_out, n_cap + 1)
+    for zc in (-length / 2, length / 2):
+        parts.append(axisymmetric(CONIC_SECTION, rr[:-1], np.full(n_cap, zc), rr[1:], np.full(n_cap, zc),
+                                  np.where(0.5 * (rr[:-1] + rr[1:]) < 0.5 * (r_in + r_out), v_in, v_out)))
+    if n_rings:
+        zr = np.linspace(-length / 4, length / 4, n_rings)
+        parts.append(axisymmetric(RING, np.full(n_rings, 0.5 * (r_in + r_out)), zr, value=v_in))
+    m = parts[0]
+    for p in parts[1:]:
+        m = m.concat(p)
+    m.name = "conic-coax"
+    m.meta = {"n_z": n_z, "n_cap": n_cap, "n_rings": n_rings}
+    return m
 
 
 def triangles_from_vertices(p0, p1, p2, value, boundary=DIRICHLET) -> Mesh:

@@ -83,12 +83,33 @@ template<class Boundary> KSurfacePrimitive* make_line(const double* g, double va
     return s;
 }
 
+// axisymmetric elements: conic section g = (r0, z0, r1, z1), ring g = (r, z)
+template<class Boundary> KSurfacePrimitive* make_conic(const double* g, double value)
+{
+    auto* s = new KSurface<KElectrostaticBasis, Boundary, KConicSection>();
+    s->SetValues(g[0], g[1], g[2], g[3]);
+    set_value<Boundary>(s, value);
+    return s;
+}
+
+template<class Boundary> KSurfacePrimitive* make_ring(const double* g, double value)
+{
+    auto* s = new KSurface<KElectrostaticBasis, Boundary, KRing>();
+    s->SetValues(g[0], g[1]);
+    set_value<Boundary>(s, value);
+    return s;
+}
+
 template<class Boundary> KSurfacePrimitive* make_element(int shape, const double* g, double value)
 {
     if (shape == 0)
         return make_planar<Boundary, KTriangle>(g, value);
     if (shape == 1)
         return make_planar<Boundary, KRectangle>(g, value);
+    if (shape == 3)
+        return make_conic<Boundary>(g, value);
+    if (shape == 4)
+        return make_ring<Boundary>(g, value);
     return make_line<Boundary>(g, value);
 }
 
@@ -209,6 +230,8 @@ void kemref_element_field(void* h, int elem, int npts, const double* P, double* 
     auto* tri = dynamic_cast<KTriangle*>(s);
     auto* rect = dynamic_cast<KRectangle*>(s);
     auto* line = dynamic_cast<KLineSegment*>(s);
+    auto* conic = dynamic_cast<KConicSection*>(s);
+    auto* ring = dynamic_cast<KRing*>(s);
     for (int i = 0; i < npts; i++) {
         KPosition X(P[3 * i], P[3 * i + 1], P[3 * i + 2]);
         std::pair<KFieldVector, double> r;
@@ -216,6 +239,10 @@ void kemref_element_field(void* h, int elem, int npts, const double* P, double* 
             r = ctx->integrator.ElectricFieldAndPotential(tri, X);
         else if (rect)
             r = ctx->integrator.ElectricFieldAndPotential(rect, X);
+        else if (conic)
+            r = ctx->integrator.ElectricFieldAndPotential(conic, X);
+        else if (ring)
+            r = ctx->integrator.ElectricFieldAndPotential(ring, X);
         else
             r = ctx->integrator.ElectricFieldAndPotential(line, X);
         out[4 * i] = r.first[0];

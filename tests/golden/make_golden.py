@@ -23,6 +23,12 @@ Fixtures:
   rk8            4 electrons x 40 RK8 steps of 1e-11 s in the icosphere_L2 field
   robinhood      KRobinHood<double> (default residual-check interval, tolerances 1e-8 and
                  1e-10) on the icosphere_L2 and mixed_small meshes: sigma, iterations, residual
+  axisym         conic sections and rings (KElectrostaticAnalyticConicSectionIntegrator /
+                 ...RingIntegrator): per-element field of one conic section and one ring at
+                 points in every quadrature band of the conic section (20, 100, 500 intervals
+                 and the subdivided near branch, on and beyond the generator, on the axis); a
+                 120-section sphere and a conic coax with rings: matrix, right-hand side,
+                 direct solution, field at seeded points
 
 Usage: python tests/golden/make_golden.py [fixture ...]   (default: all)
 """
@@ -224,8 +230,61 @@ def robinhood():
     save("robinhood", **out)
 
 
+def _band_points(r0, z0, r1, z1, seed):
+    # points at distance d = f L from the generator (both sides), at fractions t along it and
+    # beyond its ends, each turned to a seeded azimuth; plus points on the axis
+    rng = np.random.default_rng(seed)
+    L = np.hypot(r1 - r0, z1 - z0)
+    u = np.array([r1 - r0, z1 - z0]) / L
+    nrm = np.array([-u[1], u[0]])
+    pts = []
+    for t in (-0.3, 0.0, 0.1, 0.5, 0.9, 1.0, 1.3):
+        for f in (0.5, 0.2, 0.1, 0.05, 0.02, 0.01, 0.003, 0.001, 0.0003, 0.0):
+            for side in ((1.0, -1.0) if f > 0 else (1.0,)):
+                rz = np.array([r0, z0]) + t * L * u + side * f * L * nrm
+                if rz[0] < 0:
+                    continue
+                phi = rng.uniform(0, 2 * np.pi)
+                pts.append([rz[0] * np.cos(phi), rz[0] * np.sin(phi), rz[1]])
+    for z in (-1.0, 0.0, 0.05, 0.7):
+        pts.append([0.0, 0.0, z])
+    return np.array(pts)
+
+
+def axisym():
+    out = {}
+    # single elements at unit charge density
+    cone = G.axisymmetric(G.CONIC_SECTION, 0.5, -0.2, 0.7, 0.3)
+    ring = G.axisymmetric(G.RING, 0.6, 0.1)
+    for name, m, pts in (("cone", cone, _band_points(0.5, -0.2, 0.7, 0.3, seed=41)),
+                         ("ring", ring, _band_points(0.45, 0.1, 0.75, 0.1, seed=43))):
+        p = ref.RefProblem(m)
+        f = p.element_field(0, pts)
+        keep = np.isfinite(f).all(axis=1)  # a point on the ring itself has no finite field
+        out[name + "_points"] = pts[keep]
+        out[name + "_field"] = f[keep]
+        out.update(mesh_arrays(m, name + "_"))
+    # whole problems
+    for name, m, pts in (("sphere", G.conic_sphere(120), G.shell_points(64, seed=47)),
+                         ("coax", G.conic_coax(n_z=40, n_cap=6, n_rings=4), G.gap_points(64, seed=53))):
+        p = ref.RefProblem(m)
+        A = p.matrix()
+        b = p.rhs()
+        x = np.linalg.solve(A, b)
+        p.set_sigma(x)
+        out[name + "_A"] = A
+        out[name + "_b"] = b
+        out[name + "_sigma"] = x
+        out[name + "_points"] = pts
+        out[name + "_field"] = p.field(pts)
+        out.update(mesh_arrays(m, name + "_"))
+    out["sphere_capacitance"] = np.array(float((out["sphere_sigma"] * G.conic_sphere(120).areas()).sum()) /
+                                         (4 * np.pi * ref.constant("eps0")))
+    save("axisym", **out)
+
+
 FIXTURES = {f.__name__: f for f in (rules, integrators, lines, icosphere, mixed_small, coax_small, rk8, adjoint,
-                                     robinhood)}
+                                     robinhood, axisym)}
 
 if __name__ == "__main__":
     for name in sys.argv[1:] or list(FIXTURES):

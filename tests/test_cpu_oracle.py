@@ -104,3 +104,25 @@ def test_port_rk8():
     st, traj = p.rk8_track(rk["state0"][0], float(rk["dt"]), 10, float(rk["charge"]), float(rk["mass"]))
     ref_ = rk["traj"][0, :10]
     assert np.max(np.abs(traj[:, 2:8] - ref_[:, 2:8]) / np.abs(ref_[:, 2:8]).max(axis=0)) < 1e-12
+
+
+def test_axisym_fixture_known_answers():
+    # a sphere of conic sections at 1 V: C = 4 pi eps0 R as the sections shrink, and the
+    # potential outside is 1/r (120 sections: within 1e-4)
+    fx = golden.load("axisym")
+    assert abs(float(fx["sphere_capacitance"]) - 1.0) < 1e-4
+    r = np.linalg.norm(fx["sphere_points"], axis=1)
+    assert np.max(np.abs(fx["sphere_field"][:, 3] * r - 1.0)) < 1e-4
+    # on the axis the field of an axisymmetric charge is axial
+    on_axis = np.hypot(fx["cone_points"][:, 0], fx["cone_points"][:, 1]) == 0.0
+    assert on_axis.sum() == 4 and np.all(fx["cone_field"][on_axis, :2] == 0.0)
+
+
+@needs_ref
+def test_reference_reproduces_axisym_fixture():
+    fx = golden.load("axisym")
+    for name in ("cone", "ring"):
+        p = ref.RefProblem(golden.mesh_from(fx, name + "_"))
+        np.testing.assert_array_equal(p.element_field(0, fx[name + "_points"]), fx[name + "_field"])
+    q = ref.RefProblem(golden.mesh_from(fx, "coax_"))
+    np.testing.assert_array_equal(q.matrix(), fx["coax_A"])
