@@ -235,6 +235,7 @@ def run_native(args, rank, world, dist):
 
     # tracking sample (configuration 3: 65,536 electrons in the 1,280-triangle sphere field)
     extra = {}
+    axisym_case = None
     if not args.quick:
         sph = G.icosphere(3)
         tctx = K.CUDAElectrostaticContext(dev)
@@ -264,6 +265,21 @@ def run_native(args, rank, world, dist):
             _, rs = tctx.SolveRobinHood(tol=1e-8, assembled=assembled)
             extra[f"robinhood_c1_{name}"] = {"seconds": rs["seconds"], "corrections": rs["subiterations"],
                                              "checks": rs["iterations"], "rel_residual_inf": rs["rel_residual"]}
+        # axisymmetric model (conic sections and rings, KElectrostaticAnalyticConicSectionIntegrator
+        # / ...RingIntegrator): coax of 2 x 2,000 cylinder sections, 2 x 200 cap sections and 16
+        # rings; assembled solve, then the FP64 field at 100,000 gap points
+        ax = G.conic_coax(n_z=2000, n_cap=200, n_rings=16)
+        tctx.SetGeometry(ax)
+        xa, sa = tctx.Solve(tol=TOL, mode=K.SOLVE_ASSEMBLED)
+        Pa = G.gap_points(100_000, seed=77)
+        tctx.ElectricFieldAndPotential(Pa[:4096])
+        tctx.ElectricFieldAndPotential(Pa)
+        ms_ax = tctx.last_kernel_ms
+        extra["axisym_conic_coax"] = {
+            "elements": ax.n, "points": len(Pa), "field_ms": ms_ax, "points_per_s": len(Pa) / (ms_ax * 1e-3),
+            "epi_per_s": len(Pa) * ax.n / (ms_ax * 1e-3), "assembled_solve_s": sa["seconds"],
+            "krylov_iterations": sa["iterations"], "rel_residual": sa["rel_residual"]}
+        axisym_case = (ax, xa, Pa)
         tctx.close()
         # configuration 5: 100,000 jittered triangles on 8 stacked rings, 8 right-hand sides:
         # one matrix-free FP64 matvec for 8 RHS, and the assembled solve (120 GB operator; the
@@ -289,7 +305,7 @@ def run_native(args, rank, world, dist):
         ms_mixed=ms_mixed, ms_fp64=ms_fp64, wall_mixed=wall_mixed, e2e_s=e2e_s, launches=int(launches),
         err_E=err_E, err_phi=err_phi, flops_per_step=flops_per_step, fp64_peak=f64.value, fp32_peak=f32.value,
         counts=counts.tolist(), st_plain=st_plain, st_asm=st_asm, sigma_diff=sigma_diff, clocks=clk.summary(),
-        extra=extra, mesh=mesh, sigma=x_asm, P=P)
+        extra=extra, mesh=mesh, sigma=x_asm, P=P, axisym=axisym_case)
     ctx.close()
     return res
 
@@ -386,6 +402,12 @@ def main():
             # the single-core figure beside it (one process, a ~5 s sample)
             rate1, sample1 = cpu_reference_rate(r["mesh"], r["sigma"], r["P"], 1, seconds_target=5.0)
             cpu["one_core"] = {"value": rate1, "sample": sample1}
+            if r["axisym"] is not None:
+                # the axisymmetric model's field on the reference CPU code, one core
+                am, ax_sigma, ax_pts = r["axisym"]
+                rate_ax, sample_ax = cpu_reference_rate(am, ax_sigma, ax_pts, 1, seconds_target=4.0)
+                cpu["axisym_conic_coax_one_core"] = {"value": rate_ax, "unit": "points/s",
+                                                     "sample": sample_ax.replace("gap points", "axisymmetric gap points")}
         else:
             cpu = {"value": None, "unit": "points/s", "cores": 0, "kind": "reference", "sample": sample}
 

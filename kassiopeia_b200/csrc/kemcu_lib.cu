@@ -842,6 +842,9 @@ int kemcu_create(kemcu_ctx** out, const kemcu_config* cfg)
     KC(cudaMemcpyToSymbol(c_qp, qp.data(), qp.size() * sizeof(double)));
     KC(cudaMemcpyToSymbol(c_qc, qc, sizeof qc));
     KC(cudaMemcpyToSymbol(c_gl, gl.data(), gl.size() * sizeof(double)));
+    double ek[kEkTerms];
+    ek_series_coefficients(ek);
+    KC(cudaMemcpyToSymbol(c_ek_coef, ek, sizeof ek));
     KC(cudaMemcpyToSymbol(c_k, &ctx->k, sizeof(Constants)));
     double rk[kStages][kStages];
     rk8_table(rk);

@@ -80,6 +80,43 @@ static double sigma_of(KSurfaceContainer& c, unsigned i)
     return dynamic_cast<KElectrostaticBasis*>(c[i]->GetBasis())->GetSolution();
 }
 
+// an axisymmetric model through the same adaptors: a sphere of 120 conic sections at 1 V solved
+// on the device, then the reference's CPU field solver and the CUDA one on its charge densities
+static int axisym_check()
+{
+    KSurfaceContainer c;
+    const int ns = 120;
+    for (int k = 0; k < ns; k++) {
+        const double t0 = M_PI * k / ns, t1 = M_PI * (k + 1) / ns;
+        auto* s = new KSurface<KElectrostaticBasis, KDirichletBoundary, KConicSection>();
+        s->SetValues(k == 0 ? 0. : std::sin(t0), std::cos(t0), k == ns - 1 ? 0. : std::sin(t1), std::cos(t1));
+        s->SetBoundaryValue(1.);
+        c.push_back(s);
+    }
+    KCUDASurfaceContainer gpu(c);
+    kemcu_solve_stats st = KCUDAChargeDensitySolver(1e-12, 300, KEMCU_SOLVE_ASSEMBLED).Solve(gpu);
+    double q = 0.;
+    for (unsigned i = 0; i < c.size(); i++)
+        q += sigma_of(c, i) * c[i]->GetShape()->Area();
+    const double cap = q / (4. * M_PI * KEMConstants::Eps0);
+    KElectrostaticBoundaryIntegrator integrator = KEBIFactory::MakeNumeric();
+    KIntegratingFieldSolver<KElectrostaticBoundaryIntegrator> cpu(c, integrator);
+    KCUDAIntegratingFieldSolver cuda(gpu);
+    gpu.WriteBasisData();
+    double worst = 0.;
+    for (int i = 0; i < 16; i++) {
+        const double r = 1.1 + 0.1 * i, th = 0.37 * i, ph = 1.1 * i;
+        KPosition P(r * std::sin(th) * std::cos(ph), r * std::sin(th) * std::sin(ph), r * std::cos(th));
+        auto a = cpu.ElectricFieldAndPotential(P);
+        auto b = cuda.ElectricFieldAndPotential(P);
+        worst = std::max(worst, std::fabs(a.second - b.second) / std::fabs(a.second));
+        worst = std::max(worst, (a.first - b.first).Magnitude() / a.first.Magnitude());
+    }
+    std::printf("axisymmetric sphere (%d conic sections): %d GMRES iterations, C / (4 pi eps0 R) = %.6f, field "
+                "CPU vs CUDA max relative difference %.3e\n", ns, st.iterations, cap, worst);
+    return !(std::fabs(cap - 1.) < 1e-4 && worst < 1e-11);
+}
+
 // KEMField's solution cache with CUDA-solved charge densities, through the reference's own
 // FindSolution / SaveSolution (KChargeDensitySolver.cc:51-280):
 //  1. nothing stored: solved on the device and stored;
@@ -235,6 +272,7 @@ int main()
         failures += !(wr / nr < 1e-6 && std::abs((int) rh.GetIteration() - rs.iterations) <= 1);
 
         failures += cache_round_trip();
+        failures += axisym_check();
     }
     catch (std::exception& e) {
         std::printf("exception: %s\n", e.what());
