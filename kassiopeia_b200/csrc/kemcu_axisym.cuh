@@ -186,6 +186,23 @@ struct RingField
     }
 };
 
+// both at once: (E_r, E_z, potential) from one ring geometry per node; each component is the
+// value the two integrands above give, so the sums are theirs
+struct RingFieldAndPotential
+{
+    static constexpr int M = 3;
+    __device__ __forceinline__ void operator()(double p, const AxPar& q, double* v) const
+    {
+        const RingGeom g = ring_at(p, q);
+        const double k = sqrt(1. - g.eta);
+        const double E = ell_E(k);
+        const double S3 = g.S * g.S * g.S;
+        v[0] = g.R / S3 * add(mul(mul(-2., g.R), ell_EK(k)), mul(g.dr / g.eta, E));
+        v[1] = g.dz / S3 * E / g.eta * g.R;
+        v[2] = g.R * ell_K(g.eta > 1. ? 0. : k) / g.S;
+    }
+};
+
 // F. Glueck's composite rule on [a, b] with n >= 20 intervals: n + 1 equidistant nodes,
 // end-corrected weights on the first and last ten and weight 1 inside, times (b - a) / n
 // (KGaussianQuadrature.cc:18-86, its n >= 20 branch, the only one the conic-section
@@ -336,6 +353,26 @@ __device__ __forceinline__ void ax_field(const double* e, double x, double y, do
     }
 }
 
+// field and potential per unit charge density in one pass over the generator
+__device__ __forceinline__ void ax_field_potential(const double* e, double x, double y, double z, double* out)
+{
+    const AxPar q = ax_par(e, x, y, z);
+    double v[3];
+    if (e[aType] == kAxRing)
+        RingFieldAndPotential()(x, q, v);
+    else
+        conic_integral(RingFieldAndPotential(), q, v);
+    const double er = e[aPre] * v[0];
+    out[2] = e[aPre] * v[1];
+    out[3] = e[aPre] * v[2];
+    if (q.r < 1.e-14)
+        out[0] = out[1] = 0.;
+    else {
+        out[0] = x / q.r * er;
+        out[1] = y / q.r * er;
+    }
+}
+
 constexpr int kAxThreads = 128;
 
 // direct sum over all elements at each point, compensated (Kahan) over the elements as
@@ -355,9 +392,11 @@ __global__ void __launch_bounds__(kAxThreads) axisym_field_kernel(const double* 
         const double* e = rec + (size_t) j * rec_stride;
         const double sg = sigma[j];
         double v[4] = {0., 0., 0., 0.};
-        if (FIELD)
+        if (FIELD && POT)
+            ax_field_potential(e, x, y, z, v);
+        else if (FIELD)
             ax_field(e, x, y, z, v);
-        if (POT)
+        else
             v[3] = ax_potential(e, x, y, z);
 #pragma unroll
         for (int m = 0; m < 4; m++) {
