@@ -131,6 +131,43 @@ __device__ __forceinline__ double ell_EK(double k)
     return ek;
 }
 
+// K(k), E(k) and (E - K) / k^2 together, each the value of the three functions above: one
+// logarithm serves both series and the k^2 > 0.8 branch of (E - K) / k^2 reuses them
+__device__ __forceinline__ void ell_KE_EK(double k, double& K, double& E, double& EK)
+{
+    const double eta = sub(1., mul(k, k));
+    const double lg = log(fabs(eta) + 1.e-19);
+    double en = eta, sa = 0., sb = 0., sc = 0., sd = 0.;
+    bool e_on = true;  // E stops at the first eta^n below 1e-20, K runs all ten terms
+#pragma unroll
+    for (int i = 0; i < 10; i++) {
+        sa += c_cody_ka[i] * en;
+        sb += c_cody_kb[i] * en;
+        if (e_on) {
+            sc += c_cody_ec[i] * en;
+            sd += c_cody_ed[i] * en;
+        }
+        en *= eta;
+        if (en < 1.e-20)
+            e_on = false;
+    }
+    K = kLn4 + sa - (0.5 + sb) * lg;
+    E = 1. + sc - sd * lg;
+    const double k2 = k * k;
+    if (k2 > 0.8) {
+        EK = (E - K) / k2;
+        return;
+    }
+    double k2n = 1., ek = 0.;
+    for (int n = 0; n < kEkTerms; n++) {
+        ek += c_ek_coef[n] * k2n;
+        k2n *= k2;
+        if (k2n < 1.e-16)
+            break;
+    }
+    EK = ek;
+}
+
 // evaluation point (z, r) and generator (za, ra) -> (zb, rb) of length len; the ring sits at
 // distance p along the generator (KElectrostaticAnalyticRingIntegrator.cc:70-94)
 struct AxPar
@@ -194,12 +231,13 @@ struct RingFieldAndPotential
     __device__ __forceinline__ void operator()(double p, const AxPar& q, double* v) const
     {
         const RingGeom g = ring_at(p, q);
-        const double k = sqrt(1. - g.eta);
-        const double E = ell_E(k);
+        const double k = g.eta > 1. ? 0. : sqrt(1. - g.eta);  // eta <= 1 for r, R >= 0
+        double K, E, EK;
+        ell_KE_EK(k, K, E, EK);
         const double S3 = g.S * g.S * g.S;
-        v[0] = g.R / S3 * add(mul(mul(-2., g.R), ell_EK(k)), mul(g.dr / g.eta, E));
+        v[0] = g.R / S3 * add(mul(mul(-2., g.R), EK), mul(g.dr / g.eta, E));
         v[1] = g.dz / S3 * E / g.eta * g.R;
-        v[2] = g.R * ell_K(g.eta > 1. ? 0. : k) / g.S;
+        v[2] = g.R * K / g.S;
     }
 };
 
