@@ -344,6 +344,21 @@ def profile_tracker():
                           "track_steps_per_s": ts["steps"] / ts["seconds"]}), flush=True)
 
 
+def profile_axisym():
+    import kassiopeia_b200 as K
+    from kassiopeia_b200 import geometry as G
+
+    ctx = K.CUDAElectrostaticContext(int(os.environ.get("LOCAL_RANK", 0)))
+    ax = G.conic_coax(n_z=2000, n_cap=200, n_rings=16)
+    ctx.SetGeometry(ax)
+    ctx.Solve(tol=TOL, mode=K.SOLVE_ASSEMBLED)
+    P = G.gap_points(10_000, seed=77)
+    for _ in range(2):  # the first launch warms up, the second is the one to capture
+        ctx.ElectricFieldAndPotential(P)
+        print(json.dumps({"axisym_field": "FP64", "elements": ax.n, "points": len(P), "ms": ctx.last_kernel_ms,
+                          "points_per_s": len(P) / (ctx.last_kernel_ms * 1e-3)}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -357,11 +372,18 @@ def main():
     ap.add_argument("--points", type=int, default=N_POINTS, help="gap points per GPU (default 1,000,000)")
     ap.add_argument("--profile-operator", action="store_true",
                     help="profiling case for ncu: assembled operator of a 16,320-element coax (2.1 GB FP64 + "
-                         "1.1 GB FP32), three FP32 and two FP64 dense matvecs; prints one JSON line per matvec")
+                         "1.1 GB FP32), three FP32 and two FP64 dense matvecs with one right-hand side, then two "
+                         "FP32 and two FP64 with eight; prints one JSON line per matvec")
     ap.add_argument("--profile-tracker", action="store_true",
                     help="profiling case for ncu: 65,536 electrons in the field of the 1,280-triangle sphere, "
                          "one persistent RK8 launch of 8 steps per track, FP64 then MIXED; prints track steps/s")
+    ap.add_argument("--profile-axisym", action="store_true",
+                    help="profiling case for ncu: axisymmetric coax (4,416 conic sections and rings), field and "
+                         "potential at 10,000 gap points, two launches; prints points/s")
     args = ap.parse_args()
+    if args.profile_axisym:
+        profile_axisym()
+        return
     if args.profile_operator:
         profile_operator()
         return

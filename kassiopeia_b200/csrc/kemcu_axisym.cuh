@@ -413,20 +413,24 @@ __device__ __forceinline__ void ax_field_potential(const double* e, double x, do
 
 constexpr int kAxThreads = 128;
 
-// direct sum over all elements at each point, compensated (Kahan) over the elements as
-// KIntegratingFieldSolver does (KElectrostaticIntegratingFieldSolver.hh:261-339); out n x 4
+// direct sum over the elements [e0, e1) of split blockIdx.y at each point, compensated (Kahan)
+// over the elements as KIntegratingFieldSolver does (KElectrostaticIntegratingFieldSolver.hh:
+// 261-339); out n x 4, or partial[split][n][4] summed by reduce_splits in split order
 template<bool POT, bool FIELD>
 __global__ void __launch_bounds__(kAxThreads) axisym_field_kernel(const double* __restrict__ rec, int rec_stride,
                                                                    const double* __restrict__ sigma, int ne,
                                                                    const double* __restrict__ P, int np,
-                                                                   double* __restrict__ out)
+                                                                   double* __restrict__ out,
+                                                                   double* __restrict__ partial)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np)
         return;
+    const int per = (ne + gridDim.y - 1) / gridDim.y;
+    const int e0 = blockIdx.y * per, e1 = min(ne, e0 + per);
     const double x = P[3 * i], y = P[3 * i + 1], z = P[3 * i + 2];
     double s[4] = {0., 0., 0., 0.}, c[4] = {0., 0., 0., 0.};
-    for (int j = 0; j < ne; j++) {
+    for (int j = e0; j < e1; j++) {
         const double* e = rec + (size_t) j * rec_stride;
         const double sg = sigma[j];
         double v[4] = {0., 0., 0., 0.};
@@ -444,49 +448,56 @@ __global__ void __launch_bounds__(kAxThreads) axisym_field_kernel(const double* 
             s[m] = t;
         }
     }
+    double* dst = partial ? partial + (size_t) blockIdx.y * np * 4 : out;
 #pragma unroll
     for (int m = 0; m < 4; m++)
-        out[4 * (size_t) i + m] = s[m];
+        dst[4 * (size_t) i + m] = s[m];
 }
 
 // y[r][i] = sum_j A_ij x[r][j], A_ij = potential of element j at the centroid of element i
-// (Dirichlet rows, KBoundaryIntegralMatrix.hh:31-55); one thread per row
+// (Dirichlet rows, KBoundaryIntegralMatrix.hh:31-55); one thread per row, the columns split
+// over gridDim.y (partial[split][nrhs][n] when split > 1)
 template<int NR>
 __global__ void __launch_bounds__(kAxThreads) axisym_matvec_kernel(const double* __restrict__ rec, int rec_stride, int n,
                                                                     const double* __restrict__ x, int nrhs,
-                                                                    double* __restrict__ y)
+                                                                    double* __restrict__ y, double* __restrict__ partial)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
+    const int per = (n + gridDim.y - 1) / gridDim.y;
+    const int j0 = blockIdx.y * per, j1 = min(n, j0 + per);
     const double* t = rec + (size_t) i * rec_stride;
     const double cx = t[aCx], cy = t[aCy], cz = t[aCz];
     double acc[NR];
 #pragma unroll
     for (int r = 0; r < NR; r++)
         acc[r] = 0.;
-    for (int j = 0; j < n; j++) {
+    for (int j = j0; j < j1; j++) {
         const double a = ax_potential(rec + (size_t) j * rec_stride, cx, cy, cz);
 #pragma unroll
         for (int r = 0; r < NR; r++)
             if (r < nrhs)
                 acc[r] += a * x[(size_t) r * n + j];
     }
+    double* dst = partial ? partial + (size_t) blockIdx.y * nrhs * n : y;
 #pragma unroll
     for (int r = 0; r < NR; r++)
         if (r < nrhs)
-            y[(size_t) r * n + i] = acc[r];
+            dst[(size_t) r * n + i] = acc[r];
 }
 
 // the operator column-major with leading dimension ld, FP64 and (when a32) FP32; one thread
-// per row, columns [j0, j1)
+// per row, the columns [0, n) split over gridDim.y
 __global__ void __launch_bounds__(kAxThreads) axisym_assemble_kernel(const double* __restrict__ rec, int rec_stride,
-                                                                      int n, int j0, int j1, size_t ld,
-                                                                      double* __restrict__ a64, float* __restrict__ a32)
+                                                                      int n, size_t ld, double* __restrict__ a64,
+                                                                      float* __restrict__ a32)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
+    const int per = (n + gridDim.y - 1) / gridDim.y;
+    const int j0 = blockIdx.y * per, j1 = min(n, j0 + per);
     const double* t = rec + (size_t) i * rec_stride;
     const double cx = t[aCx], cy = t[aCy], cz = t[aCz];
     for (int j = j0; j < j1; j++) {
@@ -495,6 +506,17 @@ __global__ void __launch_bounds__(kAxThreads) axisym_assemble_kernel(const doubl
         if (a32)
             a32[(size_t) j * ld + i] = (float) a;
     }
+}
+
+// blocks along the element (or column) range: about four waves of resident CTAs in all, each
+// block keeping at least 8 elements
+inline int axisym_split(int num_sms, size_t rows, size_t cols)
+{
+    const size_t blocks = (rows + kAxThreads - 1) / kAxThreads;
+    const size_t want = (size_t) num_sms * 5 * 4;
+    size_t split = blocks >= want ? 1 : (want + blocks - 1) / blocks;
+    split = std::min(split, std::max((size_t) 1, cols / 8));
+    return (int) std::min(split, (size_t) 65535);
 }
 
 // one matrix entry

@@ -294,21 +294,43 @@ int grid_split(const kemcu_ctx* ctx, size_t n_pts, size_t n_elem)
     return (int) std::max((size_t) 1, split);
 }
 
-// axisymmetric elements: FP64 element integrals whatever the precision argument
-int launch_axisym_field(kemcu_ctx* ctx, const double* d_pts, size_t n, double* d_out, int what)
+// axisymmetric elements: FP64 element integrals whatever the precision argument. The element
+// range is split over gridDim.y (axisym_split), partial sums in `scratch` (n x 4 x split
+// doubles, capped at `scratch_cap` doubles; null: grow-only scratch of the context)
+int launch_axisym_field(kemcu_ctx* ctx, const double* d_pts, size_t n, double* d_out, int what,
+                        double* scratch = nullptr, size_t scratch_cap = 0)
 {
-    const unsigned grid = (unsigned) ((n + kAxThreads - 1) / kAxThreads);
     const int ne = (int) ctx->n, np = (int) n;
+    int split = axisym_split(ctx->num_sms, n, ctx->n);
+    double* partial = nullptr;
+    if (scratch)
+        split = (int) std::min((size_t) split, std::max((size_t) 1, scratch_cap / (4 * n)));
+    if (split > 1) {
+        if (scratch)
+            partial = scratch;
+        else {
+            void* p;
+            if (int rc = ensure(ctx, sPartial, (size_t) split * n * 4 * sizeof(double), &p))
+                return rc;
+            partial = (double*) p;
+        }
+    }
+    const dim3 grid((unsigned) ((n + kAxThreads - 1) / kAxThreads), (unsigned) split);
     if (what == KEMCU_POTENTIAL)
         axisym_field_kernel<true, false><<<grid, kAxThreads, 0, ctx->stream>>>(ctx->d_rec, rRecSize, ctx->d_sigma, ne,
-                                                                               d_pts, np, d_out);
+                                                                               d_pts, np, d_out, partial);
     else if (what == KEMCU_FIELD)
         axisym_field_kernel<false, true><<<grid, kAxThreads, 0, ctx->stream>>>(ctx->d_rec, rRecSize, ctx->d_sigma, ne,
-                                                                               d_pts, np, d_out);
+                                                                               d_pts, np, d_out, partial);
     else
         axisym_field_kernel<true, true><<<grid, kAxThreads, 0, ctx->stream>>>(ctx->d_rec, rRecSize, ctx->d_sigma, ne,
-                                                                              d_pts, np, d_out);
+                                                                              d_pts, np, d_out, partial);
     KCHECK_LAUNCH();
+    if (split > 1) {
+        const size_t m = n * 4;
+        reduce_splits<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(partial, split, m, d_out);
+        KCHECK_LAUNCH();
+    }
     return KEMCU_OK;
 }
 
@@ -433,12 +455,27 @@ int apply_op(kemcu_ctx* ctx, int op, const double* d_x, double* d_y, int nrhs)
 {
     const int n = (int) ctx->n;
     if ((op == kFree64 || op == kFreeMixed) && ctx->axisym) {
-        const unsigned grid = (unsigned) ((n + kAxThreads - 1) / kAxThreads);
+        const int split = axisym_split(ctx->num_sms, n, n);
+        double* partial = nullptr;
+        if (split > 1) {
+            void* p;
+            if (int rc = ensure(ctx, sPartial, (size_t) split * nrhs * n * sizeof(double), &p))
+                return rc;
+            partial = (double*) p;
+        }
+        const dim3 grid((unsigned) ((n + kAxThreads - 1) / kAxThreads), (unsigned) split);
         if (nrhs == 1)
-            axisym_matvec_kernel<1><<<grid, kAxThreads, 0, ctx->stream>>>(ctx->d_rec, rRecSize, n, d_x, nrhs, d_y);
+            axisym_matvec_kernel<1><<<grid, kAxThreads, 0, ctx->stream>>>(ctx->d_rec, rRecSize, n, d_x, nrhs, d_y,
+                                                                          partial);
         else
-            axisym_matvec_kernel<kMaxRhs><<<grid, kAxThreads, 0, ctx->stream>>>(ctx->d_rec, rRecSize, n, d_x, nrhs, d_y);
+            axisym_matvec_kernel<kMaxRhs><<<grid, kAxThreads, 0, ctx->stream>>>(ctx->d_rec, rRecSize, n, d_x, nrhs,
+                                                                                d_y, partial);
         KCHECK_LAUNCH();
+        if (split > 1) {
+            const size_t m = (size_t) nrhs * n;
+            reduce_splits<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(partial, split, m, d_y);
+            KCHECK_LAUNCH();
+        }
         return KEMCU_OK;
     }
     if (op == kFree64 || op == kFreeMixed) {
@@ -548,8 +585,9 @@ int assemble(kemcu_ctx* ctx, bool want32)
         return fail(ctx, KEMCU_ENOMEM, "allocation of the FP32 operator copy failed");
     }
     if (ctx->axisym) {
-        axisym_assemble_kernel<<<(unsigned) ((n + kAxThreads - 1) / kAxThreads), kAxThreads, 0, ctx->stream>>>(
-            ctx->d_rec, rRecSize, (int) n, 0, (int) n, ld, ctx->d_a64, fill32 ? ctx->d_a32 : nullptr);
+        const dim3 grid((unsigned) ((n + kAxThreads - 1) / kAxThreads), (unsigned) axisym_split(ctx->num_sms, n, n));
+        axisym_assemble_kernel<<<grid, kAxThreads, 0, ctx->stream>>>(ctx->d_rec, rRecSize, (int) n, ld, ctx->d_a64,
+                                                                     fill32 ? ctx->d_a32 : nullptr);
         KCHECK_LAUNCH();
         return KEMCU_OK;
     }
@@ -1066,7 +1104,8 @@ int kemcu_field_dev_noalloc(kemcu_ctx* ctx, const double* dP, size_t n, double* 
     KC(cudaSetDevice(ctx->device));
     Timer t(ctx);
     if (ctx->axisym) {
-        if ((rc = launch_axisym_field(ctx, dP, n, dout4, what)))
+        if ((rc = launch_axisym_field(ctx, dP, n, dout4, what, ctx->noalloc_scratch,
+                                      KEMCU_NOALLOC_SCRATCH_BYTES / sizeof(double))))
             return rc;
         t.stop();
         return KEMCU_OK;
