@@ -141,7 +141,7 @@ int ensure(kemcu_ctx* ctx, int slot, size_t bytes, void** out)
 // ring geom = (r, z) (KConicSection.hh: P0 = (r0, 0, z0), P1 = (r1, 0, z1); KRing.hh: P = (r, 0, z)).
 // Prefactors and the centroid as KElectrostaticAnalyticConicSectionIntegrator.cc:91,
 // KElectrostaticAnalyticRingIntegrator.cc:36 and KConicSection.hh:29-32 / KRing.hh:29-32 form them.
-static_assert(aRecUsed <= rRecSize, "the axisymmetric record must fit the element record slot");
+static_assert((int) aRecUsed <= (int) rRecSize, "the axisymmetric record must fit the element record slot");
 
 void build_axisym_record(const double* g, int shape, double value, const Constants& K, double* r, double& rhs)
 {
