@@ -22,8 +22,9 @@
  *               conic section: r0, z0, r1, z1, 0... (KConicSection.hh: P0 = (r0, 0, z0),
  *               P1 = (r1, 0, z1)); ring: r, z, 0... (KRing.hh: P = (r, 0, z)). Their integrals
  *               are KElectrostaticAnalyticConicSectionIntegrator / ...RingIntegrator, FP64
- *               whatever the precision argument; tracking, the adjoint, Robin Hood and the
- *               band histogram take planar elements only (KEMCU_EINVAL otherwise).
+ *               whatever the precision argument; tracking, the adjoint, matrix-free Robin
+ *               Hood and the band histogram take planar elements only (KEMCU_EINVAL
+ *               otherwise; Robin Hood on the assembled operator takes both).
  * Units are SI; 1/(4 pi eps0) and eps0 come from kemcu_config (KEMConstants, KEMConstants.cc:11-12).
  */
 #ifndef KEMCU_H

@@ -519,6 +519,16 @@ inline int axisym_split(int num_sms, size_t rows, size_t cols)
     return (int) std::min(split, (size_t) 65535);
 }
 
+// the diagonal A(i, i) (Robin Hood on the assembled operator)
+__global__ void axisym_diag_kernel(const double* __restrict__ rec, int rec_stride, int n, double* __restrict__ diag)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const double* t = rec + (size_t) i * rec_stride;
+    diag[i] = ax_potential(t, t[aCx], t[aCy], t[aCz]);
+}
+
 // one matrix entry
 __global__ void axisym_entry_kernel(const double* __restrict__ rec, int rec_stride, int i, int j, double* __restrict__ a)
 {

@@ -99,5 +99,14 @@ def test_axisymmetric_limits(ctx):
     st = G.electrons(4, seed=3)
     with pytest.raises(K.KemcuError):
         ctx.TrackRK8(st, 1e-11, 4)
-    with pytest.raises(K.KemcuError):
+    with pytest.raises(K.KemcuError):  # matrix-free Robin Hood columns are planar-only
         ctx.SolveRobinHood()
+
+
+def test_robin_hood_on_the_assembled_axisymmetric_operator(ctx):
+    fx = golden.load("axisym")
+    ctx.SetGeometry(golden.mesh_from(fx, "sphere_"))
+    x, st = ctx.SolveRobinHood(tol=1e-10, assembled=True)
+    assert st["rel_residual"] <= 1e-10 and st["subiterations"] > 0
+    ref = fx["sphere_sigma"]
+    assert np.max(np.abs(x - ref)) / np.max(np.abs(ref)) < 1e-7
