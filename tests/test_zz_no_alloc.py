@@ -55,3 +55,35 @@ def test_noalloc_matches_allocating_entry_point_twice():
     assert "at most" in L.kemcu_last_error(ctx._h).decode()
     assert L_max == limit
     ctx.close()
+
+
+def test_noalloc_axisymmetric_elements():
+    # conic sections and rings take the same no-allocation entry point (element range split
+    # over the grid, partial sums in the fixed scratch)
+    import torch
+
+    import kassiopeia_b200 as K
+    from kassiopeia_b200 import _native as N
+    from kassiopeia_b200 import geometry as G
+
+    L = N.lib()
+    ctx = K.CUDAElectrostaticContext(0)
+    mesh = G.conic_coax(n_z=40, n_cap=6, n_rings=4)
+    ctx.SetGeometry(mesh)
+    ctx.Solve(tol=1e-10, mode=K.SOLVE_ASSEMBLED)
+    n_pts = 3000
+    P = torch.from_numpy(G.gap_points(n_pts, seed=11)).cuda()
+    ref = torch.zeros((n_pts, 4), dtype=torch.float64, device="cuda")
+    out = torch.full((n_pts, 4), float("nan"), dtype=torch.float64, device="cuda")
+    assert L.kemcu_field_dev(ctx._h, C.c_void_p(P.data_ptr()), n_pts, C.c_void_p(ref.data_ptr()), K.FP64,
+                             K.FIELD_AND_POTENTIAL) == 0
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    rc = L.kemcu_field_dev_noalloc(ctx._h, C.c_void_p(P.data_ptr()), n_pts, C.c_void_p(out.data_ptr()), K.FP64,
+                                   K.FIELD_AND_POTENTIAL)
+    assert rc == 0, L.kemcu_last_error(ctx._h).decode()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
+    r, o = ref.cpu().numpy(), out.cpu().numpy()
+    assert np.max(np.abs(o - r) / np.abs(r).max(axis=0)) < 1e-12
+    ctx.close()
