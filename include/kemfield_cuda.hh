@@ -324,6 +324,18 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
     {
         fMode = mode;
     }
+    // XML form: "plain", "mixed" or "assembled" (kemcu_solve_mode)
+    void SetModeName(const std::string& name)
+    {
+        if (name == "plain")
+            fMode = KEMCU_SOLVE_PLAIN;
+        else if (name == "mixed")
+            fMode = KEMCU_SOLVE_MIXED;
+        else if (name == "assembled")
+            fMode = KEMCU_SOLVE_ASSEMBLED;
+        else
+            throw KEMSimpleException("kemcu: unknown solve mode <" + name + "> (plain, mixed, assembled)");
+    }
     // solves A sigma = b for the boundary values and writes sigma into the container
     kemcu_solve_stats Solve(KCUDASurfaceContainer& container) const
     {
