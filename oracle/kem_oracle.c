@@ -286,6 +286,259 @@ static void line_analytic(const double* g, v3 P, double* o)
     o[2] = s * (p1.z * Da - P.z * (Da + Db) + p0.z * Db);
 }
 
+/* ------------------------------------------------------------------ axisymmetric elements
+ * conic section geom = (r0, z0, r1, z1), ring geom = (r, z): KConicSection.hh, KRing.hh */
+
+/* complete elliptic integrals in W. J. Cody's form (Math. Comp. 19 (1965) 105) with his
+   coefficient sets, as Math/src/KEllipticIntegrals.cc:17-103 (its build without GSL) */
+#define KEMO_PI 3.14159265358979323846 /* KEMConstants::Pi, KConst::Pi() */
+static const double CODY_KA[10] = {9.657359028085625e-2, 3.088514627130518e-2, 1.493801353268716e-2,
+                                   8.789801874555064e-3, 6.179627446053317e-3, 6.847909282624505e-3,
+                                   9.848929322176893e-3, 8.003003980649985e-3, 2.296634898396958e-3,
+                                   1.393087857006646e-4};
+static const double CODY_KB[10] = {1.249999999999080e-1, 7.031249973903835e-2, 4.882804190686239e-2,
+                                   3.737773975862360e-2, 3.012484901289893e-2, 2.393191332311079e-2,
+                                   1.553094163197720e-2, 5.973904299155429e-3, 9.215546349632498e-4,
+                                   2.970028096655561e-5};
+static const double CODY_EC[10] = {4.431471805608895e-1, 5.680519456755915e-2, 2.183181167613048e-2,
+                                   1.156959574529540e-2, 7.595093422559432e-3, 7.820404060959554e-3,
+                                   1.077063503986645e-2, 8.638442173604074e-3, 2.468503330460722e-3,
+                                   1.494662175718132e-4};
+static const double CODY_ED[10] = {2.499999999999017e-1, 9.374999972120314e-2, 5.859366125553149e-2,
+                                   4.271789054738309e-2, 3.347894366576162e-2, 2.614501470031387e-2,
+                                   1.680402334636338e-2, 6.432146586438301e-3, 9.898332846225384e-4,
+                                   3.185919565550157e-5};
+
+static double ell_K(double k)
+{
+    const double eta = 1. - k * k;
+    double en = eta, sa = 0., sb = 0.;
+    for (int i = 0; i < 10; i++) {
+        sa += CODY_KA[i] * en;
+        sb += CODY_KB[i] * en;
+        en *= eta;
+    }
+    return 1.386294361119890 + sa - (1. / 2. + sb) * log(fabs(eta) + 1.e-19);
+}
+
+static double ell_E(double k)
+{
+    const double eta = 1. - k * k;
+    double en = eta, sc = 0., sd = 0.;
+    for (int i = 0; i < 10; i++) {
+        sc += CODY_EC[i] * en;
+        sd += CODY_ED[i] * en;
+        en *= eta;
+        if (en < 1.e-20)
+            break;
+    }
+    return 1. + sc - sd * log(fabs(eta) + 1.e-19);
+}
+
+/* (E - K) / k^2: difference for k^2 > 0.8, power series below (KEllipticIntegrals.cc:108-131) */
+static double ell_EK(double k)
+{
+    const double k2 = k * k;
+    if (k2 > 0.8)
+        return (ell_E(k) - ell_K(k)) / k2;
+    double a = KEMO_PI / 2., k2n = 1., ek = 0.;
+    for (int n = 1; n <= 900; n++) {
+        const double cn = (2. * n - 1) / (2. * n);
+        a *= cn * cn;
+        const double b = -a / (2. * n - 1.);
+        ek += (b - a) * k2n;
+        k2n *= k2;
+        if (k2n < 1.e-16)
+            break;
+    }
+    return ek;
+}
+
+/* ring at distance p along the generator par = (z, r, zA, rA, zB, rB, L): potential R K / S and
+   field components R / S^3 (-2 R EK + dr E / eta), dz / S^3 E / eta R
+   (BoundaryIntegrals/Electrostatic/Analytic/src/KElectrostaticAnalyticRingIntegrator.cc:95-208) */
+static double ring_potential(double p, const double* par)
+{
+    const double Z = par[2] + p / par[6] * (par[4] - par[2]);
+    const double R = par[3] + p / par[6] * (par[5] - par[3]);
+    const double dz = par[0] - Z, dr = par[1] - R, sumr = R + par[1];
+    const double eta = (dr * dr + dz * dz) / (sumr * sumr + dz * dz);
+    const double k = (eta > 1. ? 0. : sqrt(1. - eta));
+    const double K = ell_K(k);
+    const double S = sqrt(sumr * sumr + dz * dz);
+    return R * K / S;
+}
+
+static double ring_er(double p, const double* par)
+{
+    const double Z = par[2] + p / par[6] * (par[4] - par[2]);
+    const double R = par[3] + p / par[6] * (par[5] - par[3]);
+    const double dz = par[0] - Z, dr = par[1] - R, sumr = R + par[1];
+    const double eta = (dr * dr + dz * dz) / (sumr * sumr + dz * dz);
+    const double k = sqrt(1. - eta);
+    const double E = ell_E(k);
+    const double S = sqrt(sumr * sumr + dz * dz);
+    const double EK = ell_EK(k);
+    return R / (S * S * S) * (-2. * R * EK + dr / eta * E);
+}
+
+static double ring_ez(double p, const double* par)
+{
+    const double Z = par[2] + p / par[6] * (par[4] - par[2]);
+    const double R = par[3] + p / par[6] * (par[5] - par[3]);
+    const double dz = par[0] - Z, dr = par[1] - R, sumr = R + par[1];
+    const double eta = (dr * dr + dz * dz) / (sumr * sumr + dz * dz);
+    const double k = sqrt(1. - eta);
+    const double E = ell_E(k);
+    const double S = sqrt(sumr * sumr + dz * dz);
+    return dz / (S * S * S) * E / eta * R;
+}
+
+/* F. Glueck's composite rule, its n >= 20 branch (Math/src/KGaussianQuadrature.cc:18-86): m = 1
+   integrates the ring potential, m = 2 the two field components */
+static void glueck(int m, double a, double b, const double* par, int n, double* ans)
+{
+    static const double w9[10] = {0.2803440531305107e0,  0.1648702325837748e1, -0.2027449845679092e0,
+                                  0.2797927414021179e1,  -0.9761199294532843e0, 0.2556499393738999e1,
+                                  0.1451083002645404e0,  0.1311227127425048e1,  0.9324249063051143e0,
+                                  0.1006631393298060e1};
+    const double deln = (b - a) / n;
+    double x;
+    for (int j = 0; j < m; j++)
+        ans[j] = 0;
+#define KEMO_F(j, x) ((m == 1) ? ring_potential((x), par) : ((j) == 0 ? ring_er((x), par) : ring_ez((x), par)))
+    for (int i = 0; i < 10; i++) {
+        x = a + deln * i;
+        for (int j = 0; j < m; j++)
+            ans[j] += w9[i] * KEMO_F(j, x);
+    }
+    for (int i = 10; i < n - 9; i++) {
+        x = a + deln * i;
+        for (int j = 0; j < m; j++)
+            ans[j] += KEMO_F(j, x);
+    }
+    for (int i = n - 9; i <= n; i++) {
+        x = a + deln * i;
+        for (int j = 0; j < m; j++)
+            ans[j] += w9[n - i] * KEMO_F(j, x);
+    }
+#undef KEMO_F
+    for (int j = 0; j < m; j++)
+        ans[j] *= deln;
+}
+
+/* the conic-section integral of m ring integrands: 20 / 100 / 500 intervals by the distance
+   excess D, else the generator cut at the foot point and each side integrated in pieces
+   shrinking by 0.3, plus the logarithmic remainder (added to every component, as the
+   reference does) (Analytic/src/KElectrostaticAnalyticConicSectionIntegrator.cc:33-93, 113-198) */
+static void conic_integral(int m, const double* par, double* q)
+{
+    const double ln4 = 1.386294361119890;
+    const double z = par[0], r = par[1], za = par[2], ra = par[3], zb = par[4], rb = par[5], L = par[6];
+    const double Da = sqrt((za - z) * (za - z) + (ra - r) * (ra - r));
+    const double Db = sqrt((zb - z) * (zb - z) + (rb - r) * (rb - r));
+    const double D = fabs(Da + Db - L) / L;
+    if (D >= 5.e-2) {
+        glueck(m, 0., L, par, 20, q);
+        return;
+    }
+    if (D >= 5.e-3 && D < 5.e-2) {
+        glueck(m, 0., L, par, 100, q);
+        return;
+    }
+    if (D >= 5.e-4 && D < 5.e-3) {
+        glueck(m, 0., L, par, 500, q);
+        return;
+    }
+    const double u0 = (zb - za) / L, u1 = (rb - ra) / L;
+    const double pp = (z - za) * u0 + (r - ra) * u1;
+    double tmp[2], a, b, h;
+    for (int j = 0; j < m; j++)
+        q[j] = 0.;
+    if (pp < L) {
+        const double pmax = L;
+        double pmin = pp;
+        if (pp < 0.)
+            pmin = 0.;
+        b = pmax;
+        a = pmin + (b - pmin) * 0.3;
+        for (int n = 1; n <= 35; n++) {
+            glueck(m, a, b, par, 50, tmp);
+            for (int j = 0; j < m; j++)
+                q[j] += tmp[j];
+            if (fabs(a - pmin) / L < 1.e-8)
+                break;
+            b = a;
+            a = pmin + (b - pmin) * 0.3;
+        }
+        h = fabs(a - pmin);
+        for (int j = 0; j < m; j++)
+            q[j] += h * (ln4 + log(2. * par[1] + 1.e-12) + 1. - log(h)) / 2.;
+    }
+    if (pp > 0.) {
+        double pmax = pp;
+        const double pmin = 0.;
+        if (pp > L)
+            pmax = L;
+        b = pmin;
+        a = pmax - (pmax - b) * 0.3;
+        for (int n = 1; n <= 35; n++) {
+            glueck(m, b, a, par, 50, tmp);
+            for (int j = 0; j < m; j++)
+                q[j] += tmp[j];
+            if (fabs(pmax - a) / L < 1.e-8)
+                break;
+            b = a;
+            a = pmax - (pmax - b) * 0.3;
+        }
+        h = fabs(pmax - a);
+        for (int j = 0; j < m; j++)
+            q[j] += h * (ln4 + log(2. * par[1] + 1.e-12) + 1. - log(h)) / 2.;
+    }
+}
+
+/* field and potential per unit charge density of a conic section (shape 3) or ring (shape 4);
+   E_r turned into (E_x, E_y), zero within 1e-14 of the axis
+   (KElectrostaticAnalyticConicSectionIntegrator.cc:9-221, KElectrostaticAnalyticRingIntegrator.cc:26-68) */
+static void axisym_element(int shape, const double* g, v3 P, double* o)
+{
+    double par[7];
+    par[0] = P.z;
+    par[1] = sqrt(P.x * P.x + P.y * P.y);
+    double c, er, ez, pot;
+    if (shape == 4) {
+        par[2] = par[4] = g[1];
+        par[3] = par[5] = g[0];
+        par[6] = 1.;
+        c = 1. / (par[3] * 2. * KEMO_PI * KEMO_PI * EPS0);
+        pot = c * ring_potential(P.x, par);
+        ez = c * ring_ez(P.x, par);
+        er = c * ring_er(P.x, par);
+    }
+    else {
+        par[2] = g[1];
+        par[3] = g[0];
+        par[4] = g[3];
+        par[5] = g[2];
+        par[6] = sqrt((g[0] - g[2]) * (g[0] - g[2]) + 0. * 0. + (g[1] - g[3]) * (g[1] - g[3]));
+        double q1[1], q2[2];
+        conic_integral(1, par, q1);
+        conic_integral(2, par, q2);
+        c = 1. / (KEMO_PI * EPS0);
+        pot = c * q1[0];
+        er = c * q2[0];
+        ez = c * q2[1];
+    }
+    o[2] = ez;
+    o[3] = pot;
+    if (par[1] < 1.e-14)
+        o[0] = o[1] = 0.;
+    else {
+        o[0] = P.x / par[1] * er;
+        o[1] = P.y / par[1] * er;
+    }
+}
+
 /* ------------------------------------------------------------------ dispatch
  * distance ratio |P - centroid| / size and the rule bands
  * (…CubatureTriangleIntegrator.cc:453-522, .hh:51-53; …CubatureRectangleIntegrator.cc:462-520,
@@ -293,6 +546,10 @@ static void line_analytic(const double* g, v3 P, double* o)
 void kemo_element(int shape, const double* g, const double* Pp, double* o)
 {
     const v3 P = ld(Pp);
+    if (shape == 3 || shape == 4) {
+        axisym_element(shape, g, P, o);
+        return;
+    }
     if (shape == 2) {
         const double L = sqrt((g[3] - g[0]) * (g[3] - g[0]) + (g[4] - g[1]) * (g[4] - g[1]) +
                               (g[5] - g[2]) * (g[5] - g[2]));
@@ -362,6 +619,13 @@ void kemo_field(size_t n, const int* shape, const double* geom, const double* si
 /* target centroid and normal of element i (KTriangle/KRectangle/KLineSegment Centroid(), Normal()) */
 static void target(int shape, const double* g, double* c, double* nv)
 {
+    if (shape == 3 || shape == 4) {  /* (P0 + P1) / 2 (KConicSection.hh:29-32), P (KRing.hh:29-32) */
+        c[0] = shape == 3 ? (g[0] + g[2]) * .5 : g[0];
+        c[1] = 0.;
+        c[2] = shape == 3 ? (g[1] + g[3]) * .5 : g[1];
+        nv[0] = nv[1] = nv[2] = 0.;
+        return;
+    }
     if (shape == 2) {
         for (int k = 0; k < 3; k++)
             c[k] = (g[k] + g[3 + k]) * .5;

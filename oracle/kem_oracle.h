@@ -13,7 +13,8 @@ void kemo_set_rules(const double* tri7, const double* tri12, const double* tri33
                     const double* rect12, const double* rect33, const double* gl4, const double* gl16);
 void kemo_set_constants(double one_over_four_pi_eps0, double eps0);
 
-/* normalised (sigma = 1) field and potential of one element at P: out[4] = Ex, Ey, Ez, phi */
+/* normalised (sigma = 1) field and potential of one element at P: out[4] = Ex, Ey, Ez, phi
+   (shapes 0-2 planar; 3 conic section, 4 ring: the analytic axisymmetric integrators) */
 void kemo_element(int shape, const double* geom11, const double* P, double* out4);
 /* Kahan-summed direct sum over n elements at m points (out: m x 4) */
 void kemo_field(size_t n, const int* shape, const double* geom, const double* sigma, size_t m, const double* P,

@@ -126,3 +126,22 @@ def test_reference_reproduces_axisym_fixture():
         np.testing.assert_array_equal(p.element_field(0, fx[name + "_points"]), fx[name + "_field"])
     q = ref.RefProblem(golden.mesh_from(fx, "coax_"))
     np.testing.assert_array_equal(q.matrix(), fx["coax_A"])
+
+
+def test_port_axisymmetric_elements_bit_exact():
+    # the C restatement of the conic-section and ring integrators reproduces the reference's
+    # values exactly: single elements in every band, the matrices and the fields of the
+    # sphere and the coax with rings
+    from oracle import port
+
+    fx = golden.load("axisym")
+    for name in ("cone", "ring"):
+        p = port.PortProblem(golden.mesh_from(fx, name + "_"))
+        np.testing.assert_array_equal(p.element_field(0, fx[name + "_points"]), fx[name + "_field"])
+    for name in ("sphere", "coax"):
+        p = port.PortProblem(golden.mesh_from(fx, name + "_"))
+        A, b = p.matrix()
+        np.testing.assert_array_equal(A, fx[name + "_A"])
+        np.testing.assert_array_equal(b, fx[name + "_b"])
+        p.set_sigma(fx[name + "_sigma"])
+        np.testing.assert_array_equal(p.field(fx[name + "_points"]), fx[name + "_field"])
