@@ -515,7 +515,9 @@ def run_reference(args):
         "impl": "reference", "metric": "field evals/s (points/s; EPI/s = points/s x 44,000 elements) at <=1e-9 rel. "
                                        "error vs FP64",
         "value": v, "unit": "points/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
-        "higher_is_better": True, "dtype": "f64", "data": "synthetic (seeded coax mesh and gap points)",
+        "ms_per_step": N_POINTS / v * 1e3,  # one step = the 1,000,000 points at the sampled rate
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded coax mesh and gap points)",
         "config": {"workload": "coax: 40,000 rectangles + 4,000 cap triangles, 1,000,000 gap points per GPU, "
                                "GMRES to 1e-10", "elements": 44000, "points_per_gpu": N_POINTS},
         "cpu_baseline": {"value": v, "unit": "points/s", "cores": workers, "kind": "reference", "sample": sample},
