@@ -158,14 +158,22 @@ __device__ __forceinline__ void ell_KE_EK(double k, double& K, double& E, double
         EK = (E - K) / k2;
         return;
     }
-    double k2n = 1., ek = 0.;
-    for (int n = 0; n < kEkTerms; n++) {
-        ek += c_ek_coef[n] * k2n;
-        k2n *= k2;
-        if (k2n < 1.e-16)
+    // the same terms as ell_EK (a term is added while the power before it is >= 1e-16 after the
+    // previous one), even and odd terms on two power chains of stride k^4 so that neither the
+    // powers nor the sums form one serial chain; the two sums are added at the end
+    const double k4 = k2 * k2;
+    double pe = 1., po = k2, se = 0., so = 0.;
+    for (int n = 0; n + 1 < kEkTerms; n += 2) {
+        se += c_ek_coef[n] * pe;
+        if (po < 1.e-16)
+            break;
+        so += c_ek_coef[n + 1] * po;
+        pe *= k4;
+        po *= k4;
+        if (pe < 1.e-16)
             break;
     }
-    EK = ek;
+    EK = se + so;
 }
 
 // evaluation point (z, r) and generator (za, ra) -> (zb, rb) of length len; the ring sits at
