@@ -111,6 +111,25 @@ def conic_sphere(n_sections: int = 200, radius: float = 1.0, potential: float = 
     return m
 
 
+def conic_disk(n_sections: int = 128, radius: float = 1.0, power: float = 1.5, potential: float = 1.0) -> Mesh:
+    """Flat disk of ``n_sections`` annular conic sections at z = 0, from the rim inwards, their
+    widths growing like a power law away from the rim: the mesh of the reference's disk
+    capacitance test (UnitTest/KEMField/Fields/src/DiskCapacitanceTest.cc:47-69, with its
+    interval split at lines 117-141: 2 n segments over the diameter, symmetric, widths
+    (mid)((i+1)/n)^p - (i/n)^p). Capacitance 8 eps0 R."""
+    n = n_sections
+    mid = radius  # half of the diameter
+    r_out, r_in = np.empty(n), np.empty(n)
+    r0 = r1 = radius
+    for i in range(n):  # r1 -= segment, in sequence, as the test builds its sections
+        r1 -= mid * (((i + 1) / n) ** power - (i / n) ** power)
+        r_out[i], r_in[i] = r0, max(r1, 0.0)  # the last edge lands on the axis up to rounding
+        r0 = r1
+    m = axisymmetric(CONIC_SECTION, r_out, 0.0, r_in, 0.0, potential, name="conic-disk")
+    m.meta = {"n_sections": n, "radius": radius, "power": power}
+    return m
+
+
 def conic_coax(n_z: int = 100, n_cap: int = 10, r_in: float = 0.5, r_out: float = 1.0, length: float = 4.0,
                v_in: float = -1000.0, v_out: float = 0.0, n_rings: int = 0) -> Mesh:
     """Axisymmetric counterpart of :func:`coax`: inner and outer cylinders of ``n_z``

@@ -145,3 +145,17 @@ def test_port_axisymmetric_elements_bit_exact():
         np.testing.assert_array_equal(b, fx[name + "_b"])
         p.set_sigma(fx[name + "_sigma"])
         np.testing.assert_array_equal(p.field(fx[name + "_points"]), fx[name + "_field"])
+
+
+def test_disk_capacitance_known_answer():
+    # DiskCapacitanceTest.cc:47-113: 128 conic sections clustered at the rim, C = Q / eps0 = 8 R
+    # within 1e-2, on the C restatement (and its matrix equals the reference build's)
+    from oracle import port
+
+    m = G.conic_disk()
+    p = port.PortProblem(m)
+    A, b = p.matrix()
+    x = np.linalg.solve(A, b)
+    assert abs(float((x * m.areas()).sum()) / 8.8541878128e-12 - 8.0) < 1e-2
+    if ref.available():
+        np.testing.assert_array_equal(ref.RefProblem(m).matrix(), A)

@@ -110,3 +110,20 @@ def test_robin_hood_on_the_assembled_axisymmetric_operator(ctx):
     assert st["rel_residual"] <= 1e-10 and st["subiterations"] > 0
     ref = fx["sphere_sigma"]
     assert np.max(np.abs(x - ref)) / np.max(np.abs(ref)) < 1e-7
+
+
+def test_disk_capacitance(ctx):
+    # the reference's DiskCapacitanceTest mesh (128 flat conic sections): coplanar neighbours
+    # put every collocation point on the extension of the other generators, the near branch
+    # with the foot point outside the generator; device solves against the oracle's direct
+    # solution and the known answer C = 8 eps0 R (test tolerance 1e-2)
+    from oracle import port
+
+    m = G.conic_disk()
+    ctx.SetGeometry(m)
+    A, b = port.PortProblem(m).matrix()
+    ref = np.linalg.solve(A, b)
+    for mode in (K.SOLVE_PLAIN, K.SOLVE_ASSEMBLED):
+        x, _ = ctx.Solve(tol=1e-12, mode=mode)
+        assert np.max(np.abs(x - ref)) / np.max(np.abs(ref)) < 1e-9
+        assert abs(float((x * m.areas()).sum()) / 8.8541878128e-12 - 8.0) < 1e-2
