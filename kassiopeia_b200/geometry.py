@@ -114,15 +114,14 @@ def conic_sphere(n_sections: int = 200, radius: float = 1.0, potential: float = 
 def conic_disk(n_sections: int = 128, radius: float = 1.0, power: float = 1.5, potential: float = 1.0) -> Mesh:
     """Flat disk of ``n_sections`` annular conic sections at z = 0, from the rim inwards, their
     widths growing like a power law away from the rim: the mesh of the reference's disk
-    capacitance test (UnitTest/KEMField/Fields/src/DiskCapacitanceTest.cc:47-69, with its
-    interval split at lines 117-141: 2 n segments over the diameter, symmetric, widths
-    (mid)((i+1)/n)^p - (i/n)^p). Capacitance 8 eps0 R."""
+    capacitance test (UnitTest/KEMField/Fields/src/DiskCapacitanceTest.cc:47-69: the first half
+    of :func:`power_interval` over the diameter in 2 n segments). Capacitance 8 eps0 R."""
     n = n_sections
-    mid = radius  # half of the diameter
+    seg = power_interval(2.0 * radius, 2 * n, power)[:n]  # the rim-to-centre half of a diameter
     r_out, r_in = np.empty(n), np.empty(n)
     r0 = r1 = radius
     for i in range(n):  # r1 -= segment, in sequence, as the test builds its sections
-        r1 -= mid * (((i + 1) / n) ** power - (i / n) ** power)
+        r1 -= seg[i]
         r_out[i], r_in[i] = r0, max(r1, 0.0)  # the last edge lands on the axis up to rounding
         r0 = r1
     m = axisymmetric(CONIC_SECTION, r_out, 0.0, r_in, 0.0, potential, name="conic-disk")
@@ -199,6 +198,55 @@ def line_segments(p0, p1, diameter, value, boundary=DIRICHLET) -> Mesh:
 
 
 # --------------------------------------------------------------------------- icosphere
+def power_interval(length: float, n: int, power: float) -> np.ndarray:
+    """Segment lengths of an interval refined towards both ends: n segments symmetric about
+    the middle, half-interval widths ((i+1)/(n/2))^p - (i/(n/2))^p, a middle segment of length /
+    n when n is odd (the DiscretizeInterval of the reference's capacitance tests,
+    UnitTest/KEMField/Fields/src/DiskCapacitanceTest.cc:117-141)."""
+    seg = np.empty(n)
+    if n == 1:
+        seg[0] = length
+        return seg
+    mid = length * 0.5
+    if n % 2 == 1:
+        seg[n // 2] = length / n
+        mid -= length / (2 * n)
+    for i in range(n // 2):
+        inc1 = (i / (n / 2.0)) ** power
+        inc2 = ((i + 1) / (n / 2.0)) ** power
+        seg[i] = seg[n - (i + 1)] = mid * (inc2 - inc1)
+    return seg
+
+
+def cube(scale: int = 8, power: float = 1.5, side: float = 1.0, potential: float = 1.0) -> Mesh:
+    """Cube of ``side`` centred at the origin, each face ``scale`` x ``scale`` rectangles on the
+    power-law grid of :func:`power_interval` (the box of the reference's cube capacitance test,
+    UnitTest/KEMField/Fields/src/CubeCapacitanceTest.cc:43-60: mesh count 8, power 1.5).
+    Capacitance 0.6606785 x 4 pi eps0 side."""
+    edges = -side / 2 + np.concatenate([[0.0], np.cumsum(power_interval(side, scale, power))])
+    edges[-1] = side / 2
+    u0, v0 = np.meshgrid(edges[:-1], edges[:-1], indexing="ij")
+    u1, v1 = np.meshgrid(edges[1:], edges[1:], indexing="ij")
+    u0, v0, u1, v1 = u0.ravel(), v0.ravel(), u1.ravel(), v1.ravel()
+    h = np.full(u0.shape, side / 2)
+    parts = []
+    for axis in range(3):
+        for sgn in (-1.0, 1.0):
+            def pt(u, v):
+                c = [None, None, None]
+                c[axis] = sgn * h
+                others = [k for k in range(3) if k != axis]
+                c[others[0]], c[others[1]] = u, v
+                return np.stack(c, axis=1)
+            parts.append(rectangles_from_corners(pt(u0, v0), pt(u1, v0), pt(u0, v1), potential))
+    m = parts[0]
+    for p in parts[1:]:
+        m = m.concat(p)
+    m.name = "cube"
+    m.meta = {"scale": scale, "power": power, "side": side}
+    return m
+
+
 def icosphere_vertices(level: int, radius: float = 1.0):
     """Vertices and faces of a subdivided icosahedron (20 * 4**level faces, outward winding)."""
     t = (1.0 + 5.0 ** 0.5) / 2.0

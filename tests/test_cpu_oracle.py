@@ -159,3 +159,15 @@ def test_disk_capacitance_known_answer():
     assert abs(float((x * m.areas()).sum()) / 8.8541878128e-12 - 8.0) < 1e-2
     if ref.available():
         np.testing.assert_array_equal(ref.RefProblem(m).matrix(), A)
+
+
+def test_cube_capacitance_known_answer():
+    # CubeCapacitanceTest.cc:43-113: unit cube, 8 x 8 rectangles per face on a power-1.5 grid,
+    # C / (4 pi eps0) = 0.6606785 within 1e-2, on the C restatement
+    from oracle import port
+
+    m = G.cube()
+    p = port.PortProblem(m)
+    A, b = p.matrix()
+    x = np.linalg.solve(A, b)
+    assert abs(float((x * m.areas()).sum()) / (4 * np.pi * 8.8541878128e-12) - 0.6606785) < 1e-2

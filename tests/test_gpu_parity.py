@@ -292,3 +292,19 @@ def test_empty_and_boundary_sized_point_sets(ctx):
     for n in (1, 127, 4095, 4096, 4097, 4097 + 129):
         out = ctx.ElectricFieldAndPotential(P[:n])
         np.testing.assert_allclose(out, ref[:n], rtol=1e-13, atol=1e-13 * np.abs(ref).max())
+
+
+def test_cube_capacitance(ctx):
+    # the reference's CubeCapacitanceTest box (384 rectangles, refined towards the edges):
+    # device solves against the oracle's direct solution and the accepted 0.6606785 (tol 1e-2)
+    from oracle import port
+
+    m = G.cube()
+    ctx.SetGeometry(m)
+    A, b = port.PortProblem(m).matrix()
+    ref = np.linalg.solve(A, b)
+    for mode in (K.SOLVE_PLAIN, K.SOLVE_MIXED, K.SOLVE_ASSEMBLED):
+        x, _ = ctx.Solve(tol=1e-12, mode=mode)
+        assert np.max(np.abs(x - ref)) / np.max(np.abs(ref)) < 1e-9, mode
+        c = float((x * m.areas()).sum()) / (4 * np.pi * 8.8541878128e-12)
+        assert abs(c - 0.6606785) < 1e-2
