@@ -17,7 +17,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "kemcu.h")
 OK, EINVAL, ECUDA, ENONFINITE, ENOTCONVERGED, ETIMEOUT, ENOMEM, ESTATE = 0, -1, -2, -3, -4, -5, -6, -7
 FP64, MIXED = 0, 1
 FIELD_AND_POTENTIAL, POTENTIAL, FIELD = 0, 1, 2
-SOLVE_PLAIN, SOLVE_MIXED, SOLVE_ASSEMBLED = 0, 1, 2
+SOLVE_PLAIN, SOLVE_MIXED, SOLVE_ASSEMBLED, SOLVE_ASSEMBLED_FP64 = 0, 1, 2, 3
 TRACK_ACTIVE, TRACK_HIT, TRACK_MAX_STEPS, TRACK_LEFT, TRACK_NONFINITE = 0, 1, 2, 3, 4
 
 _ERRNAMES = {EINVAL: "EINVAL", ECUDA: "ECUDA", ENONFINITE: "ENONFINITE", ENOTCONVERGED: "ENOTCONVERGED",
@@ -66,6 +66,24 @@ def header_symbols() -> list[str]:
     txt = open(HEADER).read()
     decl = r"^\s*(?:int|void|double|size_t|unsigned\s+long\s+long|const\s+char\s*\*)\s*(kemcu_[a-z0-9_]+)\s*\("
     return sorted(set(re.findall(decl, txt, flags=re.M)))
+
+
+def header_constant(name: str) -> int:
+    """Value of an integer #define of the C header (literals, u suffixes, <<, *, /, +, - and
+    other such defines), so that tests follow the header instead of restating its numbers."""
+    txt = open(HEADER).read()
+    defs = dict(re.findall(r"^\s*#define\s+(KEMCU_[A-Z0-9_]+)\s+(.+?)\s*(?:/\*.*)?$", txt, flags=re.M))
+
+    def value(n, depth=0):
+        if n not in defs or depth > 8:
+            raise KeyError(f"{n} is not an integer #define of {HEADER}")
+        expr = re.sub(r"\b(\d+)[uUlL]+\b", r"\1", defs[n])
+        expr = re.sub(r"\bKEMCU_[A-Z0-9_]+\b", lambda m: str(value(m.group(0), depth + 1)), expr)
+        if not re.fullmatch(r"[0-9\s()+\-*/<>]+", expr):
+            raise ValueError(f"{n}: cannot evaluate {defs[n]!r}")
+        return int(eval(expr.replace("/", "//"), {"__builtins__": {}}))
+
+    return value(name)
 
 
 def lib():

@@ -28,7 +28,8 @@ def test_noalloc_matches_allocating_entry_point_twice():
     ctx.SetGeometry(mesh)
     rng = np.random.default_rng(3)
     ctx.SetSigma(np.where(mesh.value < -1.0, -1e-8, 1e-8) * (1 + 0.1 * rng.normal(size=mesh.n)))
-    limit = L_max = 8 * 2**20 // 32
+    limit = N.header_constant("KEMCU_NOALLOC_MAX_POINTS")
+    assert limit * 32 == N.header_constant("KEMCU_NOALLOC_SCRATCH_BYTES")
     # two calls in a row with different sizes: the second reuses (and must fully overwrite)
     # the scratch the first one left behind
     for n_pts, prec in ((3000, K.MIXED), (20000, K.FP64)):
@@ -47,13 +48,22 @@ def test_noalloc_matches_allocating_entry_point_twice():
         r, o = ref.cpu().numpy(), out.cpu().numpy()
         # same kernels, same element splits up to the scratch cap: agreement to rounding
         assert np.max(np.abs(o - r) / np.abs(r).max(axis=0)) < 1e-12
-    # sizes beyond the fixed scratch are refused with a clear error
-    big = limit + 1
-    rc = L.kemcu_field_dev_noalloc(ctx._h, C.c_void_p(P.data_ptr()), big, C.c_void_p(out.data_ptr()), K.FP64,
-                                   K.FIELD_AND_POTENTIAL)
+    # the largest accepted call (one partial sum per point fills the scratch exactly) against
+    # the allocating entry point, then one point more, refused with a clear error
+    P = torch.from_numpy(G.gap_points(limit + 1, seed=5)).cuda()
+    ref = torch.zeros((limit, 4), dtype=torch.float64, device="cuda")
+    out = torch.full((limit + 1, 4), float("nan"), dtype=torch.float64, device="cuda")
+    assert L.kemcu_field_dev(ctx._h, C.c_void_p(P.data_ptr()), limit, C.c_void_p(ref.data_ptr()), K.MIXED,
+                             K.POTENTIAL) == 0
+    rc = L.kemcu_field_dev_noalloc(ctx._h, C.c_void_p(P.data_ptr()), limit, C.c_void_p(out.data_ptr()), K.MIXED,
+                                   K.POTENTIAL)
+    assert rc == 0, L.kemcu_last_error(ctx._h).decode()
+    r, o = ref.cpu().numpy()[:, 3], out.cpu().numpy()[:limit, 3]
+    assert np.max(np.abs(o - r)) / np.abs(r).max() < 1e-12
+    rc = L.kemcu_field_dev_noalloc(ctx._h, C.c_void_p(P.data_ptr()), limit + 1, C.c_void_p(out.data_ptr()),
+                                   K.FP64, K.FIELD_AND_POTENTIAL)
     assert rc == N.EINVAL
     assert "at most" in L.kemcu_last_error(ctx._h).decode()
-    assert L_max == limit
     ctx.close()
 
 
