@@ -68,8 +68,11 @@ enum kemcu_solve_mode {
     KEMCU_SOLVE_PLAIN = 0,     /* GMRES, FP64 matrix-free matvec (the reference algorithm) */
     KEMCU_SOLVE_MIXED = 1,     /* iterative refinement: inner GMRES on the MIXED matrix-free
                                   operator, FP64 matrix-free residual and correction */
-    KEMCU_SOLVE_ASSEMBLED = 2  /* operator assembled once in HBM (FP64, plus an FP32 copy);
+    KEMCU_SOLVE_ASSEMBLED = 2, /* operator assembled once in HBM (FP64, plus an FP32 copy);
                                   inner GMRES on FP32, FP64 residual (refinement) */
+    KEMCU_SOLVE_ASSEMBLED_FP64 = 3 /* GMRES on the assembled FP64 operator alone (no FP32 copy,
+                                  no refinement): the plain algorithm with the same assembly,
+                                  which separates the gain of assembly from that of precision */
 };
 
 typedef struct kemcu_ctx kemcu_ctx;
@@ -141,7 +144,9 @@ int kemcu_field_dev(kemcu_ctx* ctx, const double* dP, size_t n, double* dout4, i
    For callers that cannot call cudaMalloc while they evaluate fields: a host framework that has
    given all device memory to its own pool allocator, or a loop that must not incur the implicit
    device synchronisation a cudaMalloc / cudaFree can cause while other work runs on the GPU.
-   Same result as kemcu_field_dev (points evaluated in the caller's order, not re-sorted). The
+   Same result as kemcu_field_dev to rounding: the points are evaluated in the caller's order
+   (kemcu_field_dev re-sorts them above 4,096 points) and the element list may be split into
+   fewer partial sums, so the summation order can differ. The
    element-split partial sums live in one file-scope device array of
    KEMCU_NOALLOC_SCRATCH_BYTES (8 MiB, held by every GPU that loads the library until the
    process exits); its device address is looked up once per context in kemcu_create. n may be

@@ -342,6 +342,34 @@ def coax_potential(r, r_in=0.5, r_out=1.0, v_in=-1000.0, v_out=0.0):
     return v_out + (v_in - v_out) * np.log(r_out / r) / np.log(r_out / r_in)
 
 
+def coax_density(mesh: Mesh, seed: int = 31, spread: float = 0.05, eps0: float = 8.8541878128e-12) -> np.ndarray:
+    """A fixed charge density for field evaluations on :func:`coax` meshes without a solve:
+    the ideal infinite-coax surface density eps0 (v_out - v_in) / (r ln(r_out / r_in)) (negative
+    on the inner electrode, positive on the outer one, a tenth of the outer value on the caps)
+    times 1 + spread N(0, 1) from a seeded generator. The direct sum is linear in the density,
+    so any fixed density pins the evaluation; this one has the solution's size and signs."""
+    meta = mesh.meta
+    r_in, r_out = meta.get("r_in", 0.5), meta.get("r_out", 1.0)
+    dv = meta.get("v_out", 0.0) - meta.get("v_in", -1000.0)
+    c = mesh.centroids()
+    r = np.hypot(c[:, 0], c[:, 1])
+    s = eps0 * dv / (r * np.log(r_out / r_in))
+    inner = (mesh.shape == RECTANGLE) & (np.abs(r - r_in) < 0.5 * (r_out - r_in))
+    s = np.where(mesh.shape == RECTANGLE, np.where(inner, -s, s), 0.1 * s)
+    rng = np.random.default_rng(seed)
+    return s * (1.0 + spread * rng.normal(size=mesh.n))
+
+
+def sphere_density(mesh: Mesh, radius: float = 1.0, potential: float = 1.0, seed: int | None = None,
+                   spread: float = 0.1, eps0: float = 8.8541878128e-12) -> np.ndarray:
+    """Surface density eps0 V / R of a conducting sphere at potential V, optionally times
+    1 + spread N(0, 1) from a seeded generator (the perturbed density of configuration 4)."""
+    s = np.full(mesh.n, eps0 * potential / radius)
+    if seed is not None:
+        s = s * (1.0 + spread * np.random.default_rng(seed).normal(size=mesh.n))
+    return s
+
+
 # --------------------------------------------------------------------------- stacked rings
 def stacked_rings(n_rings: int = 8, n_phi: int = 125, n_z: int = 50, r_min: float = 0.3, r_max: float = 1.0,
                   height: float = 0.2, gap: float = 0.1, jitter: float = 1e-3, seed: int = 5) -> Mesh:

@@ -29,6 +29,24 @@ Fixtures:
                  and the subdivided near branch, on and beyond the generator, on the axis); a
                  120-section sphere and a conic coax with rings: matrix, right-hand side,
                  direct solution, field at seeded points
+  c1_sphere      configuration 1 at its stated size: 1,280-triangle icosphere at 1 V, the
+                 reference's matrix solved directly (and its GMRES at 1e-10 for the record), its
+                 Robin Hood at 1e-8, the field of the direct density at the 10,000 seeded shell
+                 points
+  c2_coax        configuration 2 at its stated size (44,000 elements): the field of a fixed
+                 density (geometry.coax_density) at 200 seeded gap points; 64 sampled rows of
+                 the boundary-integral matrix: 64 entries each (diagonal, nearest neighbours,
+                 seeded columns) and the rows of A x for a seeded x
+  c3_tracks      configuration 3's tracking in the configuration-1 field: 16 electrons x up to
+                 1,000 RK8 steps of 1e-11 s, stopping at the sphere (|x| <= 1 m); states every
+                 50 steps, the steps taken and the final states
+  c4_adjoint     configuration 4 at its stated size: 20,480-triangle sphere, perturbed density
+                 (geometry.sphere_density, seed 4), 4,096 probes, L = sum_p (E_z + phi):
+                 dL/dsigma for 512 seeded elements and central differences (h = 1e-6 m) of L
+                 over the 9 vertex coordinates of 16 elements whose quadrature bands the
+                 perturbation leaves unchanged at every probe
+  c5_rings       configuration 5 at its stated size (100,000 jittered triangles): 64 sampled
+                 matrix rows, 64 entries each, and the rows of A x for 8 seeded right-hand sides
 
 Usage: python tests/golden/make_golden.py [fixture ...]   (default: all)
 """
@@ -283,8 +301,168 @@ def axisym():
     save("axisym", **out)
 
 
+# ----------------------------------------------------------------------------- configurations
+# Fixtures at the benchmark configurations' stated sizes. Their meshes are regenerated by the
+# tests with the same geometry functions; a checksum of each mesh is stored with it.
+def mesh_checksum(m):
+    return np.array([m.geom.sum(), np.abs(m.geom).sum(), m.value.sum(), float(m.n)])
+
+
+def sampled_rows(p, m, n_rows, n_cols, seed):
+    """n_rows seeded rows of the reference's matrix; per row the diagonal, the nearest
+    neighbours by centroid (the analytic near-field band) and seeded columns, n_cols in all."""
+    rng = np.random.default_rng(seed)
+    rows = np.sort(rng.choice(m.n, n_rows, replace=False))
+    A = p.matrix(rows)
+    c = m.centroids()
+    cols = np.zeros((n_rows, n_cols), np.int64)
+    for k, i in enumerate(rows):
+        near = np.argsort(np.linalg.norm(c - c[i], axis=1))[: n_cols // 4]
+        rest = np.setdiff1d(np.arange(m.n), near)
+        cols[k] = np.concatenate([near, rng.choice(rest, n_cols - len(near), replace=False)])
+    return rows, cols, A
+
+
+def c1_sphere():
+    m = G.icosphere(3)
+    p = ref.RefProblem(m)
+    A = p.matrix()
+    b = p.rhs()
+    xd = np.linalg.solve(A, b)
+    xg, it, r = p.gmres(1e-10)
+    xr, itr, rr = p.robinhood(1e-8)
+    pts = G.shell_points(10000, seed=2025)
+    p.set_sigma(xd)
+    f = p.field(pts)
+    save("c1_sphere", sigma_direct=xd, b=b, gmres_sigma=xg, gmres_iterations=np.array(it),
+         robinhood_sigma=xr, robinhood_iterations=np.array(itr), robinhood_residual=np.array(rr),
+         gmres_true_residual=np.array(np.linalg.norm(b - A @ xg) / np.linalg.norm(b)), points=pts, field=f,
+         checksum=mesh_checksum(m))
+
+
+def c2_coax():
+    m = G.coax()
+    sigma = G.coax_density(m)
+    p = ref.RefProblem(m)
+    p.set_sigma(sigma)
+    pts = G.gap_points(200, seed=2026)
+    f = p.field(pts)
+    rows, cols, A = sampled_rows(p, m, 64, 64, seed=2027)
+    x = np.random.default_rng(2028).normal(size=m.n) * 1e-8
+    save("c2_coax", points=pts, field=f, rows=rows, cols=cols, entries=np.take_along_axis(A, cols, axis=1),
+         x_seed=np.array(2028), Ax=A @ x, checksum=mesh_checksum(m))
+
+
+def _track_worker(args):
+    geom_arrays, sigma, st, nsteps = args
+    sys.path.insert(0, ROOT)
+    from kassiopeia_b200.geometry import Mesh
+    from oracle import ref as R
+
+    q = R.RefProblem(Mesh(*geom_arrays))
+    q.set_sigma(sigma)
+    _, n, tr = q.rk8_track(st, 1e-11, nsteps, stop_radius=1.0, record=True)
+    return n, tr
+
+
+def c3_tracks():
+    import multiprocessing as mp
+
+    fx = dict(np.load(os.path.join(HERE, "c1_sphere.npz")))
+    m = G.icosphere(3)
+    # 8 electrons whose straight flight line meets the sphere between steps 100 and 900 and 8
+    # that stay clear of it, from a seeded batch, so both ends of a track are covered
+    cand = G.electrons(4096, seed=2029)
+    x, p = cand[:, 2:5], cand[:, 5:8]
+    mc = G.ELECTRON_MASS * G.SPEED_OF_LIGHT
+    v = p / (G.ELECTRON_MASS * np.sqrt(1.0 + np.sum(p * p, axis=1) / mc ** 2))[:, None]
+    b = np.sum(x * v, axis=1)
+    vv = np.sum(v * v, axis=1)
+    disc = b * b - vv * (np.sum(x * x, axis=1) - 1.0)
+    t_hit = np.where((disc > 0) & (b < 0), (-b - np.sqrt(np.maximum(disc, 0))) / vv, np.inf) / 1e-11
+    hit = np.flatnonzero((t_hit > 100) & (t_hit < 900))[:8]
+    miss = np.flatnonzero(~np.isfinite(t_hit))[:8]
+    idx = np.sort(np.concatenate([hit, miss]))
+    st0 = cand[idx]
+    arrays = (m.shape, m.boundary, m.geom, m.value)
+    with mp.get_context("spawn").Pool(min(8, os.cpu_count() or 1)) as pool:
+        res = pool.map(_track_worker, [(arrays, fx["sigma_direct"], st0[k], 1000) for k in range(16)])
+    steps = np.array([r[0] for r in res], np.int32)
+    every = 50
+    snaps = np.full((16, 1000 // every, 8), np.nan)
+    for k, (n, tr) in enumerate(res):
+        for s in range(every, n + 1, every):
+            snaps[k, s // every - 1] = tr[s - 1]
+    final = np.stack([r[1][r[0] - 1] for r in res])
+    save("c3_tracks", state0=st0, candidates_seed=np.array(2029), candidates_index=idx, steps=steps, every=np.array(every), snapshots=snaps, final=final,
+         dt=np.array(1e-11), max_steps=np.array(1000), sphere_radius=np.array(1.0))
+
+
+def _tri_bands(v0, v1, v2, P):
+    """the reference's triangle rule band of every probe (0 RWG, 1 33-point, 2 12-point,
+    3 7-point): ratio |P - centroid| / ((|P1-P0| + |P2-P0| + |P2-P1|) / 3)"""
+    size = (np.linalg.norm(v1 - v0) + np.linalg.norm(v2 - v0) + np.linalg.norm(v2 - v1)) / 3.0
+    ratio = np.linalg.norm(P - (v0 + v1 + v2) / 3.0, axis=1) / size
+    return np.digitize(ratio, [3.42, 30.4, 131.4], right=True), ratio
+
+
+def c4_adjoint():
+    m = G.icosphere(5)
+    sigma = G.sphere_density(m, seed=4)
+    P = G.shell_points(4096, seed=44)
+    w = np.zeros((4096, 4))
+    w[:, 2] = 1.0
+    w[:, 3] = 1.0
+    rng = np.random.default_rng(2030)
+    ds_elems = np.sort(rng.choice(m.n, 512, replace=False))
+    p = ref.RefProblem(m)
+    dsig = np.array([np.sum(w * p.element_field(k, P)) for k in ds_elems])
+    g = m.geom
+    verts = np.stack([g[:, 2:5], g[:, 2:5] + g[:, 0:1] * g[:, 5:8], g[:, 2:5] + g[:, 1:2] * g[:, 8:11]], axis=1)
+    h = 1e-6
+    chosen, fd = [], []
+    for j in rng.permutation(m.n):
+        if len(chosen) == 16:
+            break
+        base, ratio = _tri_bands(*verts[j], P)
+        cuts = np.array([3.42, 30.4, 131.4])
+        if np.min(np.abs(ratio[:, None] / cuts[None, :] - 1.0)) < 1e-4:
+            continue  # a probe close to a band cut: the difference quotient would straddle rules
+        ok = True
+        rowfd = np.zeros(9)
+        for c in range(9):
+            vals = []
+            for sgn in (1.0, -1.0):
+                vv = verts[j].copy()
+                vv[c // 3, c % 3] += sgn * h
+                if not np.array_equal(_tri_bands(*vv, P)[0], base):
+                    ok = False
+                    break
+                e = G.triangles_from_vertices(vv[0], vv[1], vv[2], 1.0)
+                vals.append(sigma[j] * float(np.sum(w * ref.RefProblem(e).element_field(0, P))))
+            if not ok:
+                break
+            rowfd[c] = (vals[0] - vals[1]) / (2 * h)
+        if ok:
+            chosen.append(j)
+            fd.append(rowfd)
+    order = np.argsort(chosen)
+    save("c4_adjoint", sigma_seed=np.array(4), points=P, w=w, dsigma_elems=ds_elems, dsigma=dsig,
+         fd_elems=np.array(chosen)[order], dvert_fd=np.array(fd)[order], h=np.array(h),
+         fd_vertices=verts[np.array(chosen)[order]], checksum=mesh_checksum(m))
+
+
+def c5_rings():
+    m = G.stacked_rings()
+    p = ref.RefProblem(m)
+    rows, cols, A = sampled_rows(p, m, 64, 64, seed=2031)
+    X = np.random.default_rng(2032).normal(size=(8, m.n)) * 1e-8
+    save("c5_rings", rows=rows, cols=cols, entries=np.take_along_axis(A, cols, axis=1), x_seed=np.array(2032),
+         Ax=(A @ X.T).T, checksum=mesh_checksum(m))
+
+
 FIXTURES = {f.__name__: f for f in (rules, integrators, lines, icosphere, mixed_small, coax_small, rk8, adjoint,
-                                     robinhood, axisym)}
+                                     robinhood, axisym, c1_sphere, c2_coax, c3_tracks, c4_adjoint, c5_rings)}
 
 if __name__ == "__main__":
     for name in sys.argv[1:] or list(FIXTURES):

@@ -84,3 +84,32 @@ def test_robin_hood_callback_stops(ctx):
         ctx.SetIterationCallback(None)
     assert st["status"] == K._native.ENOTCONVERGED
     assert [s[0] for s in seen] == [1, 2, 3]
+
+
+def test_robin_hood_c1_at_size_on_many_ctas(ctx):
+    # configuration 1 (1,280 triangles): the rows are spread over several CTAs of one
+    # cooperative launch; the reference's KRobinHood needs the same number of checks, and the
+    # matrix-free and assembled columns give the same corrections bit for bit
+    from kassiopeia_b200 import geometry as G
+
+    fx = golden.load("c1_sphere")
+    ctx.SetGeometry(G.icosphere(3))
+    x, st = ctx.SolveRobinHood(tol=1e-8)
+    assert st["rel_residual"] <= 1e-8
+    assert abs(st["iterations"] - int(fx["robinhood_iterations"])) <= 1
+    ref_err = rel(fx["robinhood_sigma"], fx["sigma_direct"])
+    assert rel(x, fx["sigma_direct"]) <= max(5 * ref_err, 100 * 1e-8)
+    xa, sa = ctx.SolveRobinHood(tol=1e-8, assembled=True)
+    assert sa["subiterations"] == st["subiterations"]
+    np.testing.assert_array_equal(xa, x)
+
+
+def test_robin_hood_many_ctas_equals_gmres_solution(ctx):
+    # 5,120 triangles: twenty CTAs exchange their residual maxima every correction
+    from kassiopeia_b200 import geometry as G
+
+    ctx.SetGeometry(G.icosphere(4))
+    xg, _ = ctx.Solve(tol=1e-12, mode=K.SOLVE_ASSEMBLED)
+    x, st = ctx.SolveRobinHood(tol=1e-9, assembled=True)
+    assert st["rel_residual"] <= 1e-9
+    assert rel(x, xg) < 1e-6
