@@ -38,8 +38,8 @@ sys.path.insert(0, ROOT)
 N_POINTS = 1_000_000
 TOL = 1e-10
 # DRAM bytes (read + write) of one MIXED direct-sum launch over the default 1,000,000-point
-# workload, from a one-pass ncu capture (profiles/field_kernel_coax1m_dram.md); bench.py
-# cannot run ncu itself, so the figure is reported only for that workload
+# workload, from a one-pass ncu capture of `python bench.py --profile --points 1000000`;
+# bench.py cannot run ncu itself, so the figure is reported only for that workload
 FIELD_TRAFFIC_BYTES_1M = 69.49e6 + 83.10e6
 # algorithmic flops per element-point interaction (field + potential) by band:
 # cubature / Gauss with n nodes: 20 n + 30 (node sums, ratio test); analytic near field:
@@ -70,22 +70,35 @@ def _ref_worker(args):
     p = ref.RefProblem(m)
     p.set_sigma(sigma)
     t0 = time.perf_counter()
-    p.field(pts)
-    return time.perf_counter() - t0, len(pts)
+    out = p.field(pts)
+    return time.perf_counter() - t0, len(pts), out
+
+
+def host_cores():
+    """(physical cores, logical CPUs) of this host"""
+    logical = os.cpu_count() or 1
+    try:
+        import psutil
+
+        physical = psutil.cpu_count(logical=False) or logical
+    except Exception:
+        physical = logical
+    return physical, logical
 
 
 def cpu_reference_rate(mesh, sigma, pts, workers, seconds_target=12.0):
     """points/s of the reference CPU direct sum on `workers` processes (spawned), each taking a
-    disjoint slice of a bounded point sample; returns (points/s, sample description)."""
+    disjoint slice of a bounded point sample; returns (points/s, sample description, the
+    sampled points, the reference's (Ex, Ey, Ez, phi) there)."""
     from oracle import ref as R
 
     if not R.available():
-        return None, "oracle/_ref not built"
+        return None, "oracle/_ref not built", None, None
     # calibrate: one point on one process
     ctx = mp.get_context("spawn")
     arrays = (mesh.shape, mesh.boundary, mesh.geom, mesh.value)
     with ctx.Pool(1) as pool:
-        dt, _ = pool.map(_ref_worker, [(arrays, sigma, pts[:2])])[0]
+        dt, _, _ = pool.map(_ref_worker, [(arrays, sigma, pts[:2])])[0]
     per_point = dt / 2
     per_worker = max(1, int(seconds_target / max(per_point, 1e-6)))
     n = min(len(pts), per_worker * workers)
@@ -96,7 +109,28 @@ def cpu_reference_rate(mesh, sigma, pts, workers, seconds_target=12.0):
         res = pool.map(_ref_worker, [(arrays, sigma, c) for c in chunks if len(c)])
     wall = time.perf_counter() - t0
     busy = max(r[0] for r in res)
-    return n / busy, f"{n} of the {len(pts)} gap points on {workers} processes ({wall:.1f} s wall incl. setup)"
+    values = np.zeros((n, 4))
+    for i, r in enumerate(res):
+        values[i::workers] = r[2]
+    return (n / busy, f"{n} of the {len(pts)} gap points on {workers} processes ({wall:.1f} s wall incl. setup)",
+            sample, values)
+
+
+def accuracy_vs(out, ref):
+    """max per-point relative error of |E| and of phi, and max error relative to the largest
+    value of each quantity"""
+    eE = np.linalg.norm(out[:, :3] - ref[:, :3], axis=1) / np.linalg.norm(ref[:, :3], axis=1)
+    eP = np.abs(out[:, 3] - ref[:, 3]) / np.abs(ref[:, 3])
+    return {"max_rel_err_E_per_point": float(eE.max()), "max_rel_err_phi_per_point": float(eP.max()),
+            "max_err_E_over_max_E": float(np.abs(out[:, :3] - ref[:, :3]).max() / np.abs(ref[:, :3]).max()),
+            "max_err_phi_over_max_phi": float(np.abs(out[:, 3] - ref[:, 3]).max() / np.abs(ref[:, 3]).max())}
+
+
+def workload_config(world):
+    return {"workload": "coax: 40,000 rectangles + 4,000 cap triangles, 1,000,000 gap points per GPU, "
+                        "GMRES to 1e-10", "elements": 44000, "points_per_gpu": N_POINTS,
+            "parallelism": f"replicated geometry, points sharded over {world} GPU(s)",
+            "l2": "inputs re-read every step; 24 MB points + 11 MB elements, compute-bound kernel"}
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -159,13 +193,18 @@ def run_native(args, rank, world, dist):
     # charge densities: plain FP64 matrix-free GMRES (the reference algorithm) vs the
     # assembled mixed-precision solve with FP64 refinement
     if args.profile:
-        x_asm = np.where(mesh.value < -1.0, -1e-8, 1e-8)
+        x_asm = G.coax_density(mesh)
         st_plain = st_asm = {"seconds": float("nan"), "iterations": 0, "rel_residual": float("nan")}
         sigma_diff = float("nan")
     else:
         x_plain, st_plain = ctx.Solve(tol=TOL, max_iter=300, mode=K.SOLVE_PLAIN)
         x_asm, st_asm = ctx.Solve(tol=TOL, max_iter=300, mode=K.SOLVE_ASSEMBLED)  # includes the assembly
         st_asm["repeat_seconds"] = ctx.Solve(tol=TOL, max_iter=300, mode=K.SOLVE_ASSEMBLED)[1]["seconds"]
+        # the same assembled operator in FP64 alone (plain GMRES, no FP32 copy, no refinement):
+        # against the repeat above this isolates what precision alone gains in the solve
+        x_a64, st_a64 = ctx.Solve(tol=TOL, max_iter=300, mode=K.SOLVE_ASSEMBLED_FP64)
+        st_a64["repeat_seconds"] = ctx.Solve(tol=TOL, max_iter=300, mode=K.SOLVE_ASSEMBLED_FP64)[1]["seconds"]
+        st_asm["fp64_assembled"] = st_a64
         sigma_diff = float(np.max(np.abs(x_asm - x_plain)) / np.max(np.abs(x_plain)))
     ctx.SetSigma(x_asm)
 
@@ -233,17 +272,28 @@ def run_native(args, rank, world, dist):
     f32 = C.c_double()
     NN.lib().kemcu_fma_peak(ctx._h, C.byref(f64), C.byref(f32))
 
-    # tracking sample (configuration 3: 65,536 electrons in the 1,280-triangle sphere field)
     extra = {}
     axisym_case = None
     if not args.quick:
+        # Robin Hood on the coax (44,000 elements, tolerance 1e-8), a bounded number of
+        # corrections: columns from the assembled FP64 operator (already in place from the
+        # solves above) and computed on the fly
+        for assembled, name, cap in ((True, "assembled", 200_000), (False, "matrix_free", 20_000)):
+            _, rs = ctx.SolveRobinHood(tol=1e-8, assembled=assembled, max_subiterations=cap, raise_on_failure=False)
+            extra[f"robinhood_coax44k_{name}"] = {
+                "seconds": rs["seconds"], "corrections": rs["subiterations"], "checks": rs["iterations"],
+                "rel_residual_inf": rs["rel_residual"], "ms_per_correction": 1e3 * rs["seconds"] / rs["subiterations"],
+                "converged": rs["status"] == 0, "correction_cap": cap}
+        # tracking sample (configuration 3: 65,536 electrons in the 1,280-triangle sphere field,
+        # 50 steps per track in one persistent launch; the whole configured run is
+        # `bench.py --tracking-c3`)
         sph = G.icosphere(3)
         tctx = K.CUDAElectrostaticContext(dev)
         tctx.SetGeometry(sph)
         tctx.Solve(tol=TOL, mode=K.SOLVE_ASSEMBLED)
         E = G.electrons(65536, seed=99 + rank)
         for prec, name in ((K.FP64, "fp64"), (K.MIXED, "mixed")):
-            _, _, _, ts = tctx.TrackRK8(E, 1e-11, 10000, step_budget=2, sphere_radius=1.0, precision=prec)
+            _, _, _, ts = tctx.TrackRK8(E, 1e-11, 10000, step_budget=50, sphere_radius=1.0, precision=prec)
             extra[f"tracking_track_steps_per_s_{name}"] = ts["steps"] / ts["seconds"]
         # adjoint sample (configuration 4: 20,480 triangles, 4,096 probes)
         s5 = G.icosphere(5)
@@ -307,6 +357,15 @@ def run_native(args, rank, world, dist):
         counts=counts.tolist(), st_plain=st_plain, st_asm=st_asm, sigma_diff=sigma_diff, clocks=clk.summary(),
         extra=extra, mesh=mesh, sigma=x_asm, P=P, axisym=axisym_case)
     ctx.close()
+
+    def field_at(pts, precision):
+        """the field of the benched charge densities at pts (a fresh context on this GPU)"""
+        with K.CUDAElectrostaticContext(dev) as c:
+            c.SetGeometry(mesh)
+            c.SetSigma(x_asm)
+            return c.ElectricFieldAndPotential(pts, precision=precision)
+
+    res["field_at"] = field_at
     return res
 
 
@@ -359,6 +418,55 @@ def profile_axisym():
                           "points_per_s": len(P) / (ctx.last_kernel_ms * 1e-3)}), flush=True)
 
 
+def tracking_c3(args):
+    """Configuration 3 as configured: 65,536 electrons (1-18.6 keV, isotropic, starting in the
+    1.2-3 m shell) in the field of the 1,280-triangle sphere at 1 V, RK8 steps of 1e-11 s, every
+    track run to its end (|x| <= 1 m: electrode hit, or 10,000 steps), in persistent launches of
+    at most --c3-chunk steps per track (the host re-lists the active tracks between launches)."""
+    import kassiopeia_b200 as K
+    from kassiopeia_b200 import geometry as G
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    ctx = K.CUDAElectrostaticContext(dev)
+    sph = G.icosphere(3)
+    ctx.SetGeometry(sph)
+    ctx.Solve(tol=TOL, mode=K.SOLVE_ASSEMBLED)
+    n = args.c3_tracks
+    E = G.electrons(n, seed=99)
+    prec = K.MIXED if args.c3_precision == "mixed" else K.FP64
+    # the rate of a launch in which every slot is busy from start to end (all tracks active,
+    # 50 steps each): the reference for the slot occupancy of the whole run
+    _, _, _, full = ctx.TrackRK8(E, 1e-11, 10000, step_budget=50, sphere_radius=1.0, precision=prec)
+    full_rate = full["steps"] / full["seconds"]
+    st, steps, status = E.copy(), np.zeros(n, np.int32), np.zeros(n, np.int32)
+    launches, seconds, total = 0, 0.0, 0
+    with ClockSampler(dev) as clk:
+        while True:
+            st, steps, status, ts = ctx.TrackRK8(st, 1e-11, 10000, steps=steps, status=status,
+                                                step_budget=args.c3_chunk, sphere_radius=1.0, precision=prec)
+            if ts["steps"] == 0:
+                break
+            launches += 1
+            seconds += ts["seconds"]
+            total += ts["steps"]
+    T = K._native
+    hist = {name: int(np.sum(status == code)) for name, code in
+            (("hit", T.TRACK_HIT), ("max_steps", T.TRACK_MAX_STEPS), ("left", T.TRACK_LEFT),
+             ("nonfinite", T.TRACK_NONFINITE), ("active", T.TRACK_ACTIVE))}
+    rate = total / seconds
+    print(json.dumps({
+        "tracking_c3": {"tracks": n, "precision": args.c3_precision, "dt_s": 1e-11, "max_steps": 10000,
+                        "launches": launches, "steps_per_launch_max": args.c3_chunk, "seconds": seconds,
+                        "track_steps": int(total), "track_steps_per_s": rate,
+                        "field_sums_per_step": 12, "epi_per_s": rate * 12 * sph.n,
+                        "status_histogram": hist,
+                        "steps_per_track": {"min": int(steps.min()), "median": float(np.median(steps)),
+                                            "max": int(steps.max())},
+                        "slot_occupancy": rate / full_rate, "full_slot_rate_track_steps_per_s": full_rate,
+                        "clocks": clk.summary()}}), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -380,7 +488,16 @@ def main():
     ap.add_argument("--profile-axisym", action="store_true",
                     help="profiling case for ncu: axisymmetric coax (4,416 conic sections and rings), field and "
                          "potential at 10,000 gap points, two launches; prints points/s")
+    ap.add_argument("--tracking-c3", action="store_true",
+                    help="configuration 3 as configured: 65,536 electrons to the end of every track (hit or "
+                         "10,000 steps) in launches of --c3-chunk steps; prints one JSON line (several minutes)")
+    ap.add_argument("--c3-chunk", type=int, default=500)
+    ap.add_argument("--c3-tracks", type=int, default=65536)
+    ap.add_argument("--c3-precision", default="mixed", choices=["mixed", "fp64"])
     args = ap.parse_args()
+    if args.tracking_c3:
+        tracking_c3(args)
+        return
     if args.profile_axisym:
         profile_axisym()
         return
@@ -416,18 +533,28 @@ def main():
     r = run_native(args, rank, world, dist)
 
     cpu = None
+    acc_ref = None
     if rank == 0 and world == 1 and not args.quick:
-        workers = os.cpu_count() or 1
-        rate, sample = cpu_reference_rate(r["mesh"], r["sigma"], r["P"], workers)
+        physical, logical = host_cores()
+        workers = physical
+        rate, sample, ref_pts, ref_vals = cpu_reference_rate(r["mesh"], r["sigma"], r["P"], workers)
         if rate is not None:
-            cpu = {"value": rate, "unit": "points/s", "cores": workers, "kind": "reference", "sample": sample}
+            cpu = {"value": rate, "unit": "points/s", "cores": workers, "kind": "reference", "sample": sample,
+                   "host": {"physical_cores": physical, "logical_cpus": logical,
+                            "processes": f"{workers} (one per physical core)"}}
+            # the GPU's field at the points the reference evaluated, against the reference's values
+            acc_ref = {"points": int(len(ref_pts)), "reference": "oracle/_ref (KIntegratingFieldSolver, FP64)"}
+            for prec, name in ((0, "fp64"), (1, "mixed")):
+                acc_ref[name] = accuracy_vs(r["field_at"](ref_pts, prec), ref_vals)
+            acc_ref["bound_met_1e-9"] = bool(max(acc_ref["mixed"]["max_err_E_over_max_E"],
+                                                 acc_ref["mixed"]["max_err_phi_over_max_phi"]) <= 1e-9)
             # the single-core figure beside it (one process, a ~5 s sample)
-            rate1, sample1 = cpu_reference_rate(r["mesh"], r["sigma"], r["P"], 1, seconds_target=5.0)
+            rate1, sample1, _, _ = cpu_reference_rate(r["mesh"], r["sigma"], r["P"], 1, seconds_target=5.0)
             cpu["one_core"] = {"value": rate1, "sample": sample1}
             if r["axisym"] is not None:
                 # the axisymmetric model's field on the reference CPU code, one core
                 am, ax_sigma, ax_pts = r["axisym"]
-                rate_ax, sample_ax = cpu_reference_rate(am, ax_sigma, ax_pts, 1, seconds_target=4.0)
+                rate_ax, sample_ax, _, _ = cpu_reference_rate(am, ax_sigma, ax_pts, 1, seconds_target=4.0)
                 cpu["axisym_conic_coax_one_core"] = {"value": rate_ax, "unit": "points/s",
                                                      "sample": sample_ax.replace("gap points", "axisymmetric gap points")}
         else:
@@ -453,10 +580,7 @@ def main():
             "vs_baseline": None,
             "dtype": "f64 (mixed form: FP32-class hardware rsqrt estimate + FP64 Newton step per cubature node; FP64 elsewhere)",
             "data": "synthetic (seeded coax mesh and gap points)",
-            "config": {"workload": "coax: 40,000 rectangles + 4,000 cap triangles, 1,000,000 gap points per GPU, "
-                                   "GMRES to 1e-10", "elements": 44000, "points_per_gpu": N_POINTS,
-                       "parallelism": f"replicated geometry, points sharded over {world} GPU(s)",
-                       "l2": "inputs re-read every step; 24 MB points + 11 MB elements, compute-bound kernel"},
+            "config": workload_config(world),
             "e2e": {"value": pts / r["e2e_s"], "unit": "points/s",
                     "h2d_bytes_per_step": N_POINTS * 24, "d2h_bytes_per_step": N_POINTS * 32},
             "gpu_launches": r["launches"],
@@ -472,20 +596,53 @@ def main():
                            "speedup_mixed_over_plain": value / fp64_value},
             "accuracy_mixed_vs_fp64": {"max_rel_err_E_per_point": r["err_E"],
                                        "max_abs_err_phi_over_max_phi": r["err_phi"]},
-            "gmres": {"plain_fp64_matrix_free_s": r["st_plain"]["seconds"],
-                      "plain_iterations": r["st_plain"]["iterations"],
-                      "mixed_assembled_s": r["st_asm"]["seconds"],
-                      "mixed_assembled_repeat_s": r["st_asm"].get("repeat_seconds"),
-                      "mixed_assembled_iterations": r["st_asm"]["iterations"],
-                      "mixed_assembled_rel_residual": r["st_asm"]["rel_residual"],
-                      "speedup": r["st_plain"]["seconds"] / r["st_asm"]["seconds"],
-                      "sigma_rel_diff": r["sigma_diff"]},
+            "gmres": gmres_summary(r),
+            "target_10x_met": targets(value, fp64_value, r),
+            "accuracy_vs_reference": acc_ref,
             "fp32_fma_peak_tflops": r["fp32_peak"],
             "clocks": r["clocks"],
             "cpu_baseline": cpu,
         }
         line.update(r["extra"])
         print(json.dumps(line))
+
+
+def gmres_summary(r):
+    p, a = r["st_plain"], r["st_asm"]
+    a64 = a.get("fp64_assembled", {})
+    out = {"plain_fp64_matrix_free_s": p["seconds"], "plain_iterations": p["iterations"],
+           "mixed_assembled_s": a["seconds"], "mixed_assembled_repeat_s": a.get("repeat_seconds"),
+           "mixed_assembled_iterations": a["iterations"], "mixed_assembled_rel_residual": a["rel_residual"],
+           "fp64_assembled_s": a64.get("seconds"), "fp64_assembled_repeat_s": a64.get("repeat_seconds"),
+           "fp64_assembled_iterations": a64.get("iterations"), "sigma_rel_diff": r["sigma_diff"],
+           "notes": "mixed_assembled_s includes allocating and assembling the operator (FP64 + FP32 copy); "
+                    "the *_repeat_s solves find it in place. fp64_assembled is plain GMRES on the same FP64 "
+                    "operator: repeat vs repeat isolates precision, plain_fp64_matrix_free vs fp64_assembled "
+                    "isolates assembly"}
+    if a.get("repeat_seconds") and a64.get("repeat_seconds"):
+        out["speedup_precision_only"] = a64["repeat_seconds"] / a["repeat_seconds"]
+        out["speedup_assembly_only"] = p["seconds"] / a64["repeat_seconds"]
+    if a["seconds"] == a["seconds"] and a["seconds"] > 0:
+        out["speedup_mixed_first_solve_over_plain_matrix_free"] = p["seconds"] / a["seconds"]
+    return out
+
+
+def targets(value, fp64_value, r):
+    """the north-star target (mixed precision >= 10x the plain FP64 GPU form at <= 1e-9 error),
+    each comparison like for like"""
+    g = gmres_summary(r)
+    field = value / fp64_value
+    out = {"field_mixed_over_fp64_same_kernel": field, "field_met": field >= 10.0,
+           "gmres_precision_only": g.get("speedup_precision_only"),
+           "gmres_precision_only_met": bool((g.get("speedup_precision_only") or 0) >= 10.0),
+           "gmres_mixed_assembled_first_solve_over_plain_matrix_free":
+               g.get("speedup_mixed_first_solve_over_plain_matrix_free"),
+           "gmres_end_to_end_met": bool((g.get("speedup_mixed_first_solve_over_plain_matrix_free") or 0) >= 10.0),
+           "notes": "field: same direct-sum kernel in both forms (FP64 vs Newton-refined FP32-class rsqrt per "
+                    "node); the FP64 pipe is half the FP32 rate on B200, so precision alone cannot give 10x. "
+                    "gmres_end_to_end: the mixed solve on the assembled operator, assembly included, against "
+                    "plain FP64 matrix-free GMRES (the reference algorithm)"}
+    return out
 
 
 def run_reference(args):
@@ -502,13 +659,14 @@ def run_reference(args):
     # charge densities from the reference's own solver would take hours at 44,000 elements
     # (N^2 matrix entries per GMRES iteration on the CPU); the reference field sum is timed
     # with a fixed smooth density instead -- the direct sum's cost does not depend on sigma
-    sigma = np.where(mesh.value < -1.0, -1e-8, 1e-8)
-    workers = os.cpu_count() or 1
+    sigma = G.coax_density(mesh)
+    physical, logical = host_cores()
+    workers = physical
     rates = []
     for _ in range(max(1, args.warmup // 3)):
         cpu_reference_rate(mesh, sigma, P, workers, seconds_target=2.0)
     for _ in range(args.steps):
-        rate, sample = cpu_reference_rate(mesh, sigma, P, workers, seconds_target=8.0)
+        rate, sample, _, _ = cpu_reference_rate(mesh, sigma, P, workers, seconds_target=8.0)
         rates.append(rate)
     v = float(np.median(rates))
     print(json.dumps({
@@ -518,9 +676,10 @@ def run_reference(args):
         "ms_per_step": N_POINTS / v * 1e3,  # one step = the 1,000,000 points at the sampled rate
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded coax mesh and gap points)",
-        "config": {"workload": "coax: 40,000 rectangles + 4,000 cap triangles, 1,000,000 gap points per GPU, "
-                               "GMRES to 1e-10", "elements": 44000, "points_per_gpu": N_POINTS},
-        "cpu_baseline": {"value": v, "unit": "points/s", "cores": workers, "kind": "reference", "sample": sample},
+        "config": workload_config(1),
+        "cpu_baseline": {"value": v, "unit": "points/s", "cores": workers, "kind": "reference", "sample": sample,
+                         "host": {"physical_cores": physical, "logical_cpus": logical,
+                                  "processes": f"{workers} (one per physical core)"}},
         "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 

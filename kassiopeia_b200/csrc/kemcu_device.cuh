@@ -620,19 +620,16 @@ template<bool POT, bool FIELD> __device__ __noinline__ Out4 line_analytic(const 
 // MIXED selects the Newton-refined hardware reciprocal square root for the cubature bands;
 // everything else is the same FP64 code. Triangles and rectangles have separate unrolled
 // cubature code (the element type is uniform across a warp, which evaluates one element).
-template<bool MIXED, bool POT, bool FIELD> __device__ __forceinline__ Out4 epi(const double* e, V3 P)
+//
+// epi_far: a pair in a quadrature band (band_of(e, P, d, r2) returned band >= 1, with its d and
+// r2); no analytic near-field code, so callers that route the analytic pairs elsewhere carry
+// none of its registers or calls.
+template<bool MIXED, bool POT, bool FIELD>
+__device__ __forceinline__ Out4 epi_far(const double* e, V3 P, V3 d, double r2, int band)
 {
-    V3 d;
-    double r2;
-    const int band = band_of(e, P, d, r2);
     const int type = (int) e[rType];
-    if (type == kLineSegment) {
-        if (band == 0)
-            return line_analytic<POT, FIELD>(e, P);
+    if (type == kLineSegment)
         return band == 1 ? line_gauss<POT, FIELD>(e, P, 2, 8) : line_gauss<POT, FIELD>(e, P, 0, 2);
-    }
-    if (band == 0)
-        return type == kTriangle ? rwg64<3, POT, FIELD>(e, P) : rwg64<4, POT, FIELD>(e, P);
     if (type == kTriangle) {
         if (band == 1)
             return cubq<33, kTri33, POT, FIELD, MIXED>(e, d, r2);
@@ -641,6 +638,20 @@ template<bool MIXED, bool POT, bool FIELD> __device__ __forceinline__ Out4 epi(c
     if (band == 1)
         return cubq_pairs<16, kPair33, 1, POT, FIELD, MIXED>(e, d, r2);
     return band == 2 ? cubq_pairs<6, kPair12, -1, POT, FIELD, MIXED>(e, d, r2) : cubq_pairs<3, kPair7, 0, POT, FIELD, MIXED>(e, d, r2);
+}
+
+template<bool MIXED, bool POT, bool FIELD> __device__ __forceinline__ Out4 epi(const double* e, V3 P)
+{
+    V3 d;
+    double r2;
+    const int band = band_of(e, P, d, r2);
+    if (band == 0) {
+        const int type = (int) e[rType];
+        if (type == kLineSegment)
+            return line_analytic<POT, FIELD>(e, P);
+        return type == kTriangle ? rwg64<3, POT, FIELD>(e, P) : rwg64<4, POT, FIELD>(e, P);
+    }
+    return epi_far<MIXED, POT, FIELD>(e, P, d, r2, band);
 }
 
 }  // namespace kemcu

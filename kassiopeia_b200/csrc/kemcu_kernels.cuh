@@ -369,6 +369,17 @@ template<bool MIXED> __device__ __forceinline__ double entry(const double* e, co
     return t.diag;
 }
 
+// an entry whose pair is in a quadrature band (band_of returned band >= 1 with d, r2): the same
+// value as entry<MIXED>, without the analytic near-field code (a Neumann self term is band 0)
+template<bool MIXED>
+__device__ __forceinline__ double entry_far(const double* e, const TargetRec& t, V3 C, V3 d, double r2, int band)
+{
+    if (t.neumann == 0.)
+        return epi_far<MIXED, true, false>(e, C, d, r2, band).phi;
+    const Out4 r = epi_far<MIXED, false, true>(e, C, d, r2, band);
+    return r.ex * t.normal[0] + r.ey * t.normal[1] + r.ez * t.normal[2];
+}
+
 // one entry A(i, j) (kemcu_matrix_element), the FP64 form the matvec uses
 __global__ void entry_kernel(const double* __restrict__ rec, const TargetRec* __restrict__ tgt, int i, int j,
                              double* __restrict__ a)

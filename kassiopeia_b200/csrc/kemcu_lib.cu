@@ -64,6 +64,10 @@ struct kemcu_ctx
     // assembled operator (column-major)
     double* d_a64 = nullptr;
     float* d_a32 = nullptr;
+    // near-field list of the operator's columns (matrix-free Robin Hood), built on first use
+    long long* d_near_ptr = nullptr;
+    int* d_near_row = nullptr;
+    double* d_near_val = nullptr;
     // grow-only scratch
     DevBuf scratch[9];
     unsigned* d_counter = nullptr;
@@ -907,6 +911,9 @@ int kemcu_destroy(kemcu_ctx* ctx)
         cudaFree(ctx->d_sigma);
         cudaFree(ctx->d_a64);
         cudaFree(ctx->d_a32);
+        cudaFree(ctx->d_near_ptr);
+        cudaFree(ctx->d_near_row);
+        cudaFree(ctx->d_near_val);
         cudaFree(ctx->d_counter);
         cudaFree(ctx->d_flag);
         cudaEventDestroy(ctx->ev0);
@@ -969,11 +976,17 @@ int kemcu_set_geometry(kemcu_ctx* ctx, size_t n, const int32_t* shape, const int
     cudaFree(ctx->d_sigma);
     cudaFree(ctx->d_a64);
     cudaFree(ctx->d_a32);
+    cudaFree(ctx->d_near_ptr);
+    cudaFree(ctx->d_near_row);
+    cudaFree(ctx->d_near_val);
     ctx->d_rec = nullptr;
     ctx->d_tgt = nullptr;
     ctx->d_sigma = nullptr;
     ctx->d_a64 = nullptr;
     ctx->d_a32 = nullptr;
+    ctx->d_near_ptr = nullptr;
+    ctx->d_near_row = nullptr;
+    ctx->d_near_val = nullptr;
     ctx->have_sigma = false;
     ctx->n = 0;
     ctx->h_rec.assign(n * rRecSize, 0.);
@@ -1110,7 +1123,7 @@ int kemcu_field_dev_noalloc(kemcu_ctx* ctx, const double* dP, size_t n, double* 
                                       KEMCU_NOALLOC_SCRATCH_BYTES / sizeof(double))))
             return rc;
         t.stop();
-        return KEMCU_OK;
+        return check_finite(ctx, dout4, n * 4, "field result");
     }
     const size_t cap = KEMCU_NOALLOC_SCRATCH_BYTES / sizeof(double);
     const int split = (int) std::min((size_t) grid_split(ctx, n, ctx->n), std::max((size_t) 1, cap / (4 * n)));
@@ -1236,7 +1249,7 @@ int kemcu_gmres(kemcu_ctx* ctx, const double* b, double* x, int n_rhs, double re
     if (rc)
         return rc;
     if (!x || n_rhs < 1 || n_rhs > kMaxRhs || (b == nullptr && n_rhs != 1) || !(rel_tol > 0.) || max_iter < 1 ||
-        mode < 0 || mode > 2)
+        mode < 0 || mode > KEMCU_SOLVE_ASSEMBLED_FP64)
         return fail(ctx, KEMCU_EINVAL, "invalid gmres arguments");
     KC(cudaSetDevice(ctx->device));
     if ((rc = clear_pipe_flag(ctx)))
@@ -1262,8 +1275,14 @@ int kemcu_gmres(kemcu_ctx* ctx, const double* b, double* x, int n_rhs, double re
     auto t0 = std::chrono::steady_clock::now();
     int iters = 0, fp64 = 0, low = 0;
     double est = 0., rel = 0.;
-    if (mode == KEMCU_SOLVE_PLAIN) {
-        if ((rc = gmres_core(ctx, kFree64, d_b, d_x, n_rhs, rel_tol, max_iter, iters, est, fp64)))
+    if (mode == KEMCU_SOLVE_PLAIN || mode == KEMCU_SOLVE_ASSEMBLED_FP64) {
+        int op = kFree64;
+        if (mode == KEMCU_SOLVE_ASSEMBLED_FP64) {
+            if ((rc = assemble(ctx, false)))
+                return rc;
+            op = kDense64;
+        }
+        if ((rc = gmres_core(ctx, op, d_b, d_x, n_rhs, rel_tol, max_iter, iters, est, fp64)))
             return rc;
         st.outer = 1;
         rel = est;
