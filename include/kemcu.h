@@ -82,6 +82,9 @@ typedef struct {
     double one_over_four_pi_eps0;  /* KEMConstants::OneOverFourPiEps0 (KEMConstants.cc:12) */
     double eps0;                   /* KEMConstants::Eps0 (KEMConstants.cc:11) */
     size_t assembled_budget_bytes; /* device bytes an assembled operator may take; 0 = 70% of free */
+    int autotune;                  /* nonzero (default): the first field-and-potential calls of each
+                                      precision and size class try the direct-sum kernel's launch
+                                      shapes in turn and keep the fastest (kemcu_tune_field) */
 } kemcu_config;
 
 typedef struct {
@@ -156,6 +159,23 @@ int kemcu_field_dev(kemcu_ctx* ctx, const double* dP, size_t n, double* dout4, i
 #define KEMCU_NOALLOC_SCRATCH_BYTES (8u << 20)
 #define KEMCU_NOALLOC_MAX_POINTS (KEMCU_NOALLOC_SCRATCH_BYTES / 32u)
 int kemcu_field_dev_noalloc(kemcu_ctx* ctx, const double* dP, size_t n, double* dout4, int precision, int what);
+
+/* ---- autotuner of the direct sum's launch shape (no counterpart in the reference: the OpenCL
+        plugin fixes its work-group size at build time, KOpenCLElectrostaticIntegratingFieldSolver.hh)
+   The direct-sum kernel exists in kemcu_field_variant_count() launch shapes (resident CTAs per SM
+   its registers are bounded for, element-ring stages: kemcu_field_variant_info); all compute the
+   same operations in the same order, so every shape returns the same bits. Per context, precision
+   and size class (the bit length of the point count) the library keeps the fastest shape: with
+   kemcu_config.autotune set, the first field-and-potential calls of a class each run one shape
+   (timed with CUDA events) until all have run; kemcu_tune_field times every shape at once on the
+   caller's device points dP (n x 3; dout4 n x 4 receives the field) and records the choice, with
+   the K1 time of each shape in ms (kemcu_field_variant_count() values) when ms is not NULL.
+   kemcu_field_variant gives the shape chosen for n points (-1: none yet). ---- */
+int kemcu_tune_field(kemcu_ctx* ctx, const double* dP, size_t n, double* dout4, int precision, int* variant,
+                     float* ms);
+int kemcu_field_variant(const kemcu_ctx* ctx, size_t n, int precision, int* variant);
+int kemcu_field_variant_info(int variant, int* min_blocks, int* ring_stages);
+int kemcu_field_variant_count(void);
 
 /* ---- boundary-integral matrix (KBoundaryIntegralMatrix, KBoundaryIntegralMatrix.hh:16-99) ---- */
 /* single entry A(i, j) = BoundaryIntegral(source j, target i) (KBoundaryIntegralMatrix.hh:31-55) */

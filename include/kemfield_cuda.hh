@@ -7,7 +7,16 @@
 //                                KOpenCLSurfaceContainer (KOpenCLSurfaceContainer.cc:10-266)
 //   KCUDAIntegratingFieldSolver  Potential / ElectricField / ElectricFieldAndPotential of
 //                                KIntegratingFieldSolver (KElectrostaticIntegratingFieldSolver.hh:261-339),
-//                                plus a batched ElectricFieldAndPotential over many points
+//                                plus a batched ElectricFieldAndPotential over many points; it is
+//                                KIntegratingFieldSolver<Integrator, ElectrostaticCUDA>, the
+//                                specialisation for the ElectrostaticCUDA Kind, as the OpenCL
+//                                plugin specialises ElectrostaticOpenCL
+//                                (KOpenCLElectrostaticIntegratingFieldSolver.hh:20)
+//   KCUDAElectricFieldSolver     a KElectricFieldSolver (KElectricFieldSolver.hh:19-77), the
+//                                object KElectrostaticBoundaryField::SetFieldSolver takes
+//                                (KElectrostaticBoundaryField.cc:39-42) beside
+//                                KIntegratingElectrostaticFieldSolver; Kassiopeia's
+//                                KSElectricKEMField then evaluates its fields on the GPU
 //   KCUDABoundaryIntegralMatrix  a KSquareMatrix whose virtual Multiply (KMatrix.hh:87-99) and
 //                                operator()(i, j) (KBoundaryIntegralMatrix.hh:31-55) run on the GPU
 //   KCUDAChargeDensitySolver     the whole GMRES charge-density solve on the device
@@ -22,14 +31,17 @@
 #pragma once
 
 #include "KChargeDensitySolver.hh"
+#include "KElectricFieldSolver.hh"
 #include "KElectrostaticBasis.hh"
 #include "KEMConstants.hh"
 #include "KEMSimpleException.hh"
+#include "KIntegratingFieldSolverTemplate.hh"
 #include "KSquareMatrix.hh"
 #include "KSurfaceContainer.hh"
 #include "KSurfaceTypes.hh"
 #include "kemcu.h"
 
+#include <memory>
 #include <string>
 #include <utility>
 #include <vector>
@@ -37,7 +49,27 @@
 namespace KEMField
 {
 
-class ElectrostaticCUDA;  // backend Kind tag, next to ElectrostaticSingleThread / ElectrostaticOpenCL
+// backend Kind tag, next to ElectrostaticSingleThread (KElectrostaticBoundaryIntegrator.hh:44) and
+// ElectrostaticOpenCL (KOpenCLElectrostaticBoundaryIntegrator.hh:24)
+class ElectrostaticCUDA;
+
+// The integrator of the CUDA Kind: the device evaluates the reference's numeric policy
+// (KEBIFactory::MakeNumeric: cubature bands, RWG near field, analytic wires); what is chosen here
+// is only the arithmetic of the cubature nodes (KEMCU_FP64 or KEMCU_MIXED, kemcu_precision).
+class KCUDAElectrostaticBoundaryIntegrator
+{
+  public:
+    using Basis = KElectrostaticBasis;
+    using Kind = ElectrostaticCUDA;
+    explicit KCUDAElectrostaticBoundaryIntegrator(int precision = KEMCU_FP64) : fPrecision(precision) {}
+    int Precision() const
+    {
+        return fPrecision;
+    }
+
+  private:
+    int fPrecision;
+};
 
 inline void KCUDACheck(kemcu_ctx* ctx, int rc)
 {
@@ -213,6 +245,107 @@ class KCUDAIntegratingFieldSolver
     int fPrecision;
 };
 
+// KIntegratingFieldSolver<KCUDAElectrostaticBoundaryIntegrator> resolves here through the
+// integrator's Kind, as KIntegratingFieldSolver<KOpenCLElectrostaticBoundaryIntegrator> does for
+// OpenCL (KIntegratingElectrostaticFieldSolver.cc:44-69)
+template<class Integrator>
+class KIntegratingFieldSolver<Integrator, ElectrostaticCUDA> : public KCUDAIntegratingFieldSolver
+{
+  public:
+    KIntegratingFieldSolver(KCUDASurfaceContainer& container, const Integrator& integrator) :
+        KCUDAIntegratingFieldSolver(container, integrator.Precision())
+    {}
+};
+
+// The field solver KElectrostaticBoundaryField holds (SetFieldSolver). Initialize, called by the
+// boundary field after its charge-density solver has written sigma into every
+// KElectrostaticBasis (KElectrostaticBoundaryField.cc:75-93), flattens the container onto the
+// device with those charge densities; every field call then runs on the GPU. Deinitialize
+// releases the device context.
+class KCUDAElectricFieldSolver : public KElectricFieldSolver
+{
+  public:
+    explicit KCUDAElectricFieldSolver(int precision = KEMCU_FP64, int device = 0) :
+        fPrecision(precision),
+        fDevice(device)
+    {}
+    // the arithmetic of the cubature nodes: KEMCU_FP64 (default) or KEMCU_MIXED
+    void SetPrecision(int precision)
+    {
+        fPrecision = precision;
+    }
+    void UseMixedPrecision(bool choice)
+    {
+        fPrecision = choice ? KEMCU_MIXED : KEMCU_FP64;
+    }
+    void SetDevice(int device)
+    {
+        fDevice = device;
+    }
+    // batched extension: n points P (x, y, z each), out n x 4 (Ex, Ey, Ez, phi); one device call
+    void ElectricFieldAndPotential(const double* P, size_t n, double* out) const
+    {
+        Solver().ElectricFieldAndPotential(P, n, out);
+    }
+    void ElectricFieldAndPotential(const std::vector<KPosition>& P, std::vector<KFieldVector>& E,
+                                   std::vector<double>& phi) const
+    {
+        std::vector<double> p(3 * P.size()), o(4 * P.size());
+        for (size_t i = 0; i < P.size(); i++)
+            for (int c = 0; c < 3; c++)
+                p[3 * i + c] = P[i][c];
+        Solver().ElectricFieldAndPotential(p.data(), P.size(), o.data());
+        E.resize(P.size());
+        phi.resize(P.size());
+        for (size_t i = 0; i < P.size(); i++) {
+            E[i] = KFieldVector(o[4 * i], o[4 * i + 1], o[4 * i + 2]);
+            phi[i] = o[4 * i + 3];
+        }
+    }
+    KCUDASurfaceContainer* DeviceContainer() const
+    {
+        return fContainer.get();
+    }
+
+  private:
+    using Solver_t = KIntegratingFieldSolver<KCUDAElectrostaticBoundaryIntegrator>;
+    const Solver_t& Solver() const
+    {
+        if (!fSolver)
+            throw KEMSimpleException("kemcu: KCUDAElectricFieldSolver used before Initialize");
+        return *fSolver;
+    }
+    void InitializeCore(KSurfaceContainer& container) override
+    {
+        fContainer = std::make_unique<KCUDASurfaceContainer>(container, fDevice);
+        fContainer->WriteBasisData();
+        fIntegrator = KCUDAElectrostaticBoundaryIntegrator(fPrecision);
+        fSolver = std::make_unique<Solver_t>(*fContainer, fIntegrator);
+    }
+    void DeinitializeCore() override
+    {
+        fSolver.reset();
+        fContainer.reset();
+    }
+    double PotentialCore(const KPosition& P) const override
+    {
+        return Solver().Potential(P);
+    }
+    KFieldVector ElectricFieldCore(const KPosition& P) const override
+    {
+        return Solver().ElectricField(P);
+    }
+    std::pair<KFieldVector, double> ElectricFieldAndPotentialCore(const KPosition& P) const override
+    {
+        return Solver().ElectricFieldAndPotential(P);
+    }
+
+    int fPrecision, fDevice;
+    KCUDAElectrostaticBoundaryIntegrator fIntegrator;
+    std::unique_ptr<KCUDASurfaceContainer> fContainer;
+    std::unique_ptr<Solver_t> fSolver;
+};
+
 class KCUDABoundaryIntegralMatrix : public KSquareMatrix<double>
 {
   public:
@@ -324,7 +457,7 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
     {
         fMode = mode;
     }
-    // XML form: "plain", "mixed" or "assembled" (kemcu_solve_mode)
+    // XML form: "plain", "mixed", "assembled" or "assembled_fp64" (kemcu_solve_mode)
     void SetModeName(const std::string& name)
     {
         if (name == "plain")
@@ -333,8 +466,11 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
             fMode = KEMCU_SOLVE_MIXED;
         else if (name == "assembled")
             fMode = KEMCU_SOLVE_ASSEMBLED;
+        else if (name == "assembled_fp64")
+            fMode = KEMCU_SOLVE_ASSEMBLED_FP64;
         else
-            throw KEMSimpleException("kemcu: unknown solve mode <" + name + "> (plain, mixed, assembled)");
+            throw KEMSimpleException("kemcu: unknown solve mode <" + name +
+                                     "> (plain, mixed, assembled, assembled_fp64)");
     }
     // solves A sigma = b for the boundary values and writes sigma into the container
     kemcu_solve_stats Solve(KCUDASurfaceContainer& container) const

@@ -44,7 +44,7 @@ def _i(a):
 class CUDAElectrostaticContext:
     """One device context; not re-entrant (use one per thread)."""
 
-    def __init__(self, device: int = 0, assembled_budget_bytes: int = 0):
+    def __init__(self, device: int = 0, assembled_budget_bytes: int = 0, autotune: bool = True):
         L = N.lib()
         cfg = N.Config()
         L.kemcu_default_config(C.byref(cfg))
@@ -52,6 +52,7 @@ class CUDAElectrostaticContext:
         cfg.one_over_four_pi_eps0 = ONE_OVER_FOUR_PI_EPS0
         cfg.eps0 = EPS0
         cfg.assembled_budget_bytes = assembled_budget_bytes
+        cfg.autotune = int(bool(autotune))
         h = C.c_void_p()
         rc = L.kemcu_create(C.byref(h), C.byref(cfg))
         self._h = h
@@ -131,6 +132,31 @@ class CUDAElectrostaticContext:
         """Device-pointer variant (e.g. torch tensors' data_ptr())."""
         self._check(N.lib().kemcu_field_dev(self._h, C.c_void_p(d_points_ptr), n, C.c_void_p(d_out_ptr), precision,
                                             what))
+
+    # -- autotuner of the direct sum's launch shape
+    def TuneField(self, d_points_ptr: int, n: int, d_out_ptr: int, precision=FP64):
+        """Time every launch shape of the direct-sum kernel on these device points (the field lands
+        in d_out); returns (chosen shape, [K1 milliseconds per shape])."""
+        L = N.lib()
+        nv = L.kemcu_field_variant_count()
+        ms = (C.c_float * nv)()
+        v = C.c_int(-1)
+        self._check(L.kemcu_tune_field(self._h, C.c_void_p(d_points_ptr), n, C.c_void_p(d_out_ptr), precision,
+                                       C.byref(v), ms))
+        return v.value, [float(x) for x in ms]
+
+    def FieldVariant(self, n: int, precision=FP64) -> int:
+        """The launch shape the autotuner chose for n points (-1: none yet)."""
+        v = C.c_int(-1)
+        self._check(N.lib().kemcu_field_variant(self._h, n, precision, C.byref(v)))
+        return v.value
+
+    @staticmethod
+    def FieldVariantInfo(v: int) -> dict:
+        mb, rs = C.c_int(), C.c_int()
+        if N.lib().kemcu_field_variant_info(v, C.byref(mb), C.byref(rs)) != N.OK:
+            raise KemcuError(N.EINVAL, f"no launch shape {v}")
+        return {"variant": v, "ctas_per_sm": mb.value, "ring_stages": rs.value}
 
     # -- matrix
     def MatrixElement(self, i, j):

@@ -32,7 +32,7 @@ class KemcuError(RuntimeError):
 
 class Config(C.Structure):
     _fields_ = [("device", C.c_int), ("one_over_four_pi_eps0", C.c_double), ("eps0", C.c_double),
-                ("assembled_budget_bytes", C.c_size_t)]
+                ("assembled_budget_bytes", C.c_size_t), ("autotune", C.c_int)]
 
 
 class SolveStats(C.Structure):
@@ -127,5 +127,10 @@ def lib():
     L.kemcu_band_histogram.argtypes = [vp, _dp, C.c_size_t, C.POINTER(C.c_longlong)]
     L.kemcu_fma_peak.argtypes = [vp, _dp, _dp]
     L.kemcu_selftest_timeout.argtypes = [vp, C.c_int]
+    L.kemcu_tune_field.argtypes = [vp, C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.POINTER(C.c_int),
+                                   C.POINTER(C.c_float)]
+    L.kemcu_field_variant.argtypes = [vp, C.c_size_t, C.c_int, C.POINTER(C.c_int)]
+    L.kemcu_field_variant_info.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.kemcu_field_variant_count.argtypes = []
     _lib = L
     return L

@@ -270,21 +270,28 @@ template<int SIDE, int NP = kPipe, bool CYCLIC = false> struct ElementRing
 };
 
 // K1: field and/or potential at points. out layout per point: (Ex, Ey, Ez, phi).
+// The analytic near-field pairs (band 0: RWG triangles and rectangles, analytic wires) are
+// evaluated in place through a non-inlined call: a design with a call-free quadrature kernel and
+// a second kernel for the analytic pairs was built and measured slower (the near pass ran alone,
+// latency-bound, where here its latency hides behind other warps' quadrature work).
 // nsplit == gridDim.y; partial != nullptr when nsplit > 1 (then out is untouched).
 // flag |= 2 if a pipeline wait timed out (the outputs are then incomplete).
-template<bool MIXED, bool POT, bool FIELD>
-__global__ void __launch_bounds__(kThreads, kMinBlocks) field_kernel(const double* __restrict__ rec, const double* __restrict__ sigma,
-                                                         int n_elem, const double* __restrict__ pts, int n_pts,
-                                                         double* __restrict__ out, double* __restrict__ partial,
-                                                         int* __restrict__ flag)
+// MINB (resident CTAs per SM the registers are bounded for) and NP (ring stages) are the shapes
+// the autotuner chooses between (field_variants); neither changes an operation or its order, so
+// every variant gives the same result bit for bit.
+template<bool MIXED, bool POT, bool FIELD, int MINB = kMinBlocks, int NP = kPipe>
+__global__ void __launch_bounds__(kThreads, MINB) field_kernel(const double* __restrict__ rec, const double* __restrict__ sigma,
+                                                               int n_elem, const double* __restrict__ pts, int n_pts,
+                                                               double* __restrict__ out, double* __restrict__ partial,
+                                                               int* __restrict__ flag)
 {
-    __shared__ __align__(128) RingStorage<1> S;
+    __shared__ __align__(128) RingStorage<1, NP> S;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = p < n_pts;
     V3 P = v3(0., 0., 0.);
     if (active)
         P = v3(pts[3 * p], pts[3 * p + 1], pts[3 * p + 2]);
-    ElementRing<1> R(S, 0, n_elem);
+    ElementRing<1, NP> R(S, 0, n_elem);
     auto side = [&](double (*sd)[kFieldTile], int t0, int cnt, int lane) {
         if (lane < cnt)
             sd[0][lane] = sigma[t0 + lane];

@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -76,6 +77,16 @@ struct kemcu_ctx
     kemcu_iteration_callback cb = nullptr;
     void* cb_user = nullptr;
     unsigned long long launches = 0;
+    // autotuner of the direct sum (field_variants): per (precision, size class) the chosen
+    // variant, or the K1 times of the variants tried so far; a call that times a variant
+    // leaves its key and variant pending until its result is back
+    bool autotune = true;
+    std::map<int, int> tuned;
+    std::map<int, std::vector<float>> explored;
+    int force_variant = -1;
+    bool time_k1 = false;  // time the K1 launch of forced variants (kemcu_tune_field)
+    int pending_key = -1, pending_variant = -1;
+    cudaEvent_t tv0 = nullptr, tv1 = nullptr;
 };
 
 namespace
@@ -340,6 +351,134 @@ int launch_axisym_field(kemcu_ctx* ctx, const double* d_pts, size_t n, double* d
     return KEMCU_OK;
 }
 
+// Launch shapes of K1 the autotuner chooses between: (resident CTAs per SM the registers are
+// bounded for, ring stages), the build default first. They change no operation and no order of
+// summation, so every variant returns the same bits; only the field-and-potential kernels (the
+// path of field evaluation and tracking at scale) are instantiated in every shape.
+struct FieldVariant
+{
+    int min_blocks, ring_stages;
+};
+constexpr FieldVariant kFieldVariants[] = {{kMinBlocks, kPipe}, {4, 4}, {5, 3}, {4, 3}};
+constexpr int kNumFieldVariants = (int) (sizeof(kFieldVariants) / sizeof(kFieldVariants[0]));
+
+template<bool MIXED, bool POT, bool FIELD>
+void launch_k1(int variant, dim3 grid, cudaStream_t st, const double* rec, const double* sg, int ne, const double* pts,
+               int np, double* out, double* part, int* fl)
+{
+    if constexpr (POT && FIELD) {
+        switch (variant) {
+        case 1:
+            field_kernel<MIXED, POT, FIELD, 4, 4><<<grid, kThreads, 0, st>>>(rec, sg, ne, pts, np, out, part, fl);
+            return;
+        case 2:
+            field_kernel<MIXED, POT, FIELD, 5, 3><<<grid, kThreads, 0, st>>>(rec, sg, ne, pts, np, out, part, fl);
+            return;
+        case 3:
+            field_kernel<MIXED, POT, FIELD, 4, 3><<<grid, kThreads, 0, st>>>(rec, sg, ne, pts, np, out, part, fl);
+            return;
+        default:
+            break;
+        }
+    }
+    field_kernel<MIXED, POT, FIELD><<<grid, kThreads, 0, st>>>(rec, sg, ne, pts, np, out, part, fl);
+}
+
+// tuning key: precision and the size class (bit length of the point count)
+int tune_key(int precision, size_t n)
+{
+    int c = 0;
+    while ((n >> c) > 1)
+        c++;
+    return precision * 64 + c;
+}
+
+// the K1 variant of a planar field-and-potential call of n points; marks the call for timing
+// when the autotuner still explores this size class
+int choose_variant(kemcu_ctx* ctx, size_t n, int precision, int what)
+{
+    ctx->pending_key = -1;
+    if (what != KEMCU_FIELD_AND_POTENTIAL)
+        return 0;
+    if (ctx->force_variant >= 0)
+        return ctx->force_variant;
+    const int key = tune_key(precision, n);
+    auto it = ctx->tuned.find(key);
+    if (it != ctx->tuned.end())
+        return it->second;
+    if (!ctx->autotune)
+        return 0;
+    ctx->pending_key = key;
+    ctx->pending_variant = (int) ctx->explored[key].size();
+    return ctx->pending_variant;
+}
+
+// after a timed call's result is complete: record its K1 time; once every variant has run for
+// the size class, keep the fastest
+void finish_variant(kemcu_ctx* ctx)
+{
+    if (ctx->pending_key < 0)
+        return;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, ctx->tv0, ctx->tv1) == cudaSuccess) {
+        auto& t = ctx->explored[ctx->pending_key];
+        if ((int) t.size() == ctx->pending_variant)
+            t.push_back(ms);
+        if ((int) t.size() == kNumFieldVariants)
+            ctx->tuned[ctx->pending_key] = (int) (std::min_element(t.begin(), t.end()) - t.begin());
+    }
+    else
+        cudaGetLastError();
+    ctx->pending_key = -1;
+}
+
+// the planar direct sum at device points (d_out n x 4): K1, split `split` ways over the element
+// list (partial sums in `partial`, then reduced in split order)
+int launch_planar_field(kemcu_ctx* ctx, const double* d_pts, size_t n, double* d_out, int precision, int what,
+                        int split, double* partial)
+{
+    dim3 grid((unsigned) ((n + kThreads - 1) / kThreads), (unsigned) split);
+    if (int rc = clear_pipe_flag(ctx))
+        return rc;
+    const bool mixed = precision == KEMCU_MIXED;
+    const double* sg = ctx->d_sigma;
+    const int ne = (int) ctx->n, np = (int) n;
+    double* part = split > 1 ? partial : nullptr;
+    int* fl = ctx->d_flag + 1;
+    const int v = choose_variant(ctx, n, precision, what);
+    cudaStream_t st = ctx->stream;
+    const bool timed = ctx->pending_key >= 0 || ctx->time_k1;
+    if (timed)
+        KC(cudaEventRecord(ctx->tv0, st));
+    if (what == KEMCU_POTENTIAL) {
+        if (mixed)
+            launch_k1<true, true, false>(v, grid, st, ctx->d_rec, sg, ne, d_pts, np, d_out, part, fl);
+        else
+            launch_k1<false, true, false>(v, grid, st, ctx->d_rec, sg, ne, d_pts, np, d_out, part, fl);
+    }
+    else if (what == KEMCU_FIELD) {
+        if (mixed)
+            launch_k1<true, false, true>(v, grid, st, ctx->d_rec, sg, ne, d_pts, np, d_out, part, fl);
+        else
+            launch_k1<false, false, true>(v, grid, st, ctx->d_rec, sg, ne, d_pts, np, d_out, part, fl);
+    }
+    else {
+        if (mixed)
+            launch_k1<true, true, true>(v, grid, st, ctx->d_rec, sg, ne, d_pts, np, d_out, part, fl);
+        else
+            launch_k1<false, true, true>(v, grid, st, ctx->d_rec, sg, ne, d_pts, np, d_out, part, fl);
+    }
+    KCHECK_LAUNCH();
+    if (timed)
+        KC(cudaEventRecord(ctx->tv1, st));
+    if (split > 1) {
+        const size_t m = n * 4;
+        reduce_splits<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(part, split, m, d_out);
+        KCHECK_LAUNCH();
+    }
+    return KEMCU_OK;
+}
+
 // field at device points; d_out n x 4
 int launch_field(kemcu_ctx* ctx, const double* d_pts, size_t n, double* d_out, int precision, int what)
 {
@@ -354,37 +493,7 @@ int launch_field(kemcu_ctx* ctx, const double* d_pts, size_t n, double* d_out, i
             return rc;
         partial = (double*) p;
     }
-    dim3 grid((unsigned) ((n + kThreads - 1) / kThreads), (unsigned) split);
-    if (int rc = clear_pipe_flag(ctx))
-        return rc;
-    const bool mixed = precision == KEMCU_MIXED;
-    const double* sg = ctx->d_sigma;
-    const int ne = (int) ctx->n;
-    if (what == KEMCU_POTENTIAL) {
-        if (mixed)
-            field_kernel<true, true, false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial, ctx->d_flag + 1);
-        else
-            field_kernel<false, true, false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial, ctx->d_flag + 1);
-    }
-    else if (what == KEMCU_FIELD) {
-        if (mixed)
-            field_kernel<true, false, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial, ctx->d_flag + 1);
-        else
-            field_kernel<false, false, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial, ctx->d_flag + 1);
-    }
-    else {
-        if (mixed)
-            field_kernel<true, true, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial, ctx->d_flag + 1);
-        else
-            field_kernel<false, true, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, d_pts, (int) n, d_out, partial, ctx->d_flag + 1);
-    }
-    KCHECK_LAUNCH();
-    if (split > 1) {
-        const size_t m = n * 4;
-        reduce_splits<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(partial, split, m, d_out);
-        KCHECK_LAUNCH();
-    }
-    return KEMCU_OK;
+    return launch_planar_field(ctx, d_pts, n, d_out, precision, what, split, partial);
 }
 
 constexpr size_t kSortMin = 4096;  // below this the point set is evaluated in caller order
@@ -784,6 +893,7 @@ void kemcu_default_config(kemcu_config* cfg)
     cfg->one_over_four_pi_eps0 = 1. / (4. * 3.141592653589793238462643383279502884 * 8.8541878128e-12);
     cfg->eps0 = 8.8541878128e-12;
     cfg->assembled_budget_bytes = 0;
+    cfg->autotune = 1;
 }
 
 int kemcu_create(kemcu_ctx** out, const kemcu_config* cfg)
@@ -820,6 +930,9 @@ int kemcu_create(kemcu_ctx** out, const kemcu_config* cfg)
     KC(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     KC(cudaEventCreate(&ctx->ev0));
     KC(cudaEventCreate(&ctx->ev1));
+    KC(cudaEventCreate(&ctx->tv0));
+    KC(cudaEventCreate(&ctx->tv1));
+    ctx->autotune = cfg->autotune != 0;
     KC(cudaMalloc(&ctx->d_counter, 64 * sizeof(unsigned)));
     KC(cudaMemset(ctx->d_counter, 0, 64 * sizeof(unsigned)));
     // [0]: non-finite values seen; [1]: a direct-sum pipeline wait timed out
@@ -918,6 +1031,8 @@ int kemcu_destroy(kemcu_ctx* ctx)
         cudaFree(ctx->d_flag);
         cudaEventDestroy(ctx->ev0);
         cudaEventDestroy(ctx->ev1);
+        cudaEventDestroy(ctx->tv0);
+        cudaEventDestroy(ctx->tv1);
         cudaStreamDestroy(ctx->stream);
     }
     delete ctx;
@@ -1095,7 +1210,11 @@ int kemcu_field_dev(kemcu_ctx* ctx, const double* dP, size_t n, double* dout4, i
         KCHECK_LAUNCH();
     }
     t.stop();
-    return check_finite(ctx, dout4, n * 4, "field result");
+    rc = check_finite(ctx, dout4, n * 4, "field result");
+    if (rc == KEMCU_OK)
+        finish_variant(ctx);
+    ctx->pending_key = -1;
+    return rc;
 }
 
 // Allocation-free direct sum (declared in kemcu.h): the element-split partial sums go to the
@@ -1127,39 +1246,14 @@ int kemcu_field_dev_noalloc(kemcu_ctx* ctx, const double* dP, size_t n, double* 
     }
     const size_t cap = KEMCU_NOALLOC_SCRATCH_BYTES / sizeof(double);
     const int split = (int) std::min((size_t) grid_split(ctx, n, ctx->n), std::max((size_t) 1, cap / (4 * n)));
-    double* partial = split > 1 ? ctx->noalloc_scratch : nullptr;
-    dim3 grid((unsigned) ((n + kThreads - 1) / kThreads), (unsigned) split);
-    if ((rc = clear_pipe_flag(ctx)))
+    if ((rc = launch_planar_field(ctx, dP, n, dout4, precision, what, split, ctx->noalloc_scratch)))
         return rc;
-    const double* sg = ctx->d_sigma;
-    const int ne = (int) ctx->n, np = (int) n;
-    const bool mixed = precision == KEMCU_MIXED;
-    if (what == KEMCU_POTENTIAL) {
-        if (mixed)
-            field_kernel<true, true, false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial, ctx->d_flag + 1);
-        else
-            field_kernel<false, true, false><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial, ctx->d_flag + 1);
-    }
-    else if (what == KEMCU_FIELD) {
-        if (mixed)
-            field_kernel<true, false, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial, ctx->d_flag + 1);
-        else
-            field_kernel<false, false, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial, ctx->d_flag + 1);
-    }
-    else {
-        if (mixed)
-            field_kernel<true, true, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial, ctx->d_flag + 1);
-        else
-            field_kernel<false, true, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, sg, ne, dP, np, dout4, partial, ctx->d_flag + 1);
-    }
-    KCHECK_LAUNCH();
-    if (split > 1) {
-        const size_t m = n * 4;
-        reduce_splits<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(partial, split, m, dout4);
-        KCHECK_LAUNCH();
-    }
     t.stop();
-    return check_finite(ctx, dout4, n * 4, "field result");
+    rc = check_finite(ctx, dout4, n * 4, "field result");
+    if (rc == KEMCU_OK)
+        finish_variant(ctx);
+    ctx->pending_key = -1;
+    return rc;
 }
 
 int kemcu_field(kemcu_ctx* ctx, const double* P, size_t n, double* out4, int precision, int what)
@@ -1181,6 +1275,65 @@ int kemcu_field(kemcu_ctx* ctx, const double* P, size_t n, double* out4, int pre
     KC(cudaMemcpyAsync(out4, dout, n * 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     KC(cudaStreamSynchronize(ctx->stream));
     return KEMCU_OK;
+}
+
+int kemcu_tune_field(kemcu_ctx* ctx, const double* dP, size_t n, double* dout4, int precision, int* variant,
+                     float* ms)
+{
+    int rc = check_ready(ctx, true);
+    if (rc || (rc = planar_only(ctx, "the field autotuner")))
+        return rc;
+    if (!dP || !dout4 || n == 0 || (precision != KEMCU_FP64 && precision != KEMCU_MIXED))
+        return fail(ctx, KEMCU_EINVAL, "invalid tuning arguments");
+    // every variant runs the whole evaluation twice (the first warms it up); the K1 launch of the
+    // second run is timed
+    std::vector<float> t(kNumFieldVariants, 0.f);
+    ctx->time_k1 = true;
+    for (int v = 0; v < kNumFieldVariants && rc == KEMCU_OK; v++) {
+        ctx->force_variant = v;
+        for (int rep = 0; rep < 2 && rc == KEMCU_OK; rep++)
+            rc = kemcu_field_dev(ctx, dP, n, dout4, precision, KEMCU_FIELD_AND_POTENTIAL);
+        if (rc == KEMCU_OK && cudaEventElapsedTime(&t[v], ctx->tv0, ctx->tv1) != cudaSuccess)
+            rc = fail(ctx, KEMCU_ECUDA, "tuning timer failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    ctx->time_k1 = false;
+    ctx->force_variant = -1;
+    if (rc)
+        return rc;
+    const int key = tune_key(precision, n);
+    const int best = (int) (std::min_element(t.begin(), t.end()) - t.begin());
+    ctx->explored[key] = t;
+    ctx->tuned[key] = best;
+    if (variant)
+        *variant = best;
+    if (ms)
+        std::copy(t.begin(), t.end(), ms);
+    return KEMCU_OK;
+}
+
+int kemcu_field_variant(const kemcu_ctx* ctx, size_t n, int precision, int* variant)
+{
+    if (!ctx || !variant)
+        return KEMCU_EINVAL;
+    auto it = ctx->tuned.find(tune_key(precision, n));
+    *variant = it == ctx->tuned.end() ? -1 : it->second;
+    return KEMCU_OK;
+}
+
+int kemcu_field_variant_info(int variant, int* min_blocks, int* ring_stages)
+{
+    if (variant < 0 || variant >= kNumFieldVariants)
+        return KEMCU_EINVAL;
+    if (min_blocks)
+        *min_blocks = kFieldVariants[variant].min_blocks;
+    if (ring_stages)
+        *ring_stages = kFieldVariants[variant].ring_stages;
+    return KEMCU_OK;
+}
+
+int kemcu_field_variant_count(void)
+{
+    return kNumFieldVariants;
 }
 
 int kemcu_matrix_element(kemcu_ctx* ctx, size_t i, size_t j, double* a)

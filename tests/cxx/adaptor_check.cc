@@ -8,9 +8,11 @@
 #include "KBoundaryIntegralMatrix.hh"
 #include "KBoundaryIntegralSolutionVector.hh"
 #include "KBoundaryIntegralVector.hh"
+#include "KElectrostaticBoundaryField.hh"
 #include "KElectrostaticBoundaryIntegratorFactory.hh"
 #include "KEMFileInterface.hh"
 #include "KElectrostaticIntegratingFieldSolver.hh"
+#include "KIntegratingElectrostaticFieldSolver.hh"
 #include "KGeneralizedMinimalResidual.hh"
 #include "KRobinHood.hh"
 #include "KSimpleIterativeKrylovSolver.hh"
@@ -190,6 +192,72 @@ static int cache_round_trip()
     return fail;
 }
 
+// The boundary field as KEMField users build it (KElectrostaticBoundaryField.cc:29-42, 75-93),
+// with the CUDA charge-density solver and the CUDA field solver plugged in where
+// KKrylovChargeDensitySolver and KIntegratingElectrostaticFieldSolver go, against the
+// reference's CPU field solver on the same charge densities (and on the reference's own
+// mixed-precision form of the field, KEMCU_MIXED, within 1e-9). Batched calls agree with single ones.
+static int boundary_field_check()
+{
+    char tmpl[] = "/tmp/kemcu_fieldXXXXXX";
+    if (!mkdtemp(tmpl)) {
+        std::printf("boundary field: no scratch directory\n");
+        return 1;
+    }
+    const std::string dir(tmpl);
+    int fail = 0;
+    for (int precision : {KEMCU_FP64, KEMCU_MIXED}) {
+        auto container = std::make_shared<KSurfaceContainer>();
+        icosphere(2, *container);
+        // a cache directory of its own per round, so that each round solves on the device
+        const std::string sub = dir + (precision == KEMCU_FP64 ? "/fp64" : "/mixed");
+        std::filesystem::create_directories(sub);
+        KElectrostaticBoundaryField field;
+        field.SetDirectory(sub);
+        field.SetFile("field.kbd");
+        field.SetContainer(container);
+        auto cds = std::make_shared<KCUDAChargeDensitySolver>(1e-12, 300, KEMCU_SOLVE_PLAIN);
+        auto fs = std::make_shared<KCUDAElectricFieldSolver>(precision);
+        field.SetChargeDensitySolver(cds);
+        field.SetFieldSolver(fs);
+        field.Initialize();
+        KIntegratingElectrostaticFieldSolver cpu;
+        cpu.Initialize(*container);
+        std::vector<KPosition> pts;
+        double worst = 0.;
+        for (int i = 0; i < 24; i++) {
+            const double r = 1.02 + 0.09 * i, th = 0.61 * i + 0.2, ph = 1.7 * i;
+            KPosition P(r * std::sin(th) * std::cos(ph), r * std::sin(th) * std::sin(ph), r * std::cos(th));
+            pts.push_back(P);
+            const auto a = cpu.ElectricFieldAndPotential(P);
+            const auto b = field.ElectricFieldAndPotential(P, 0.);
+            const double pb = field.Potential(P, 0.);
+            const KFieldVector eb = field.ElectricField(P, 0.);
+            worst = std::max(worst, std::fabs(a.second - b.second) / std::fabs(a.second));
+            worst = std::max(worst, (a.first - b.first).Magnitude() / a.first.Magnitude());
+            worst = std::max(worst, std::fabs(a.second - pb) / std::fabs(a.second));
+            worst = std::max(worst, (a.first - eb).Magnitude() / a.first.Magnitude());
+        }
+        std::vector<KFieldVector> E;
+        std::vector<double> phi;
+        fs->ElectricFieldAndPotential(pts, E, phi);
+        double wb = 0.;
+        for (size_t i = 0; i < pts.size(); i++) {
+            const auto b = field.ElectricFieldAndPotential(pts[i], 0.);
+            wb = std::max(wb, std::fabs(phi[i] - b.second) / std::fabs(b.second));
+            wb = std::max(wb, (E[i] - b.first).Magnitude() / b.first.Magnitude());
+        }
+        const double tol = precision == KEMCU_FP64 ? 1e-12 : 1e-9;
+        std::printf("boundary field (%s, CUDA charge densities + CUDA field solver): max relative difference to the "
+                    "CPU field solver %.3e, batched vs single %.3e, %d GMRES iterations\n",
+                    precision == KEMCU_FP64 ? "FP64" : "MIXED", worst, wb, cds->LastStats().iterations);
+        fail += !(worst < tol && wb < 1e-15 && cds->LastStats().iterations > 0);
+        field.Deinitialize();
+    }
+    std::filesystem::remove_all(dir);
+    return fail;
+}
+
 int main()
 {
     KSurfaceContainer container;
@@ -273,6 +341,7 @@ int main()
 
         failures += cache_round_trip();
         failures += axisym_check();
+        failures += boundary_field_check();
     }
     catch (std::exception& e) {
         std::printf("exception: %s\n", e.what());
