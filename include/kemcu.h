@@ -220,10 +220,12 @@ int kemcu_robin_hood(kemcu_ctx* ctx, const double* b, double* x, double rel_tol,
    state: n x 8 (t, s, x, y, z, px, py, pz), updated in place; steps: n step counters
    (in/out, tracks stop at max_steps); status: n kemcu_track_status values (in/out, only
    KEMCU_TRACK_ACTIVE tracks advance). step_budget bounds the steps of this call per track
-   (<= 0: no extra bound). */
+   (<= 0: no extra bound). momentum_change (n values, in/out, may be NULL): per track, the sum over
+   its steps of |p_after - p_before|, added to the values passed in (KSStep::ContinuousMomentumChange,
+   which KSRoot sums into KSTrack, KSRootTrajectory.cxx:217-218, KSRoot.cxx:695-705). */
 int kemcu_track_rk8(kemcu_ctx* ctx, double* state, int32_t* steps, int32_t* status, size_t n, double dt,
                     int max_steps, int step_budget, double charge, double mass, const kemcu_hit_model* hit,
-                    int precision, kemcu_track_stats* stats);
+                    int precision, kemcu_track_stats* stats, double* momentum_change);
 
 /* ---- adjoint: vector-Jacobian product of the direct sum (no reference counterpart) ----
    w: n x 4 weights on (Ex, Ey, Ez, phi) at points P (n x 3); L = sum_p w_p . out_p.

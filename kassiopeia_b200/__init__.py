@@ -217,7 +217,9 @@ class CUDAElectrostaticContext:
 
     # -- tracking
     def TrackRK8(self, state, dt, max_steps, steps=None, status=None, step_budget=0, charge=None, mass=None,
-                 sphere_radius=0.0, max_radius=0.0, precision=FP64):
+                 sphere_radius=0.0, max_radius=0.0, precision=FP64, momentum_change=None):
+        """Advance the tracks; returns (state, steps, status, stats dict). momentum_change: an [n]
+        array that receives, added to its values, each track's sum of |p_after - p_before| per step."""
         from .geometry import ELECTRON_MASS, ELEMENTARY_CHARGE
         st = np.ascontiguousarray(state, np.float64).copy()
         n = st.shape[0]
@@ -227,8 +229,13 @@ class CUDAElectrostaticContext:
         ts = N.TrackStats()
         q = -ELEMENTARY_CHARGE if charge is None else charge
         m = ELECTRON_MASS if mass is None else mass
+        dpp = C.cast(None, C.POINTER(C.c_double))
+        if momentum_change is not None:
+            assert momentum_change.dtype == np.float64 and momentum_change.shape == (n,)
+            assert momentum_change.flags.c_contiguous
+            dpp = _d(momentum_change)
         self._check(N.lib().kemcu_track_rk8(self._h, _d(st), _i(steps), _i(status), n, dt, max_steps, step_budget, q, m,
-                                            C.byref(hit), precision, C.byref(ts)))
+                                            C.byref(hit), precision, C.byref(ts), dpp))
         return st, steps, status, {k: getattr(ts, k) for k, _ in N.TrackStats._fields_}
 
     # -- adjoint

@@ -119,7 +119,7 @@ def lib():
     L.kemcu_robin_hood.argtypes = [vp, _dp, _dp, C.c_double, C.c_int, C.c_longlong, C.c_int, C.POINTER(RhStats)]
     L.kemcu_set_iteration_callback.restype = None
     L.kemcu_track_rk8.argtypes = [vp, _dp, _ip, _ip, C.c_size_t, C.c_double, C.c_int, C.c_int, C.c_double,
-                                  C.c_double, C.POINTER(HitModel), C.c_int, C.POINTER(TrackStats)]
+                                  C.c_double, C.POINTER(HitModel), C.c_int, C.POINTER(TrackStats), _dp]
     L.kemcu_field_vjp.argtypes = [vp, _dp, C.c_size_t, _dp, _dp, _dp, C.c_int]
     L.kemcu_rule_nodes.argtypes = [C.c_int, _dp]
     L.kemcu_launch_count.argtypes = [vp]

@@ -83,7 +83,8 @@ inline unsigned rk8_live_stages(const double a[kStages][kStages])
 }
 
 // state: n x 8; steps, status: n; list: n_list track indices to work on; next: work counter;
-// done_steps: total steps taken (for statistics); flag |= 2 if a ring wait timed out.
+// done_steps: total steps taken (for statistics); dpsum (n, may be null): per track the sum over
+// its steps of |p_after - p_before|, accumulated; flag |= 2 if a ring wait timed out.
 // Dynamic shared memory: kStages * kTrackK * kTrackSlots doubles.
 template<bool MIXED>
 __global__ void __launch_bounds__(kTrackSlots) rk8_tracker_kernel(const double* __restrict__ rec, const double* __restrict__ sigma,
@@ -91,7 +92,8 @@ __global__ void __launch_bounds__(kTrackSlots) rk8_tracker_kernel(const double* 
                                                                   int* __restrict__ steps, int* __restrict__ status,
                                                                   const int* __restrict__ list, unsigned* __restrict__ next,
                                                                   unsigned long long* __restrict__ done_steps,
-                                                                  TrackParams prm, int* __restrict__ flag)
+                                                                  double* __restrict__ dpsum, TrackParams prm,
+                                                                  int* __restrict__ flag)
 {
     extern __shared__ __align__(16) double s_k[];  // [kStages][kTrackK][kTrackSlots]
     __shared__ __align__(128) RingStorage<1, kTrackPipe> S;
@@ -110,6 +112,7 @@ __global__ void __launch_bounds__(kTrackSlots) rk8_tracker_kernel(const double* 
 
     int track = -1, tsteps = 0;
     double y[8];
+    double dps = 0.;
     int nstep = 0;
     auto pull = [&]() {
         track = -1;
@@ -120,6 +123,7 @@ __global__ void __launch_bounds__(kTrackSlots) rk8_tracker_kernel(const double* 
             for (int c = 0; c < 8; c++)
                 y[c] = state[(size_t) track * 8 + c];
             nstep = steps[track];
+            dps = dpsum ? dpsum[track] : 0.;
         }
     };
     pull();
@@ -203,8 +207,14 @@ __global__ void __launch_bounds__(kTrackSlots) rk8_tracker_kernel(const double* 
             }
             y[0] += prm.dt * dtt;
             y[1] += prm.dt * ds;
-            for (int c = 0; c < 6; c++)
+            double dp2 = 0.;
+            for (int c = 0; c < 6; c++) {
+                const double before = y[2 + c];
                 y[2 + c] += prm.dt * d[c];
+                if (c >= 3)
+                    dp2 += (y[2 + c] - before) * (y[2 + c] - before);
+            }
+            dps += sqrt(dp2);  // KSStep::ContinuousMomentumChange (KSRootTrajectory.cxx:217-218)
             nstep++;
             my_steps++;
             const double r2 = y[2] * y[2] + y[3] * y[3] + y[4] * y[4];
@@ -225,6 +235,8 @@ __global__ void __launch_bounds__(kTrackSlots) rk8_tracker_kernel(const double* 
                 for (int c = 0; c < 8; c++)
                     state[(size_t) track * 8 + c] = y[c];
                 steps[track] = nstep;
+                if (dpsum)
+                    dpsum[track] = dps;
                 if (stat != 0)
                     status[track] = stat;
                 pull();

@@ -20,3 +20,17 @@ def test_kemfield_adaptors_against_reference_classes():
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "OK" in r.stdout
+
+
+BATCH = os.path.join(ROOT, "oracle", "_ref", "batch_driver_check")
+
+
+@pytest.mark.skipif(not os.path.exists(BATCH), reason="batch driver check not built (needs the reference tree)")
+def test_kassiopeia_batch_driver_against_reference_rk8():
+    # include/kassiopeia_cuda.hh: Kassiopeia KSParticles tracked as one batch on the GPU fill
+    # KSTrack objects that match the reference's KSMathRK8 driven by the reference field solver
+    # (tests/cxx/batch_driver_check.cc, built by `make -C oracle batch`)
+    r = subprocess.run([BATCH], capture_output=True, text=True, timeout=900)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "OK" in r.stdout
