@@ -282,6 +282,16 @@ class KCUDAElectricFieldSolver : public KElectricFieldSolver
     {
         fDevice = device;
     }
+    int GetPrecision() const
+    {
+        return fPrecision;
+    }
+    int GetDevice() const
+    {
+        return fDevice;
+    }
+    // the single-point calls of KElectricFieldSolver stay visible beside the batched ones
+    using KElectricFieldSolver::ElectricFieldAndPotential;
     // batched extension: n points P (x, y, z each), out n x 4 (Ex, Ey, Ez, phi); one device call
     void ElectricFieldAndPotential(const double* P, size_t n, double* out) const
     {
@@ -457,6 +467,14 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
     {
         fMode = mode;
     }
+    int GetMaxIterations() const
+    {
+        return fMaxIterations;
+    }
+    int GetMode() const
+    {
+        return fMode;
+    }
     // XML form: "plain", "mixed", "assembled" or "assembled_fp64" (kemcu_solve_mode)
     void SetModeName(const std::string& name)
     {
@@ -515,6 +533,14 @@ class KCUDARobinHoodChargeDensitySolver : public KCUDAChargeDensitySolverBase
     void CacheMatrixElements(bool choice)
     {
         fAssembled = choice;
+    }
+    int GetCheckSubInterval() const
+    {
+        return fCheckInterval;
+    }
+    bool MatrixElementsCached() const
+    {
+        return fAssembled;
     }
     kemcu_rh_stats Solve(KCUDASurfaceContainer& container) const
     {

@@ -89,3 +89,17 @@ def test_kemfield_adaptor_builds_against_reference():
     r = subprocess.run(["make", "-s", "-C", os.path.join(root, "oracle"), "adaptor"], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-2000:]
     assert os.path.exists(os.path.join(root, "oracle", "_ref", "adaptor_check"))
+
+
+def test_xml_bindings_parse_without_a_device():
+    # the XML half of tests/cxx/bindings_check.cc: the reference's Kommon tokenizer reads a
+    # configuration with the CUDA elements and the use_cuda switch, and every setting arrives
+    import os
+
+    binary = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                          "bindings_check")
+    if not os.path.exists(binary):
+        pytest.skip("bindings check not built (needs the reference tree)")
+    r = subprocess.run([binary, "--parse-only"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "parsed 3 field elements" in r.stdout and "settings from the XML: as written" in r.stdout

@@ -34,3 +34,17 @@ def test_kassiopeia_batch_driver_against_reference_rk8():
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "OK" in r.stdout
+
+
+XML = os.path.join(ROOT, "oracle", "_ref", "bindings_check")
+
+
+@pytest.mark.skipif(not os.path.exists(XML), reason="bindings check not built (needs the reference tree)")
+def test_xml_bindings_configure_the_gpu_solvers():
+    # include/kemfield_cuda_bindings.hh: a KEMField-style XML file parsed by the reference's own
+    # Kommon tokenizer configures the CUDA solvers (and the use_cuda switch) of boundary fields
+    # whose fields then match the reference CPU field solver (tests/cxx/bindings_check.cc)
+    r = subprocess.run([XML], capture_output=True, text=True, timeout=600)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "OK" in r.stdout
