@@ -207,6 +207,10 @@ def run_native(args, rank, world, dist):
         x_a64, st_a64 = ctx.Solve(tol=TOL, max_iter=300, mode=K.SOLVE_ASSEMBLED_FP64)
         st_a64["repeat_seconds"] = ctx.Solve(tol=TOL, max_iter=300, mode=K.SOLVE_ASSEMBLED_FP64)[1]["seconds"]
         st_asm["fp64_assembled"] = st_a64
+        # the north-star pattern, matrix-free like the plain solve: inner GMRES on the FP32
+        # far-field operator, FP64 residual and refinement
+        x_f32, st_f32 = ctx.Solve(tol=TOL, max_iter=300, mode=K.SOLVE_FP32)
+        st_asm["fp32_refined_matrix_free"] = st_f32
         sigma_diff = float(np.max(np.abs(x_asm - x_plain)) / np.max(np.abs(x_plain)))
     ctx.SetSigma(x_asm)
 
@@ -248,6 +252,11 @@ def run_native(args, rank, world, dist):
     ms_mixed = max_over_ranks(ms_mixed)
     barrier()
     ms_fp64 = max_over_ranks(device_steps(K.FP64, args.steps))
+    # the FP32 far-field form (a few 1e-8 of the largest value: outside the metric's 1e-9 bound,
+    # so reported beside it, not as the value)
+    device_steps(K.FP32, 1)
+    barrier()
+    ms_fp32 = max_over_ranks(device_steps(K.FP32, args.steps))
 
     # end-to-end through the C ABI with pinned host buffers
     hP = torch.from_numpy(P).pin_memory()
@@ -270,6 +279,8 @@ def run_native(args, rank, world, dist):
     o32 = ctx.ElectricFieldAndPotential(sub, precision=K.MIXED)
     err_E = float(np.max(np.linalg.norm(o32[:, :3] - o64[:, :3], axis=1) / np.linalg.norm(o64[:, :3], axis=1)))
     err_phi = float(np.max(np.abs(o32[:, 3] - o64[:, 3])) / np.max(np.abs(o64[:, 3])))
+    of32 = ctx.ElectricFieldAndPotential(sub, precision=K.FP32)
+    err_fp32 = accuracy_vs(of32, o64)
 
     # algorithmic work (band histogram on a 2% sample, scaled) and the FP64 roofline
     hs = P[::50]
@@ -370,7 +381,7 @@ def run_native(args, rank, world, dist):
             "krylov_iterations": s5["iterations"], "rel_residual": s5["rel_residual"]}
 
     res = dict(
-        ms_mixed=ms_mixed, ms_fp64=ms_fp64, wall_mixed=wall_mixed, e2e_s=e2e_s, launches=int(launches),
+        ms_mixed=ms_mixed, ms_fp64=ms_fp64, ms_fp32=ms_fp32, err_fp32=err_fp32, wall_mixed=wall_mixed, e2e_s=e2e_s, launches=int(launches),
         err_E=err_E, err_phi=err_phi, flops_per_step=flops_per_step, fp64_peak=f64.value, fp32_peak=f32.value,
         counts=counts.tolist(), st_plain=st_plain, st_asm=st_asm, sigma_diff=sigma_diff, clocks=clk.summary(),
         extra=extra, mesh=mesh, sigma=x_asm, P=P, axisym=axisym_case, tune=tune)
@@ -562,7 +573,7 @@ def main():
                             "processes": f"{workers} (one per physical core)"}}
             # the GPU's field at the points the reference evaluated, against the reference's values
             acc_ref = {"points": int(len(ref_pts)), "reference": "oracle/_ref (KIntegratingFieldSolver, FP64)"}
-            for prec, name in ((0, "fp64"), (1, "mixed")):
+            for prec, name in ((0, "fp64"), (1, "mixed"), (2, "fp32")):
                 acc_ref[name] = accuracy_vs(r["field_at"](ref_pts, prec), ref_vals)
             acc_ref["bound_met_1e-9"] = bool(max(acc_ref["mixed"]["max_err_E_over_max_E"],
                                                  acc_ref["mixed"]["max_err_phi_over_max_phi"]) <= 1e-9)
@@ -613,6 +624,14 @@ def main():
             "autotune_coax": r["tune"],
             "plain_fp64": {"value": fp64_value, "unit": "points/s", "ms_per_step": r["ms_fp64"] / steps,
                            "speedup_mixed_over_plain": value / fp64_value},
+            "fp32_far_field": {"value": pts / (r["ms_fp32"] / steps * 1e-3), "unit": "points/s",
+                               "ms_per_step": r["ms_fp32"] / steps,
+                               "speedup_over_plain_fp64": r["ms_fp64"] / r["ms_fp32"],
+                               "speedup_over_mixed": r["ms_mixed"] / r["ms_fp32"],
+                               "accuracy_vs_fp64": r["err_fp32"],
+                               "notes": "cubature nodes of triangles and rectangles in FP32 relative to each "
+                                        "element's FP64 centre distance; analytic near field, wires and the "
+                                        "compensated element sums in FP64"},
             "accuracy_mixed_vs_fp64": {"max_rel_err_E_per_point": r["err_E"],
                                        "max_abs_err_phi_over_max_phi": r["err_phi"]},
             "gmres": gmres_summary(r),
@@ -643,6 +662,12 @@ def gmres_summary(r):
         out["speedup_assembly_only"] = p["seconds"] / a64["repeat_seconds"]
     if a["seconds"] == a["seconds"] and a["seconds"] > 0:
         out["speedup_mixed_first_solve_over_plain_matrix_free"] = p["seconds"] / a["seconds"]
+    f32 = a.get("fp32_refined_matrix_free")
+    if f32:
+        out["fp32_refined_matrix_free_s"] = f32["seconds"]
+        out["fp32_refined_matrix_free_iterations"] = f32["iterations"]
+        out["fp32_refined_matrix_free_rel_residual"] = f32["rel_residual"]
+        out["speedup_fp32_refined_over_plain_matrix_free"] = p["seconds"] / f32["seconds"]
     return out
 
 
@@ -657,6 +682,7 @@ def targets(value, fp64_value, r):
            "gmres_mixed_assembled_first_solve_over_plain_matrix_free":
                g.get("speedup_mixed_first_solve_over_plain_matrix_free"),
            "gmres_end_to_end_met": bool((g.get("speedup_mixed_first_solve_over_plain_matrix_free") or 0) >= 10.0),
+           "gmres_fp32_refined_over_plain_matrix_free": g.get("speedup_fp32_refined_over_plain_matrix_free"),
            "notes": "field: same direct-sum kernel in both forms (FP64 vs Newton-refined FP32-class rsqrt per "
                     "node); the FP64 pipe is half the FP32 rate on B200, so precision alone cannot give 10x. "
                     "gmres_end_to_end: the mixed solve on the assembled operator, assembly included, against "

@@ -57,9 +57,15 @@ enum kemcu_boundary { KEMCU_DIRICHLET = 0, KEMCU_NEUMANN = 1 };
 /* arithmetic form of the element integrals */
 enum kemcu_precision {
     KEMCU_FP64 = 0,  /* every node in FP64: the plain form */
-    KEMCU_MIXED = 1  /* cubature nodes with the FP32-class hardware reciprocal square root
+    KEMCU_MIXED = 1, /* cubature nodes with the FP32-class hardware reciprocal square root
                         refined by one FP64 Newton step (~1e-13 relative); RWG / analytic
                         near field and the compensated accumulation as in FP64 */
+    KEMCU_FP32 = 2   /* far field in FP32: the cubature nodes of triangles and rectangles on
+                        FP32 FMAs and the FP32 hardware reciprocal square root, relative to the
+                        element's FP64 centre distance (~1e-7 relative per element); the RWG /
+                        analytic near field, wires, the per-element set-up and the compensated
+                        element sums in FP64. Field evaluation and matrix-free matvec only (the
+                        tracker, the adjoint and the autotuner take FP64 and MIXED) */
 };
 /* which quantities a field evaluation produces (out4 = Ex, Ey, Ez, phi) */
 enum kemcu_what { KEMCU_FIELD_AND_POTENTIAL = 0, KEMCU_POTENTIAL = 1, KEMCU_FIELD = 2 };
@@ -70,9 +76,12 @@ enum kemcu_solve_mode {
                                   operator, FP64 matrix-free residual and correction */
     KEMCU_SOLVE_ASSEMBLED = 2, /* operator assembled once in HBM (FP64, plus an FP32 copy);
                                   inner GMRES on FP32, FP64 residual (refinement) */
-    KEMCU_SOLVE_ASSEMBLED_FP64 = 3 /* GMRES on the assembled FP64 operator alone (no FP32 copy,
+    KEMCU_SOLVE_ASSEMBLED_FP64 = 3, /* GMRES on the assembled FP64 operator alone (no FP32 copy,
                                   no refinement): the plain algorithm with the same assembly,
                                   which separates the gain of assembly from that of precision */
+    KEMCU_SOLVE_FP32 = 4       /* iterative refinement, matrix-free: inner GMRES on the FP32
+                                  far-field operator (KEMCU_FP32), FP64 matrix-free residual and
+                                  correction; FP64-accurate charge densities */
 };
 
 typedef struct kemcu_ctx kemcu_ctx;
@@ -181,7 +190,8 @@ int kemcu_field_variant_count(void);
 /* single entry A(i, j) = BoundaryIntegral(source j, target i) (KBoundaryIntegralMatrix.hh:31-55) */
 int kemcu_matrix_element(kemcu_ctx* ctx, size_t i, size_t j, double* a);
 /* y = A x for n_rhs right-hand sides (x, y: n_rhs x n), KMatrix::Multiply (KMatrix.hh:87-99);
-   assembled != 0 uses (and on first use builds) the assembled FP64 operator */
+   assembled != 0 uses (and on first use builds) the assembled operator: its FP64 copy for
+   KEMCU_FP64, its FP32 copy for KEMCU_MIXED and KEMCU_FP32 */
 int kemcu_matvec(kemcu_ctx* ctx, const double* x, double* y, int n_rhs, int precision, int assembled);
 
 /* ---- charge-density solve (KSimpleIterativeKrylovSolver<double, KGeneralizedMinimalResidual>::Solve,

@@ -269,7 +269,7 @@ class KCUDAElectricFieldSolver : public KElectricFieldSolver
         fPrecision(precision),
         fDevice(device)
     {}
-    // the arithmetic of the cubature nodes: KEMCU_FP64 (default) or KEMCU_MIXED
+    // the arithmetic of the cubature nodes: KEMCU_FP64 (default), KEMCU_MIXED or KEMCU_FP32
     void SetPrecision(int precision)
     {
         fPrecision = precision;
@@ -475,7 +475,7 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
     {
         return fMode;
     }
-    // XML form: "plain", "mixed", "assembled" or "assembled_fp64" (kemcu_solve_mode)
+    // XML form: "plain", "mixed", "assembled", "assembled_fp64" or "fp32" (kemcu_solve_mode)
     void SetModeName(const std::string& name)
     {
         if (name == "plain")
@@ -486,9 +486,11 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
             fMode = KEMCU_SOLVE_ASSEMBLED;
         else if (name == "assembled_fp64")
             fMode = KEMCU_SOLVE_ASSEMBLED_FP64;
+        else if (name == "fp32")
+            fMode = KEMCU_SOLVE_FP32;
         else
             throw KEMSimpleException("kemcu: unknown solve mode <" + name +
-                                     "> (plain, mixed, assembled, assembled_fp64)");
+                                     "> (plain, mixed, assembled, assembled_fp64, fp32)");
     }
     // solves A sigma = b for the boundary values and writes sigma into the container
     kemcu_solve_stats Solve(KCUDASurfaceContainer& container) const

@@ -7,11 +7,11 @@
 // RegisterKEMCUBuilders<KElectrostaticBoundaryFieldBuilder>() in one source file of the build):
 //
 //   <cuda_krylov_charge_density_solver tolerance max_iterations mode device/>
-//       KCUDAChargeDensitySolver: GMRES on the device; mode = plain | mixed | assembled | assembled_fp64
+//       KCUDAChargeDensitySolver: GMRES on the device; mode = plain | mixed | assembled | assembled_fp64 | fp32
 //   <cuda_robin_hood_charge_density_solver tolerance check_sub_interval cache_matrix_elements device/>
 //       KCUDARobinHoodChargeDensitySolver (attribute names of the reference's robin_hood element)
 //   <cuda_field_solver precision device/>
-//       KCUDAElectricFieldSolver; precision = fp64 | mixed
+//       KCUDAElectricFieldSolver; precision = fp64 | mixed | fp32
 //   <integrating_field_solver integrator use_opencl use_cuda cuda_precision cuda_device/>
 //       KIntegratingElectrostaticFieldSolverCUDA: the reference's integrating field solver with a
 //       use_cuda switch beside use_opencl (KIntegratingElectrostaticFieldSolverBuilder.cc:20-21);
@@ -102,13 +102,15 @@ class KIntegratingElectrostaticFieldSolverCUDA : public KElectricFieldSolver
     KCUDAElectricFieldSolver fCUDA;
 };
 
-// "fp64" | "mixed" -> kemcu_precision; -1 for anything else
+// "fp64" | "mixed" | "fp32" -> kemcu_precision; -1 for anything else
 inline int KEMCUPrecisionFromName(const std::string& name)
 {
     if (name == "fp64")
         return KEMCU_FP64;
     if (name == "mixed")
         return KEMCU_MIXED;
+    if (name == "fp32")
+        return KEMCU_FP32;
     return -1;
 }
 
@@ -167,7 +169,7 @@ template<> inline bool KCUDAElectricFieldSolverBuilder::AddAttribute(KContainer*
     if (name == "precision") {
         const int p = KEMField::KEMCUPrecisionFromName(aContainer->AsString());
         if (p < 0) {
-            BINDINGMSG(eWarning) << "cuda_field_solver: precision must be <fp64> or <mixed>" << eom;
+            BINDINGMSG(eWarning) << "cuda_field_solver: precision must be <fp64>, <mixed> or <fp32>" << eom;
             return false;
         }
         fObject->SetPrecision(p);
@@ -193,7 +195,8 @@ template<> inline bool KIntegratingElectrostaticFieldSolverCUDABuilder::AddAttri
     else if (name == "cuda_precision") {
         const int p = KEMField::KEMCUPrecisionFromName(aContainer->AsString());
         if (p < 0) {
-            BINDINGMSG(eWarning) << "integrating_field_solver: cuda_precision must be <fp64> or <mixed>" << eom;
+            BINDINGMSG(eWarning) << "integrating_field_solver: cuda_precision must be <fp64>, <mixed> or <fp32>"
+                                 << eom;
             return false;
         }
         fObject->SetCUDAPrecision(p);

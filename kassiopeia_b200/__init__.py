@@ -23,11 +23,11 @@ import ctypes as C
 import numpy as np
 
 from . import _native as N
-from ._native import (FIELD, FIELD_AND_POTENTIAL, FP64, MIXED, POTENTIAL, SOLVE_ASSEMBLED, SOLVE_ASSEMBLED_FP64,
-                      SOLVE_MIXED, SOLVE_PLAIN, KemcuError)
+from ._native import (FIELD, FIELD_AND_POTENTIAL, FP32, FP64, MIXED, POTENTIAL, SOLVE_ASSEMBLED, SOLVE_ASSEMBLED_FP64,
+                      SOLVE_FP32, SOLVE_MIXED, SOLVE_PLAIN, KemcuError)
 
-__all__ = ["CUDAElectrostaticContext", "KemcuError", "FP64", "MIXED", "SOLVE_PLAIN", "SOLVE_MIXED",
-           "SOLVE_ASSEMBLED", "SOLVE_ASSEMBLED_FP64", "FIELD_AND_POTENTIAL", "POTENTIAL", "FIELD"]
+__all__ = ["CUDAElectrostaticContext", "KemcuError", "FP64", "MIXED", "FP32", "SOLVE_PLAIN", "SOLVE_MIXED",
+           "SOLVE_ASSEMBLED", "SOLVE_ASSEMBLED_FP64", "SOLVE_FP32", "FIELD_AND_POTENTIAL", "POTENTIAL", "FIELD"]
 
 ONE_OVER_FOUR_PI_EPS0 = 1.0 / (4.0 * np.pi * 8.8541878128e-12)  # KEMConstants (KConst epoch 2021)
 EPS0 = 8.8541878128e-12

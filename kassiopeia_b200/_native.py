@@ -15,9 +15,9 @@ LIB_PATH = os.path.join(HERE, "libkemcu.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "kemcu.h")
 
 OK, EINVAL, ECUDA, ENONFINITE, ENOTCONVERGED, ETIMEOUT, ENOMEM, ESTATE = 0, -1, -2, -3, -4, -5, -6, -7
-FP64, MIXED = 0, 1
+FP64, MIXED, FP32 = 0, 1, 2
 FIELD_AND_POTENTIAL, POTENTIAL, FIELD = 0, 1, 2
-SOLVE_PLAIN, SOLVE_MIXED, SOLVE_ASSEMBLED, SOLVE_ASSEMBLED_FP64 = 0, 1, 2, 3
+SOLVE_PLAIN, SOLVE_MIXED, SOLVE_ASSEMBLED, SOLVE_ASSEMBLED_FP64, SOLVE_FP32 = 0, 1, 2, 3, 4
 TRACK_ACTIVE, TRACK_HIT, TRACK_MAX_STEPS, TRACK_LEFT, TRACK_NONFINITE = 0, 1, 2, 3, 4
 
 _ERRNAMES = {EINVAL: "EINVAL", ECUDA: "ECUDA", ENONFINITE: "ENONFINITE", ENOTCONVERGED: "ENOTCONVERGED",

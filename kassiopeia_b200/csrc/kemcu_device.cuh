@@ -87,6 +87,10 @@ __constant__ double c_q[kNumNodes * kQ];
 constexpr int kPair7 = 0, kPair12 = 3, kPair33 = 9, kNumPairs = 25;
 __constant__ double c_qp[kNumPairs * kQ];
 __constant__ double c_qc[2];
+// the same three tables rounded to FP32, for the FP32 far-field form (cubq32, cubq_pairs32)
+__constant__ float c_q32[kNumNodes * kQ];
+__constant__ float c_qp32[kNumPairs * kQ];
+__constant__ float c_qc32[2];
 __constant__ double c_gl[10 * 2];
 __constant__ Constants c_k;
 
@@ -326,6 +330,123 @@ __device__ __forceinline__ Out4 cubq_pairs(const double* e, V3 d, double R2)
         o.ez = pff * (d.z * s0 - a.z * ss - b.z * st);
     }
     return o;
+}
+
+// ------------------------------------------------------------------------- FP32 far field
+// The FP32 form of the cubature bands (precision KEMCU_FP32): the per-element set-up stays FP64
+// (d = P - centroid, R^2 from the band test, R^-1 to an ulp), and every node works on the
+// distance relative to R: with C1, C2 and the quadratic-form coefficients divided by R^2 (then
+// rounded to FP32), |P - Q_k|^2 / R^2 = 1 + x_k, x_k = c0 C1' + c1 C2' + c2 |A N1|^2' + ...
+// (five FP32 FMAs), and R / |P - Q_k| = rsqrt(1 + x_k) from the FP32 hardware estimate. The
+// node sums run in FP32 on values near 1 (the weights sum to 1), then scale back in FP64:
+// phi = area/(4 pi eps0) R^-1 sum w f, E = area/(4 pi eps0) R^-3 (d S0 - A N1 Ss - B N2 St).
+// Relative error per element-point pair ~1e-7 (FP32 rounding of x and of the estimate); the
+// element sums are compensated in FP64 by the callers.
+__device__ __forceinline__ float rsqrt_f32(float x)
+{
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+struct Far32
+{
+    float u1, u2, aa, ab, bb;  // C1 / R^2, C2 / R^2, |A N1|^2 / R^2, 2 (A N1).(B N2) / R^2, |B N2|^2 / R^2
+    double ir;                 // R^-1
+};
+
+__device__ __forceinline__ Far32 far32_setup(const double* e, V3 d, double R2, V3 a, V3 b)
+{
+    Far32 f;
+    f.ir = 0.5 * rsqrt2_acc(R2);
+    const double inv = f.ir * f.ir;
+    f.u1 = (float) (dot(d, a) * inv);
+    f.u2 = (float) (dot(d, b) * inv);
+    f.aa = (float) (e[rAA] * inv);
+    f.ab = (float) (e[rAB2] * inv);
+    f.bb = (float) (e[rBB] * inv);
+    return f;
+}
+
+template<bool POT, bool FIELD>
+__device__ __forceinline__ Out4 far32_finish(const double* e, V3 d, V3 a, V3 b, const Far32& f, float sp, float s0,
+                                             float ss, float st)
+{
+    const double pf = e[rPrefac];
+    Out4 o{0., 0., 0., 0.};
+    if (POT)
+        o.phi = (pf * f.ir) * (double) sp;
+    if (FIELD) {
+        const double pff = pf * (f.ir * f.ir * f.ir);
+        const double S0 = s0, Ss = ss, St = st;
+        o.ex = pff * (d.x * S0 - a.x * Ss - b.x * St);
+        o.ey = pff * (d.y * S0 - a.y * Ss - b.y * St);
+        o.ez = pff * (d.z * S0 - a.z * Ss - b.z * St);
+    }
+    return o;
+}
+
+template<int N, int OFF, bool POT, bool FIELD>
+__device__ __forceinline__ Out4 cubq32(const double* e, V3 d, double R2)
+{
+    const V3 a = ld3(e + rEa), b = ld3(e + rEb);
+    const Far32 f = far32_setup(e, d, R2, a, b);
+    float sp = 0.f, s0 = 0.f, ss = 0.f, st = 0.f;
+    constexpr int G = N % KEMCU_GROUP == 0 ? KEMCU_GROUP : N;
+#pragma unroll 1
+    for (int g = 0; g < N / G; g++) {
+        const float* cg = c_q32 + kQ * (OFF + g * G);
+#pragma unroll
+        for (int k = 0; k < G; k++) {
+            const float* c = cg + kQ * k;
+            float x = c[4] * f.bb;
+            x = fmaf(c[3], f.ab, x);
+            x = fmaf(c[2], f.aa, x);
+            x = fmaf(c[1], f.u2, x);
+            x = fmaf(c[0], f.u1, x);
+            const float r = rsqrt_f32(1.f + x);
+            if (POT)
+                sp = fmaf(c[5], r, sp);
+            if (FIELD) {
+                const float r3 = r * r * r;
+                s0 = fmaf(c[5], r3, s0);
+                ss = fmaf(c[6], r3, ss);
+                st = fmaf(c[7], r3, st);
+            }
+        }
+    }
+    return far32_finish<POT, FIELD>(e, d, a, b, f, sp, s0, ss, st);
+}
+
+template<int NP, int POFF, int CENTER, bool POT, bool FIELD>
+__device__ __forceinline__ Out4 cubq_pairs32(const double* e, V3 d, double R2)
+{
+    const V3 a = ld3(e + rEa), b = ld3(e + rEb);
+    const Far32 f = far32_setup(e, d, R2, a, b);
+    float sp = 0.f, s0 = 0.f, ss = 0.f, st = 0.f;
+    if (CENTER >= 0) {  // the centroid node: distance R, relative 1
+        sp = c_qc32[CENTER];
+        s0 = c_qc32[CENTER];
+    }
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+        const float* c = c_qp32 + kQ * (POFF + k);
+        const float L = fmaf(c[1], f.u2, c[0] * f.u1);
+        float Q = fmaf(c[4], f.bb, 1.f);
+        Q = fmaf(c[3], f.ab, Q);
+        Q = fmaf(c[2], f.aa, Q);
+        const float rp = rsqrt_f32(Q + L), rm = rsqrt_f32(Q - L);
+        if (POT)
+            sp = fmaf(c[5], rp + rm, sp);
+        if (FIELD) {
+            const float r3p = rp * rp * rp, r3m = rm * rm * rm;
+            s0 = fmaf(c[5], r3p + r3m, s0);
+            const float dd = r3p - r3m;
+            ss = fmaf(c[6], dd, ss);
+            st = fmaf(c[7], dd, st);
+        }
+    }
+    return far32_finish<POT, FIELD>(e, d, a, b, f, sp, s0, ss, st);
 }
 
 // ------------------------------------------------------------------------- RWG (analytic)
@@ -624,12 +745,25 @@ template<bool POT, bool FIELD> __device__ __noinline__ Out4 line_analytic(const 
 // epi_far: a pair in a quadrature band (band_of(e, P, d, r2) returned band >= 1, with its d and
 // r2); no analytic near-field code, so callers that route the analytic pairs elsewhere carry
 // none of its registers or calls.
-template<bool MIXED, bool POT, bool FIELD>
+// F32 selects the FP32 far-field form for the triangle and rectangle cubature bands (wires keep
+// their FP64 Gauss-Legendre sums).
+template<bool MIXED, bool POT, bool FIELD, bool F32 = false>
 __device__ __forceinline__ Out4 epi_far(const double* e, V3 P, V3 d, double r2, int band)
 {
     const int type = (int) e[rType];
     if (type == kLineSegment)
         return band == 1 ? line_gauss<POT, FIELD>(e, P, 2, 8) : line_gauss<POT, FIELD>(e, P, 0, 2);
+    if (F32) {
+        if (type == kTriangle) {
+            if (band == 1)
+                return cubq32<33, kTri33, POT, FIELD>(e, d, r2);
+            return band == 2 ? cubq32<12, kTri12, POT, FIELD>(e, d, r2) : cubq32<7, kTri7, POT, FIELD>(e, d, r2);
+        }
+        if (band == 1)
+            return cubq_pairs32<16, kPair33, 1, POT, FIELD>(e, d, r2);
+        return band == 2 ? cubq_pairs32<6, kPair12, -1, POT, FIELD>(e, d, r2)
+                         : cubq_pairs32<3, kPair7, 0, POT, FIELD>(e, d, r2);
+    }
     if (type == kTriangle) {
         if (band == 1)
             return cubq<33, kTri33, POT, FIELD, MIXED>(e, d, r2);
@@ -640,7 +774,7 @@ __device__ __forceinline__ Out4 epi_far(const double* e, V3 P, V3 d, double r2, 
     return band == 2 ? cubq_pairs<6, kPair12, -1, POT, FIELD, MIXED>(e, d, r2) : cubq_pairs<3, kPair7, 0, POT, FIELD, MIXED>(e, d, r2);
 }
 
-template<bool MIXED, bool POT, bool FIELD> __device__ __forceinline__ Out4 epi(const double* e, V3 P)
+template<bool MIXED, bool POT, bool FIELD, bool F32 = false> __device__ __forceinline__ Out4 epi(const double* e, V3 P)
 {
     V3 d;
     double r2;
@@ -651,7 +785,7 @@ template<bool MIXED, bool POT, bool FIELD> __device__ __forceinline__ Out4 epi(c
             return line_analytic<POT, FIELD>(e, P);
         return type == kTriangle ? rwg64<3, POT, FIELD>(e, P) : rwg64<4, POT, FIELD>(e, P);
     }
-    return epi_far<MIXED, POT, FIELD>(e, P, d, r2, band);
+    return epi_far<MIXED, POT, FIELD, F32>(e, P, d, r2, band);
 }
 
 }  // namespace kemcu

@@ -278,8 +278,9 @@ template<int SIDE, int NP = kPipe, bool CYCLIC = false> struct ElementRing
 // flag |= 2 if a pipeline wait timed out (the outputs are then incomplete).
 // MINB (resident CTAs per SM the registers are bounded for) and NP (ring stages) are the shapes
 // the autotuner chooses between (field_variants); neither changes an operation or its order, so
-// every variant gives the same result bit for bit.
-template<bool MIXED, bool POT, bool FIELD, int MINB = kMinBlocks, int NP = kPipe>
+// every variant gives the same result bit for bit. F32: the FP32 far-field form of the cubature
+// bands (precision KEMCU_FP32), the tile and Kahan sums staying FP64.
+template<bool MIXED, bool POT, bool FIELD, int MINB = kMinBlocks, int NP = kPipe, bool F32 = false>
 __global__ void __launch_bounds__(kThreads, MINB) field_kernel(const double* __restrict__ rec, const double* __restrict__ sigma,
                                                                int n_elem, const double* __restrict__ pts, int n_pts,
                                                                double* __restrict__ out, double* __restrict__ partial,
@@ -309,7 +310,7 @@ __global__ void __launch_bounds__(kThreads, MINB) field_kernel(const double* __r
             const int cnt = R.count(i);
             double tx = 0., ty = 0., tz = 0., tp = 0.;
             for (int j = 0; j < cnt; j++) {
-                const Out4 r = epi<MIXED, POT, FIELD>(R.element(i, j), P);
+                const Out4 r = epi<MIXED, POT, FIELD, F32>(R.element(i, j), P);
                 const double sg = R.side(i, 0, j);
                 if (FIELD) {
                     tx = fma(r.ex, sg, tx);
@@ -361,16 +362,17 @@ struct TargetRec
     double neumann;   // 0 Dirichlet, 1 Neumann
 };
 
-// one matrix entry A(i, j) with source record e and target t
-template<bool MIXED> __device__ __forceinline__ double entry(const double* e, const TargetRec& t, V3 C)
+// one matrix entry A(i, j) with source record e and target t (F32: the FP32 far-field form of
+// the cubature bands)
+template<bool MIXED, bool F32 = false> __device__ __forceinline__ double entry(const double* e, const TargetRec& t, V3 C)
 {
     if (t.neumann == 0.) {
-        return epi<MIXED, true, false>(e, C).phi;
+        return epi<MIXED, true, false, F32>(e, C).phi;
     }
     const V3 cs = ld3(e + rCen2);
     const double dist = norm(cs - C);
     if (dist >= 1e-12) {
-        const Out4 r = epi<MIXED, false, true>(e, C);
+        const Out4 r = epi<MIXED, false, true, F32>(e, C);
         return r.ex * t.normal[0] + r.ey * t.normal[1] + r.ez * t.normal[2];
     }
     return t.diag;
@@ -400,7 +402,7 @@ __global__ void entry_kernel(const double* __restrict__ rec, const TargetRec* __
 // KMatrix.hh:92-99, KBoundaryIntegralMatrix.hh:31-55). Same element ring as K1, with the
 // operand values of the tile as side data.
 constexpr int kMaxRhs = 8;
-template<bool MIXED, int NR>
+template<bool MIXED, int NR, bool F32 = false>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) matvec_kernel(const double* __restrict__ rec, const TargetRec* __restrict__ tgt,
                                                           int n, const double* __restrict__ x, int nrhs,
                                                           double* __restrict__ y, double* __restrict__ partial,
@@ -433,7 +435,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) matvec_kernel(const doub
         if (active) {
             const int cnt = R.count(q);
             for (int j = 0; j < cnt; j++) {
-                const double a = entry<MIXED>(R.element(q, j), t, C);
+                const double a = entry<MIXED, F32>(R.element(q, j), t, C);
 #pragma unroll
                 for (int r = 0; r < NR; r++)
                     if (r < nrhs)

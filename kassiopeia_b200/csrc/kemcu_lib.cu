@@ -398,8 +398,8 @@ int tune_key(int precision, size_t n)
 int choose_variant(kemcu_ctx* ctx, size_t n, int precision, int what)
 {
     ctx->pending_key = -1;
-    if (what != KEMCU_FIELD_AND_POTENTIAL)
-        return 0;
+    if (what != KEMCU_FIELD_AND_POTENTIAL || precision == KEMCU_FP32)
+        return 0;  // one launch shape outside the field-and-potential kernels of FP64 and MIXED
     if (ctx->force_variant >= 0)
         return ctx->force_variant;
     const int key = tune_key(precision, n);
@@ -450,7 +450,16 @@ int launch_planar_field(kemcu_ctx* ctx, const double* d_pts, size_t n, double* d
     const bool timed = ctx->pending_key >= 0 || ctx->time_k1;
     if (timed)
         KC(cudaEventRecord(ctx->tv0, st));
-    if (what == KEMCU_POTENTIAL) {
+    if (precision == KEMCU_FP32) {
+        const double* r = ctx->d_rec;
+        if (what == KEMCU_POTENTIAL)
+            field_kernel<false, true, false, kMinBlocks, kPipe, true><<<grid, kThreads, 0, st>>>(r, sg, ne, d_pts, np, d_out, part, fl);
+        else if (what == KEMCU_FIELD)
+            field_kernel<false, false, true, kMinBlocks, kPipe, true><<<grid, kThreads, 0, st>>>(r, sg, ne, d_pts, np, d_out, part, fl);
+        else
+            field_kernel<false, true, true, kMinBlocks, kPipe, true><<<grid, kThreads, 0, st>>>(r, sg, ne, d_pts, np, d_out, part, fl);
+    }
+    else if (what == KEMCU_POTENTIAL) {
         if (mixed)
             launch_k1<true, true, false>(v, grid, st, ctx->d_rec, sg, ne, d_pts, np, d_out, part, fl);
         else
@@ -563,13 +572,14 @@ enum OpKind
     kFree64 = 0,
     kFreeMixed,
     kDense64,
-    kDense32
+    kDense32,
+    kFree32  // matrix-free with the FP32 far-field form
 };
 
 int apply_op(kemcu_ctx* ctx, int op, const double* d_x, double* d_y, int nrhs)
 {
     const int n = (int) ctx->n;
-    if ((op == kFree64 || op == kFreeMixed) && ctx->axisym) {
+    if ((op == kFree64 || op == kFreeMixed || op == kFree32) && ctx->axisym) {
         const int split = axisym_split(ctx->num_sms, n, n);
         double* partial = nullptr;
         if (split > 1) {
@@ -593,7 +603,7 @@ int apply_op(kemcu_ctx* ctx, int op, const double* d_x, double* d_y, int nrhs)
         }
         return KEMCU_OK;
     }
-    if (op == kFree64 || op == kFreeMixed) {
+    if (op == kFree64 || op == kFreeMixed || op == kFree32) {
         const int split = grid_split(ctx, n, n);
         double* partial = nullptr;
         if (split > 1) {
@@ -605,7 +615,15 @@ int apply_op(kemcu_ctx* ctx, int op, const double* d_x, double* d_y, int nrhs)
         }
         dim3 grid((n + kThreads - 1) / kThreads, split);
         int* fl = ctx->d_flag + 1;
-        if (op == kFree64) {
+        if (op == kFree32) {
+            if (nrhs == 1)
+                matvec_kernel<false, 1, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, ctx->d_tgt, n, d_x, nrhs, d_y,
+                                                                                partial, fl);
+            else
+                matvec_kernel<false, kMaxRhs, true><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, ctx->d_tgt, n, d_x, nrhs,
+                                                                                      d_y, partial, fl);
+        }
+        else if (op == kFree64) {
             if (nrhs == 1)
                 matvec_kernel<false, 1><<<grid, kThreads, 0, ctx->stream>>>(ctx->d_rec, ctx->d_tgt, n, d_x, nrhs, d_y, partial, fl);
             else
@@ -998,6 +1016,13 @@ int kemcu_create(kemcu_ctx** out, const kemcu_config* cfg)
     }
     KC(cudaMemcpyToSymbol(c_qp, qp.data(), qp.size() * sizeof(double)));
     KC(cudaMemcpyToSymbol(c_qc, qc, sizeof qc));
+    {
+        std::vector<float> q32(q.begin(), q.end()), qp32(qp.begin(), qp.end());
+        const float qc32[2] = {(float) qc[0], (float) qc[1]};
+        KC(cudaMemcpyToSymbol(c_q32, q32.data(), q32.size() * sizeof(float)));
+        KC(cudaMemcpyToSymbol(c_qp32, qp32.data(), qp32.size() * sizeof(float)));
+        KC(cudaMemcpyToSymbol(c_qc32, qc32, sizeof qc32));
+    }
     KC(cudaMemcpyToSymbol(c_gl, gl.data(), gl.size() * sizeof(double)));
     double ek[kEkTerms];
     ek_series_coefficients(ek);
@@ -1164,7 +1189,7 @@ int kemcu_field_dev(kemcu_ctx* ctx, const double* dP, size_t n, double* dout4, i
         return rc;
     if (n == 0)
         return KEMCU_OK;
-    if (!dP || !dout4 || n > (size_t) 0x7fffffff || (precision != KEMCU_FP64 && precision != KEMCU_MIXED) || what < 0 ||
+    if (!dP || !dout4 || n > (size_t) 0x7fffffff || precision < KEMCU_FP64 || precision > KEMCU_FP32 || what < 0 ||
         what > 2)
         return fail(ctx, KEMCU_EINVAL, "invalid field arguments");
     KC(cudaSetDevice(ctx->device));
@@ -1227,7 +1252,7 @@ int kemcu_field_dev_noalloc(kemcu_ctx* ctx, const double* dP, size_t n, double* 
         return rc;
     if (n == 0)
         return KEMCU_OK;
-    if (!dP || !dout4 || (precision != KEMCU_FP64 && precision != KEMCU_MIXED) || what < 0 || what > 2)
+    if (!dP || !dout4 || precision < KEMCU_FP64 || precision > KEMCU_FP32 || what < 0 || what > 2)
         return fail(ctx, KEMCU_EINVAL, "invalid field arguments");
     if (n > (size_t) KEMCU_NOALLOC_MAX_POINTS)
         return fail(ctx, KEMCU_EINVAL, "kemcu_field_dev_noalloc takes at most %u points (got %zu): its scratch is "
@@ -1374,11 +1399,16 @@ int kemcu_matvec(kemcu_ctx* ctx, const double* x, double* y, int n_rhs, int prec
     if ((rc = clear_pipe_flag(ctx)))
         return rc;
     Timer t(ctx);
-    int op = precision == KEMCU_MIXED ? kFreeMixed : kFree64;
+    if (precision < KEMCU_FP64 || precision > KEMCU_FP32)
+        return fail(ctx, KEMCU_EINVAL, "invalid matvec precision %d", precision);
+    // matrix-free: the entries in the requested form; assembled: the FP64 operator, or its FP32
+    // copy for the reduced forms
+    int op = precision == KEMCU_MIXED ? kFreeMixed : precision == KEMCU_FP32 ? kFree32 : kFree64;
     if (assembled) {
-        if ((rc = assemble(ctx, precision == KEMCU_MIXED)))
+        const bool low = precision != KEMCU_FP64;
+        if ((rc = assemble(ctx, low)))
             return rc;
-        op = precision == KEMCU_MIXED ? kDense32 : kDense64;
+        op = low ? kDense32 : kDense64;
     }
     if ((rc = apply_op(ctx, op, (const double*) dx, (double*) dy, n_rhs)))
         return rc;
@@ -1402,7 +1432,7 @@ int kemcu_gmres(kemcu_ctx* ctx, const double* b, double* x, int n_rhs, double re
     if (rc)
         return rc;
     if (!x || n_rhs < 1 || n_rhs > kMaxRhs || (b == nullptr && n_rhs != 1) || !(rel_tol > 0.) || max_iter < 1 ||
-        mode < 0 || mode > KEMCU_SOLVE_ASSEMBLED_FP64)
+        mode < 0 || mode > KEMCU_SOLVE_FP32)
         return fail(ctx, KEMCU_EINVAL, "invalid gmres arguments");
     KC(cudaSetDevice(ctx->device));
     if ((rc = clear_pipe_flag(ctx)))
@@ -1441,7 +1471,7 @@ int kemcu_gmres(kemcu_ctx* ctx, const double* b, double* x, int n_rhs, double re
         rel = est;
     }
     else {
-        int low_op = kFreeMixed, hi_op = kFree64;
+        int low_op = mode == KEMCU_SOLVE_FP32 ? kFree32 : kFreeMixed, hi_op = kFree64;
         if (mode == KEMCU_SOLVE_ASSEMBLED) {
             if ((rc = assemble(ctx, true)))
                 return rc;
