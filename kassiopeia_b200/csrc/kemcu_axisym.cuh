@@ -82,57 +82,22 @@ __device__ __forceinline__ double ell_K(double k)
     return kLn4 + sa - (0.5 + sb) * log(fabs(eta) + 1.e-19);
 }
 
-__device__ __forceinline__ double ell_E(double k)
-{
-    const double eta = sub(1., mul(k, k));  // as rounded on the host: eta can be tiny here
-    double en = eta, sc = 0., sd = 0.;
-    for (int i = 0; i < 10; i++) {
-        sc += c_cody_ec[i] * en;
-        sd += c_cody_ed[i] * en;
-        en *= eta;
-        if (en < 1.e-20)
-            break;
-    }
-    return 1. + sc - sd * log(fabs(eta) + 1.e-19);
-}
-
-// (E - K) / k^2: the difference of the two above for k^2 > 0.8, else the power series
-// sum_n (b_n - a_n) k^(2(n-1)) with a_n = (pi/2) prod_{m<=n} ((2m-1)/(2m))^2 and
-// b_n = -a_n / (2n - 1), summed until k^(2n) < 1e-16 (KEllipticIntegrals.cc:108-131). The
-// coefficients b_n - a_n do not depend on k: ek_series_coefficients() forms them once on the
-// host with the reference's recurrence and rounding (c_ek_coef), so each term costs one
-// multiply-add instead of two divisions. For k^2 <= 0.8 the sum stops by n = 166.
-constexpr int kEkTerms = 176;
-__constant__ double c_ek_coef[kEkTerms];
-
-inline void ek_series_coefficients(double* c)
-{
-    double a = 3.14159265358979323846 / 2.;
-    for (int n = 1; n <= kEkTerms; n++) {
-        const double cn = (2. * n - 1) / (2. * n);
-        a *= cn * cn;
-        const double b = -a / (2. * n - 1.);
-        c[n - 1] = b - a;
-    }
-}
-
-__device__ __forceinline__ double ell_EK(double k)
-{
-    const double k2 = k * k;
-    if (k2 > 0.8)
-        return (ell_E(k) - ell_K(k)) / k2;
-    double k2n = 1., ek = 0.;
-    for (int n = 0; n < kEkTerms; n++) {
-        ek += c_ek_coef[n] * k2n;
-        k2n *= k2;
-        if (k2n < 1.e-16)
-            break;
-    }
-    return ek;
-}
-
-// K(k), E(k) and (E - K) / k^2 together, each the value of the three functions above: one
-// logarithm serves both series and the k^2 > 0.8 branch of (E - K) / k^2 reuses them
+// K(k), E(k) and (E - K) / k^2 together; one logarithm serves both of Cody's series.
+//
+// (E - K) / k^2 is the difference of the two for k^2 > 0.8, as KEllipticIntegrals.cc:108-131
+// forms it (near the generator, where k -> 1, the integrand is sensitive to each rounding, and
+// this branch keeps the reference's). For k^2 <= 0.8 the reference sums the power series
+// sum_n (b_n - a_n) k^(2(n-1)) until k^(2n) < 1e-16: up to 166 terms, as many as the point's
+// distance requires, so the 32 points of a warp ran up to 5x the mean number of terms. Here
+// that branch comes from the arithmetic-geometric mean instead (Abramowitz & Stegun 17.6.3-4,
+// Gauss's method): with a_0 = 1, b_0 = k', c_0 = k, a_{n+1} = (a_n + b_n) / 2,
+// b_{n+1} = sqrt(a_n b_n) and c_{n+1} = c_n^2 / (4 a_{n+1}),
+//     E = K (1 - sum_{n>=0} 2^(n-1) c_n^2),   so   (E - K) / k^2 = -K (1/2 + sum_{n>=1} 2^(n-1) c_n^2 / k^2),
+// a sum of positive terms with no cancellation. For k^2 <= 0.8, c_4^2 < 1e-15 and c_5^2 < 1e-31:
+// four terms give the full double precision (4.4e-16 relative against a 40-digit evaluation
+// over [1e-12, 0.8], where the reference's series reaches 1.7e-15), a fixed cost of three square
+// roots and three divisions. c_4 uses a_3 for a_4 (their relative difference, c_4 / a_3 < 4e-8,
+// scales a term already below 1e-14 of the sum). K is Cody's, as in the potential.
 __device__ __forceinline__ void ell_KE_EK(double k, double& K, double& E, double& EK)
 {
     const double eta = sub(1., mul(k, k));
@@ -158,22 +123,19 @@ __device__ __forceinline__ void ell_KE_EK(double k, double& K, double& E, double
         EK = (E - K) / k2;
         return;
     }
-    // the same terms as ell_EK (a term is added while the power before it is >= 1e-16 after the
-    // previous one), even and odd terms on two power chains of stride k^4 so that neither the
-    // powers nor the sums form one serial chain; the two sums are added at the end
-    const double k4 = k2 * k2;
-    double pe = 1., po = k2, se = 0., so = 0.;
-    for (int n = 0; n + 1 < kEkTerms; n += 2) {
-        se += c_ek_coef[n] * pe;
-        if (po < 1.e-16)
-            break;
-        so += c_ek_coef[n + 1] * po;
-        pe *= k4;
-        po *= k4;
-        if (pe < 1.e-16)
-            break;
-    }
-    EK = se + so;
+    const double kp = sqrt(eta);
+    const double a1 = 0.5 * (1. + kp), b1 = sqrt(kp);
+    const double t1 = k2 / (16. * a1 * a1);  // c_1^2 / k^2
+    const double q1 = k2 * t1;               // c_1^2
+    const double a2 = 0.5 * (a1 + b1), b2 = sqrt(a1 * b1);
+    const double f2 = q1 / (16. * a2 * a2);  // c_2^2 / c_1^2
+    const double t2 = t1 * f2, q2 = q1 * f2;
+    const double a3 = 0.5 * (a2 + b2);
+    const double i3 = 1. / (16. * a3 * a3);
+    const double f3 = q2 * i3;
+    const double t3 = t2 * f3, q3 = q2 * f3;
+    const double t4 = t3 * (q3 * i3);
+    EK = -K * (0.5 + t1 + 2. * t2 + 4. * t3 + 8. * t4);
 }
 
 // evaluation point (z, r) and generator (za, ra) -> (zb, rb) of length len; the ring sits at
@@ -223,10 +185,11 @@ struct RingField
     __device__ __forceinline__ void operator()(double p, const AxPar& q, double* v) const
     {
         const RingGeom g = ring_at(p, q);
-        const double k = sqrt(1. - g.eta);
-        const double E = ell_E(k);
+        const double k = g.eta > 1. ? 0. : sqrt(1. - g.eta);  // eta <= 1 for r, R >= 0
+        double K, E, EK;
+        ell_KE_EK(k, K, E, EK);
         const double S3 = g.S * g.S * g.S;
-        v[0] = g.R / S3 * add(mul(mul(-2., g.R), ell_EK(k)), mul(g.dr / g.eta, E));
+        v[0] = g.R / S3 * add(mul(mul(-2., g.R), EK), mul(g.dr / g.eta, E));
         v[1] = g.dz / S3 * E / g.eta * g.R;
     }
 };
@@ -288,23 +251,25 @@ template<class F> __device__ void glueck_quad(const F& f, const AxPar& q, double
 // 35 pieces), the last piece of length h taken as h (ln 4 + ln(2 r + 1e-12) + 1 - ln h) / 2.
 // The reference adds that logarithmic remainder to both field components as well; so does
 // this code.
-template<class F> __device__ void conic_integral(const F& f, const AxPar& q, double* out)
+//
+// The three far bands share one inlined quadrature loop; the subdivided near branch, which few
+// pairs reach, is a separate (not inlined) function so that its loops do not raise the
+// register count of the far path.
+template<class F> __device__ __noinline__ void conic_near(const F& f, const AxPar& q, double* out);
+
+template<class F> __device__ __forceinline__ void conic_integral(const F& f, const AxPar& q, double* out)
 {
     const double Da = sqrt(add(mul(sub(q.za, q.z), sub(q.za, q.z)), mul(sub(q.ra, q.r), sub(q.ra, q.r))));
     const double Db = sqrt(add(mul(sub(q.zb, q.z), sub(q.zb, q.z)), mul(sub(q.rb, q.r), sub(q.rb, q.r))));
     const double D = fabs(sub(add(Da, Db), q.len)) / q.len;
-    if (D >= 5.e-2) {
-        glueck_quad(f, q, 0., q.len, 20, out);
-        return;
-    }
-    if (D >= 5.e-3) {
-        glueck_quad(f, q, 0., q.len, 100, out);
-        return;
-    }
-    if (D >= 5.e-4) {
-        glueck_quad(f, q, 0., q.len, 500, out);
-        return;
-    }
+    if (D >= 5.e-4)
+        glueck_quad(f, q, 0., q.len, D >= 5.e-2 ? 20 : D >= 5.e-3 ? 100 : 500, out);
+    else
+        conic_near(f, q, out);
+}
+
+template<class F> __device__ __noinline__ void conic_near(const F& f, const AxPar& q, double* out)
+{
     const double L = q.len;
     const double u0 = (q.zb - q.za) / L, u1 = (q.rb - q.ra) / L;
     const double pp = add(mul(sub(q.z, q.za), u0), mul(sub(q.r, q.ra), u1));
@@ -420,16 +385,18 @@ __device__ __forceinline__ void ax_field_potential(const double* e, double x, do
 }
 
 constexpr int kAxThreads = 128;
+// resident CTAs per SM the field kernel's registers are bounded for (96 registers a thread): on
+// the axisymmetric coax at 100,000 points, 216 ms against 224 ms at four CTAs and 264 ms
+// unbounded (154 registers, three CTAs); the local-memory spills this costs stay in L1
+constexpr int kAxFieldMinBlocks = 5;
 
 // direct sum over the elements [e0, e1) of split blockIdx.y at each point, compensated (Kahan)
 // over the elements as KIntegratingFieldSolver does (KElectrostaticIntegratingFieldSolver.hh:
 // 261-339); out n x 4, or partial[split][n][4] summed by reduce_splits in split order
 template<bool POT, bool FIELD>
-__global__ void __launch_bounds__(kAxThreads) axisym_field_kernel(const double* __restrict__ rec, int rec_stride,
-                                                                   const double* __restrict__ sigma, int ne,
-                                                                   const double* __restrict__ P, int np,
-                                                                   double* __restrict__ out,
-                                                                   double* __restrict__ partial)
+__global__ void __launch_bounds__(kAxThreads, kAxFieldMinBlocks)
+    axisym_field_kernel(const double* __restrict__ rec, int rec_stride, const double* __restrict__ sigma, int ne,
+                        const double* __restrict__ P, int np, double* __restrict__ out, double* __restrict__ partial)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np)
@@ -521,7 +488,7 @@ __global__ void __launch_bounds__(kAxThreads) axisym_assemble_kernel(const doubl
 inline int axisym_split(int num_sms, size_t rows, size_t cols)
 {
     const size_t blocks = (rows + kAxThreads - 1) / kAxThreads;
-    const size_t want = (size_t) num_sms * 5 * 4;
+    const size_t want = (size_t) num_sms * kAxFieldMinBlocks * 4;
     size_t split = blocks >= want ? 1 : (want + blocks - 1) / blocks;
     split = std::min(split, std::max((size_t) 1, cols / 8));
     return (int) std::min(split, (size_t) 65535);

@@ -809,6 +809,37 @@ __global__ void morton_kernel(const double* __restrict__ P, int n, const double*
     idx[i] = i;
 }
 
+// Morton keys in the meridian plane (r, z) for axisymmetric models: the work of a point depends
+// on its (r, z) only, so points of one warp that are close in (r, z) run the same ring
+// evaluations. r is scaled over [0, r_max] with r_max the corner of the bounding box's x-y
+// rectangle farthest from the axis.
+__device__ __forceinline__ unsigned long long spread2(unsigned v)
+{
+    unsigned long long x = v;
+    x = (x | x << 16) & 0x0000ffff0000ffffULL;
+    x = (x | x << 8) & 0x00ff00ff00ff00ffULL;
+    x = (x | x << 4) & 0x0f0f0f0f0f0f0f0fULL;
+    x = (x | x << 2) & 0x3333333333333333ULL;
+    x = (x | x << 1) & 0x5555555555555555ULL;
+    return x;
+}
+
+__global__ void morton_rz_kernel(const double* __restrict__ P, int n, const double* __restrict__ box,
+                                 unsigned long long* __restrict__ key, int* __restrict__ idx)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const double xm = fmax(fabs(box[0]), fabs(box[3])), ym = fmax(fabs(box[1]), fabs(box[4]));
+    const double rmax = sqrt(xm * xm + ym * ym), zext = box[5] - box[2];
+    const double r = sqrt(P[3 * i] * P[3 * i] + P[3 * i + 1] * P[3 * i + 1]);
+    const double tr = rmax > 0. ? r / rmax : 0., tz = zext > 0. ? (P[3 * i + 2] - box[2]) / zext : 0.;
+    const unsigned qr = (unsigned) fmin(fmax(tr * 2147483647.0, 0.), 2147483647.0);
+    const unsigned qz = (unsigned) fmin(fmax(tz * 2147483647.0, 0.), 2147483647.0);
+    key[i] = spread2(qr) | (spread2(qz) << 1);
+    idx[i] = i;
+}
+
 __global__ void gather_points_kernel(const double* __restrict__ P, const int* __restrict__ perm, int n,
                                      double* __restrict__ Q)
 {

@@ -1024,9 +1024,6 @@ int kemcu_create(kemcu_ctx** out, const kemcu_config* cfg)
         KC(cudaMemcpyToSymbol(c_qc32, qc32, sizeof qc32));
     }
     KC(cudaMemcpyToSymbol(c_gl, gl.data(), gl.size() * sizeof(double)));
-    double ek[kEkTerms];
-    ek_series_coefficients(ek);
-    KC(cudaMemcpyToSymbol(c_ek_coef, ek, sizeof ek));
     KC(cudaMemcpyToSymbol(c_k, &ctx->k, sizeof(Constants)));
     double rk[kStages][kStages];
     rk8_table(rk);
@@ -1199,7 +1196,8 @@ int kemcu_field_dev(kemcu_ctx* ctx, const double* dP, size_t n, double* dout4, i
             return rc;
     }
     else {
-        // Morton order: bbox -> keys -> radix sort -> gather -> evaluate -> scatter back
+        // Morton order (meridian plane for axisymmetric models): bbox -> keys -> radix sort -> gather ->
+        // evaluate -> scatter back
         const size_t cub_bytes = cub_sort_bytes(n);
         const size_t need = n * (2 * sizeof(unsigned long long) + 2 * sizeof(int) + 7 * sizeof(double)) + cub_bytes +
                             1024 + 128 * 6 * sizeof(double);
@@ -1223,7 +1221,10 @@ int kemcu_field_dev(kemcu_ctx* ctx, const double* dP, size_t n, double* dout4, i
         void* tmp = take(cub_bytes);
         bbox_kernel<<<128, 256, 0, ctx->stream>>>(dP, (int) n, part, ctx->d_counter + 32, box);
         KCHECK_LAUNCH();
-        morton_kernel<<<(unsigned) ((n + 255) / 256), 256, 0, ctx->stream>>>(dP, (int) n, box, k0, i0);
+        if (ctx->axisym)
+            morton_rz_kernel<<<(unsigned) ((n + 255) / 256), 256, 0, ctx->stream>>>(dP, (int) n, box, k0, i0);
+        else
+            morton_kernel<<<(unsigned) ((n + 255) / 256), 256, 0, ctx->stream>>>(dP, (int) n, box, k0, i0);
         KCHECK_LAUNCH();
         size_t tb = cub_bytes;
         KC(cub::DeviceRadixSort::SortPairs(tmp, tb, k0, k1, i0, i1, (int) n, 0, 63, ctx->stream));
