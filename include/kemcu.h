@@ -272,6 +272,58 @@ int kemcu_selftest_timeout(kemcu_ctx* ctx, int complete);
    2 flops per FMA), from independent dependent-FMA chains */
 int kemcu_fma_peak(kemcu_ctx* ctx, double* fp64_tflops, double* fp32_tflops);
 
+/* ---- fast multipole method (FFTM) for the field of planar elements ----
+   The reference's fast-multipole field solver (KFMElectrostaticFastMultipoleFieldSolver.cc:47-163
+   with the tree of KFMElectrostaticTreeConstructor.hh:44-87): a cubic tree over the world cube
+   (root divided top_level_divisions times per dimension, every further level `divisions` times,
+   down to level maximum_tree_depth); every element is owned by the deepest cell that contains
+   its bounding ball's centre and whose bounding ball, scaled by insertion_ratio, contains the
+   element's bounding ball (KFMInsertionCondition.hh:52-78); multipole moments of degree `degree`
+   about the owner cells, M2M up, M2L between the cells of each level that are not neighbours
+   (within `zeromask` cells) but whose parents are, L2L down; a point is the local expansion of
+   its leaf plus the direct sum over the elements owned by the neighbours of its leaf's
+   ancestors. Only divisions == 2 and zeromask == 1 are built. */
+typedef struct {
+    int degree;                     /* expansion degree p, 1..15 (KFMElectrostaticParameters::degree) */
+    int top_level_divisions;        /* divisions of the root per dimension, 1..8 */
+    int divisions;                  /* divisions of every further level per dimension (2) */
+    int zeromask;                   /* neighbour order: cells within it are summed directly (1) */
+    int maximum_tree_depth;         /* level of the leaves, 1..10 */
+    double insertion_ratio;         /* insertion condition's ratio (4/3) */
+    double region_expansion_factor; /* world cube side over the elements' extent (1.1) */
+    double world_center[3];         /* explicit world cube, used when world_length > 0 */
+    double world_length;
+    int near_analytic;              /* direct pairs by the analytic integrals (1, as the reference's
+                                       fast-multipole field solver: KEBIFactory::MakeAnalytic) or
+                                       by the numeric policy of kemcu_field (0) */
+} kemcu_fftm_params;
+void kemcu_fftm_default_params(kemcu_fftm_params* prm);
+/* builds the tree for the context's (planar) geometry; the charge densities are read at each
+   evaluation. Replaces the previous tree. */
+int kemcu_fftm_configure(kemcu_ctx* ctx, const kemcu_fftm_params* prm);
+/* field and potential at n points (host or device buffers, out4 as kemcu_field); points outside
+   the world cube are summed directly, as the reference falls back to its direct solver
+   (KFMElectrostaticFastMultipoleFieldSolver.cc:145-160) */
+int kemcu_fftm_field(kemcu_ctx* ctx, const double* P, size_t n, double* out4, int what);
+int kemcu_fftm_field_dev(kemcu_ctx* ctx, const double* dP, size_t n, double* dout4, int what);
+/* tree summary: world4 = world cube centre and side; counts = {cells with moments, elements
+   owned per level 0..maximum_tree_depth} (counts has room for 2 + maximum_tree_depth ints) */
+int kemcu_fftm_info(const kemcu_ctx* ctx, double* world4, int* counts);
+/* multipole moments of every element of the context, for unit total charge, about the origins
+   (n x 3), as KFMElectrostaticMultipoleCalculatorAnalytic::ConstructExpansion gives them:
+   out n x (degree+1)^2 complex (re, im) in the index l(l+1)+m */
+int kemcu_fm_moments(kemcu_ctx* ctx, int degree, const double* origins, double* out);
+/* potential and field of a local expansion about `origin` (coefficients for m >= 0,
+   (degree+1)(degree+2)/2 complex in the index l(l+1)/2+m, the reference's
+   KFMElectrostaticLocalCoefficientSet layout) at n points, times 1 / (4 pi eps0), as
+   KFMElectrostaticLocalCoefficientFieldCalculator evaluates it; out4 as kemcu_field */
+int kemcu_fm_local_field(kemcu_ctx* ctx, int degree, const double* origin, const double* coeff, size_t n,
+                         const double* P, double* out4);
+/* the translation response of `kind` (0 M2M, 1 M2L, 2 L2L) between two origins, as the
+   reference's KFMResponseKernel_3DLaplace* GetResponseFunction gives it: out
+   (degree+1)^2 x (degree+1)^2 complex, [target][source]; host arithmetic (no device) */
+int kemcu_fm_response(int kind, int degree, const double* source_origin, const double* target_origin, double* out);
+
 #ifdef __cplusplus
 }
 #endif

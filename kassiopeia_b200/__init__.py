@@ -238,6 +238,72 @@ class CUDAElectrostaticContext:
                                             C.byref(hit), precision, C.byref(ts), dpp))
         return st, steps, status, {k: getattr(ts, k) for k, _ in N.TrackStats._fields_}
 
+    # -- fast multipole method (KFMElectrostaticFastMultipoleFieldSolver)
+    def ConfigureFFTM(self, **params):
+        """Builds the fast-multipole tree for the current geometry. Keyword arguments are the
+        fields of kemcu_fftm_params (degree, top_level_divisions, divisions, zeromask,
+        maximum_tree_depth, insertion_ratio, region_expansion_factor, world_center,
+        world_length, near_analytic); the others keep their defaults."""
+        prm = N.FftmParams()
+        N.lib().kemcu_fftm_default_params(C.byref(prm))
+        for k, v in params.items():
+            if k == "world_center":
+                for i in range(3):
+                    prm.world_center[i] = float(v[i])
+            elif k in ("insertion_ratio", "region_expansion_factor", "world_length"):
+                setattr(prm, k, float(v))
+            else:
+                setattr(prm, k, int(v))
+        self._check(N.lib().kemcu_fftm_configure(self._h, C.byref(prm)))
+
+    def FFTMField(self, P, what=FIELD_AND_POTENTIAL):
+        """n x 4 (Ex, Ey, Ez, phi) by the fast multipole method."""
+        P = np.ascontiguousarray(P, np.float64).reshape(-1, 3)
+        out = np.zeros((P.shape[0], 4))
+        self._check(N.lib().kemcu_fftm_field(self._h, _d(P), P.shape[0], _d(out), what))
+        return out
+
+    def FFTMFieldDevice(self, d_points_ptr: int, n: int, d_out_ptr: int, what=FIELD_AND_POTENTIAL):
+        self._check(N.lib().kemcu_fftm_field_dev(self._h, C.c_void_p(d_points_ptr), n, C.c_void_p(d_out_ptr), what))
+
+    def FFTMInfo(self, depth: int) -> dict:
+        world = np.zeros(4)
+        counts = np.zeros(depth + 2, np.int32)
+        self._check(N.lib().kemcu_fftm_info(self._h, _d(world), _i(counts)))
+        return {"world_center": world[:3].copy(), "world_length": float(world[3]), "occupied_cells": int(counts[0]),
+                "owned_per_level": counts[1:].tolist()}
+
+    def MultipoleMoments(self, degree: int, origins):
+        """n x (degree+1)^2 complex moments of every element (unit total charge) about origins."""
+        o = np.ascontiguousarray(origins, np.float64).reshape(-1, 3)
+        S = (degree + 1) ** 2
+        out = np.zeros(2 * o.shape[0] * S)
+        self._check(N.lib().kemcu_fm_moments(self._h, degree, _d(o), _d(out)))
+        return (out[0::2] + 1j * out[1::2]).reshape(o.shape[0], S)
+
+    def LocalExpansionField(self, degree: int, origin, coeff, P):
+        """(Ex, Ey, Ez, phi) of a local expansion (m >= 0 coefficients, index l(l+1)/2+m) at P."""
+        c = np.zeros(2 * len(coeff))
+        c[0::2] = np.real(coeff)
+        c[1::2] = np.imag(coeff)
+        P = np.ascontiguousarray(P, np.float64).reshape(-1, 3)
+        out = np.zeros((P.shape[0], 4))
+        o = np.ascontiguousarray(origin, np.float64)
+        self._check(N.lib().kemcu_fm_local_field(self._h, degree, _d(o), _d(c), P.shape[0], _d(P), _d(out)))
+        return out
+
+    @staticmethod
+    def MultipoleResponse(kind: int, degree: int, source_origin, target_origin):
+        """[target, source] complex translation response (0 M2M, 1 M2L, 2 L2L), host arithmetic."""
+        S = (degree + 1) ** 2
+        out = np.zeros(2 * S * S)
+        so = np.ascontiguousarray(source_origin, np.float64)
+        to = np.ascontiguousarray(target_origin, np.float64)
+        rc = N.lib().kemcu_fm_response(kind, degree, _d(so), _d(to), _d(out))
+        if rc:
+            raise N.KemcuError(rc, "kemcu_fm_response")
+        return (out[0::2] + 1j * out[1::2]).reshape(S, S)
+
     # -- adjoint
     def FieldVJP(self, P, w, precision=FP64, want_sigma=True, want_vertices=True):
         """Adjoint of the direct sum: (dL/dsigma [N], dL/dvertices [N, 9]) for L = sum_p w_p . out_p."""

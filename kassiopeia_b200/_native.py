@@ -54,6 +54,13 @@ class TrackStats(C.Structure):
                 ("left", C.c_int), ("nonfinite", C.c_int), ("active", C.c_int), ("seconds", C.c_double)]
 
 
+class FftmParams(C.Structure):
+    _fields_ = [("degree", C.c_int), ("top_level_divisions", C.c_int), ("divisions", C.c_int),
+                ("zeromask", C.c_int), ("maximum_tree_depth", C.c_int), ("insertion_ratio", C.c_double),
+                ("region_expansion_factor", C.c_double), ("world_center", C.c_double * 3),
+                ("world_length", C.c_double), ("near_analytic", C.c_int)]
+
+
 ITER_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_double)
 
 _dp = C.POINTER(C.c_double)
@@ -132,5 +139,14 @@ def lib():
     L.kemcu_field_variant.argtypes = [vp, C.c_size_t, C.c_int, C.POINTER(C.c_int)]
     L.kemcu_field_variant_info.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.kemcu_field_variant_count.argtypes = []
+    L.kemcu_fftm_default_params.argtypes = [C.POINTER(FftmParams)]
+    L.kemcu_fftm_default_params.restype = None
+    L.kemcu_fftm_configure.argtypes = [vp, C.POINTER(FftmParams)]
+    L.kemcu_fftm_field.argtypes = [vp, _dp, C.c_size_t, _dp, C.c_int]
+    L.kemcu_fftm_field_dev.argtypes = [vp, C.c_void_p, C.c_size_t, C.c_void_p, C.c_int]
+    L.kemcu_fftm_info.argtypes = [vp, _dp, _ip]
+    L.kemcu_fm_moments.argtypes = [vp, C.c_int, _dp, _dp]
+    L.kemcu_fm_local_field.argtypes = [vp, C.c_int, _dp, _dp, C.c_size_t, _dp, _dp]
+    L.kemcu_fm_response.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp]
     _lib = L
     return L

@@ -12,6 +12,7 @@
 #include "kemcu_track.cuh"
 #include "kemcu_adjoint.cuh"
 #include "kemcu_robinhood.cuh"
+#include "kemcu_fftm.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 
@@ -39,6 +40,8 @@ struct DevBuf
     void* p = nullptr;
     size_t bytes = 0;
 };
+
+struct FmState;  // fast multipole tree and buffers (kemcu_fftm_host.inc)
 
 struct kemcu_ctx
 {
@@ -87,7 +90,10 @@ struct kemcu_ctx
     bool time_k1 = false;  // time the K1 launch of forced variants (kemcu_tune_field)
     int pending_key = -1, pending_variant = -1;
     cudaEvent_t tv0 = nullptr, tv1 = nullptr;
+    FmState* fm = nullptr;  // the fast multipole tree of the current geometry (kemcu_fftm_configure)
 };
+
+void fm_release(kemcu_ctx* ctx);
 
 namespace
 {
@@ -1051,6 +1057,7 @@ int kemcu_destroy(kemcu_ctx* ctx)
         cudaFree(ctx->d_near_val);
         cudaFree(ctx->d_counter);
         cudaFree(ctx->d_flag);
+        fm_release(ctx);
         cudaEventDestroy(ctx->ev0);
         cudaEventDestroy(ctx->ev1);
         cudaEventDestroy(ctx->tv0);
@@ -1108,6 +1115,7 @@ int kemcu_set_geometry(kemcu_ctx* ctx, size_t n, const int32_t* shape, const int
         return fail(ctx, KEMCU_EINVAL, "axisymmetric elements (conic sections, rings) cannot share a context with "
                                        "triangles, rectangles or line segments");
     // release everything that depends on the old geometry
+    fm_release(ctx);
     cudaFree(ctx->d_rec);
     cudaFree(ctx->d_tgt);
     cudaFree(ctx->d_sigma);
@@ -1644,3 +1652,4 @@ int kemcu_rule_nodes(int which, double* out)
 #include "kemcu_track_host.inc"
 #include "kemcu_adjoint_host.inc"
 #include "kemcu_robinhood_host.inc"
+#include "kemcu_fftm_host.inc"

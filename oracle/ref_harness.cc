@@ -160,6 +160,12 @@ void kemref_destroy(void* h)
     delete static_cast<RefCtx*>(h);
 }
 
+// the KSurfaceContainer of a handle (for fm_harness.cc, which builds the reference FFTM tree on it)
+void* kemref_container(void* h)
+{
+    return &static_cast<RefCtx*>(h)->container;
+}
+
 // The container groups elements by (boundary, shape) type in first-seen order
 // (KSurfaceContainer.cc:36-72), so its index i (the matrix row/column) need not be the
 // caller's index k. idx[k] receives the container index of caller element k.
