@@ -47,6 +47,13 @@ Fixtures:
                  perturbation leaves unchanged at every probe
   c5_rings       configuration 5 at its stated size (100,000 jittered triangles): 64 sampled
                  matrix rows, 64 entries each, and the rows of A x for 8 seeded right-hand sides
+  fftm           the reference's fast-multipole code (oracle/_ref/libkemref_fm.so, make -C oracle
+                 fm): analytic multipole moments (degree 10) of the mixed_small elements about
+                 seeded origins; a seeded degree-8 local expansion evaluated at 100 points; the
+                 M2M, M2L and L2L response matrices (degree 6) between fixed origins; and the
+                 FFTM field (KFMElectrostaticFastMultipoleFieldSolver, degree 8, divisions 2,
+                 zeromask 1, depths 3 and 4) of the coax_small density at 300 gap points, with
+                 the world cube it estimated
 
 Usage: python tests/golden/make_golden.py [fixture ...]   (default: all)
 """
@@ -461,8 +468,57 @@ def c5_rings():
          Ax=(A @ X.T).T, checksum=mesh_checksum(m))
 
 
+def element_vertices(m):
+    """vertex lists of planar elements as the reference's point clouds (KFMElectrostaticSurfaceConverter):
+    triangle P0, P0 + A N1, P0 + B N2; rectangle P0, P0 + A N1, P0 + A N1 + B N2, P0 + B N2; wire P0, P1"""
+    out = []
+    for k in range(m.n):
+        g = m.geom[k]
+        p0, n1, n2 = g[2:5], g[5:8], g[8:11]
+        if m.shape[k] == G.TRIANGLE:
+            out.append(np.array([p0, p0 + g[0] * n1, p0 + g[1] * n2]))
+        elif m.shape[k] == G.RECTANGLE:
+            out.append(np.array([p0, p0 + g[0] * n1, p0 + g[0] * n1 + g[1] * n2, p0 + g[1] * n2]))
+        else:
+            out.append(np.array([g[0:3], g[3:6]]))
+    return out
+
+
+def fftm():
+    from oracle import ref_fm
+
+    rng = np.random.default_rng(2040)
+    mx = golden_mesh("mixed_small")
+    origins = np.array([v.mean(axis=0) for v in element_vertices(mx)]) + rng.uniform(-0.1, 0.1, (mx.n, 3))
+    moments = np.array([ref_fm.moments(v, o, 10) for v, o in zip(element_vertices(mx), origins)])
+    deg = 8
+    coeff = np.array([complex(rng.standard_normal(), rng.standard_normal() if mm else 0.) * 0.6 ** l
+                      for l in range(deg + 1) for mm in range(l + 1)])
+    l2p_origin = np.array([0.1, -0.2, 0.15])
+    l2p_points = l2p_origin + rng.uniform(-0.7, 0.7, (100, 3))
+    l2p = ref_fm.l2p(deg, l2p_origin, coeff, l2p_points)
+    src, tgt, far = np.array([0.3, -0.2, 0.5]), np.array([-0.1, 0.4, 0.2]), np.array([2.1, 1.4, -1.7])
+    resp = np.array([ref_fm.response(0, 6, src, tgt), ref_fm.response(1, 6, src, far), ref_fm.response(2, 6, src, tgt)])
+    cx = golden_mesh("coax_small")
+    sigma = np.load(os.path.join(HERE, "coax_small.npz"))["sigma"]
+    pts = G.gap_points(300, seed=2041)
+    fr = ref_fm.FmRefProblem(cx)
+    fr.set_sigma(sigma)
+    f3, w3 = fr.field(pts, degree=8, maximum_tree_depth=3)
+    f4, w4 = fr.field(pts, degree=8, maximum_tree_depth=4)
+    save("fftm", mixed_origins=origins, mixed_moments=moments, l2p_degree=np.array(deg), l2p_coeff=coeff,
+         l2p_origin=l2p_origin, l2p_points=l2p_points, l2p=l2p, resp_src=src, resp_tgt=tgt, resp_far=far,
+         resp=resp, coax_points=pts, coax_field_d3=f3, coax_world_d3=w3, coax_field_d4=f4, coax_world_d4=w4)
+
+
+def golden_mesh(name):
+    from oracle.golden import mesh_from
+
+    return mesh_from(dict(np.load(os.path.join(HERE, name + ".npz"))))
+
+
 FIXTURES = {f.__name__: f for f in (rules, integrators, lines, icosphere, mixed_small, coax_small, rk8, adjoint,
-                                     robinhood, axisym, c1_sphere, c2_coax, c3_tracks, c4_adjoint, c5_rings)}
+                                     robinhood, axisym, c1_sphere, c2_coax, c3_tracks, c4_adjoint, c5_rings, fftm)}
 
 if __name__ == "__main__":
     for name in sys.argv[1:] or list(FIXTURES):

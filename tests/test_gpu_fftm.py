@@ -1,0 +1,154 @@
+"""Device fast-multipole method against the reference's own FFTM code: element moments, the
+local-expansion field, and the whole FFTM field (KFMElectrostaticFastMultipoleFieldSolver on
+the tree of KFMElectrostaticTreeConstructor, same parameters and world cube) on the
+coax_small density (fixture) and the 1,280-triangle sphere (live, oracle/_ref/libkemref_fm.so);
+points outside the world cube take the direct sum; the truncation error against the direct sum
+shrinks with the degree."""
+
+import numpy as np
+import pytest
+
+import kassiopeia_b200 as K
+from kassiopeia_b200 import geometry as G
+from oracle import golden, ref_fm
+from oracle.golden import mesh_from
+
+pytestmark = pytest.mark.gpu
+needs_ref_fm = pytest.mark.skipif(not ref_fm.available(), reason="oracle/_ref/libkemref_fm.so not built")
+
+
+def _vertices(m):
+    out = []
+    for k in range(m.n):
+        g = m.geom[k]
+        p0, n1, n2 = g[2:5], g[5:8], g[8:11]
+        if m.shape[k] == 0:
+            out.append(np.array([p0, p0 + g[0] * n1, p0 + g[1] * n2]))
+        elif m.shape[k] == 1:
+            out.append(np.array([p0, p0 + g[0] * n1, p0 + g[0] * n1 + g[1] * n2, p0 + g[1] * n2]))
+        else:
+            out.append(np.array([g[0:3], g[3:6]]))
+    return out
+
+
+def test_moments_equal_reference_fixture():
+    fx = golden.load("fftm")
+    m = mesh_from(golden.load("mixed_small"))
+    ctx = K.CUDAElectrostaticContext(0)
+    ctx.SetGeometry(m)
+    got = ctx.MultipoleMoments(10, fx["mixed_origins"])
+    want = fx["mixed_moments"]
+    for e in range(m.n):
+        assert np.abs(got[e] - want[e]).max() <= 1e-13 * np.abs(want[e]).max(), e
+
+
+@needs_ref_fm
+@pytest.mark.parametrize("degree", [2, 8, 15])
+def test_moments_equal_live_reference(degree):
+    rng = np.random.default_rng(degree)
+    m = G.icosphere(1).concat(mesh_from(golden.load("coax_small")))
+    sel = np.r_[0:80, 80:m.n:23]
+    ctx = K.CUDAElectrostaticContext(0)
+    ctx.SetGeometry(m)
+    origins = m.centroids() + rng.uniform(-0.2, 0.2, (m.n, 3))
+    got = ctx.MultipoleMoments(degree, origins)
+    verts = _vertices(m)
+    for e in sel:
+        want = ref_fm.moments(verts[e], origins[e], degree)
+        assert np.abs(got[e] - want).max() <= 2e-13 * np.abs(want).max(), e
+
+
+def test_local_field_equals_reference_fixture():
+    fx = golden.load("fftm")
+    ctx = K.CUDAElectrostaticContext(0)
+    ctx.SetGeometry(G.icosphere(1))
+    got = ctx.LocalExpansionField(int(fx["l2p_degree"]), fx["l2p_origin"], fx["l2p_coeff"], fx["l2p_points"])
+    want = fx["l2p"]
+    assert np.all(np.abs(got - want).max(axis=0) <= 1e-13 * np.abs(want).max(axis=0))
+
+
+@pytest.mark.parametrize("depth", [3, 4])
+def test_fftm_equals_reference_fftm_fixture(depth):
+    # the coax_small density (960 rectangles, 288 triangles): same degree, divisions, zeromask,
+    # depth, insertion ratio and world cube as the reference's tree
+    fx = golden.load("fftm")
+    cs = golden.load("coax_small")
+    ctx = K.CUDAElectrostaticContext(0)
+    ctx.SetGeometry(mesh_from(cs))
+    ctx.SetSigma(cs["sigma"])
+    w = fx[f"coax_world_d{depth}"]
+    ctx.ConfigureFFTM(degree=8, maximum_tree_depth=depth, world_center=w[:3], world_length=w[3])
+    got = ctx.FFTMField(fx["coax_points"])
+    want = fx[f"coax_field_d{depth}"]
+    scale = np.abs(want).max(axis=0)
+    err = np.abs(got - want).max(axis=0) / scale
+    # the gap potential is the difference of the two cylinders' much larger contributions, so
+    # rounding shows at ~6e-12 of the largest value (the field agrees to ~1e-13)
+    assert np.all(err[:3] <= 1e-11) and err[3] <= 2e-11, err
+
+
+@needs_ref_fm
+@pytest.mark.parametrize("depth", [2, 3, 4])
+def test_fftm_equals_live_reference_fftm_on_sphere(depth):
+    fx = golden.load("c1_sphere")
+    sph = G.icosphere(3)
+    rng = np.random.default_rng(3)
+    Q = rng.uniform(-1.0, 1.0, (6000, 3))
+    P = Q[np.abs(np.linalg.norm(Q, axis=1) - 1) > 0.08][:300]
+    fr = ref_fm.FmRefProblem(sph)
+    fr.set_sigma(fx["sigma_direct"])
+    want, world = fr.field(P, degree=8, maximum_tree_depth=depth)
+    ctx = K.CUDAElectrostaticContext(0)
+    ctx.SetGeometry(sph)
+    ctx.SetSigma(fx["sigma_direct"])
+    ctx.ConfigureFFTM(degree=8, maximum_tree_depth=depth, world_center=world[:3], world_length=world[3])
+    got = ctx.FFTMField(P)
+    err = np.abs(got - want).max(axis=0) / np.abs(want).max(axis=0)
+    assert np.all(err[:3] <= 1e-11) and err[3] <= 1e-13, err
+
+
+def test_fftm_points_outside_world_take_direct_sum():
+    fx = golden.load("c1_sphere")
+    ctx = K.CUDAElectrostaticContext(0)
+    ctx.SetGeometry(G.icosphere(3))
+    ctx.SetSigma(fx["sigma_direct"])
+    ctx.ConfigureFFTM(degree=6, maximum_tree_depth=3)
+    info = ctx.FFTMInfo(3)
+    P = fx["points"]
+    far = P[np.abs(P - info["world_center"]).max(axis=1) > 0.55 * info["world_length"]][:100]
+    assert len(far) >= 50
+    got = ctx.FFTMField(far)
+    want = ctx.ElectricFieldAndPotential(far)
+    assert np.abs(got - want).max() <= 1e-14 * np.abs(want).max()
+
+
+def test_fftm_error_falls_with_degree():
+    fx = golden.load("c1_sphere")
+    ctx = K.CUDAElectrostaticContext(0)
+    ctx.SetGeometry(G.icosphere(3))
+    ctx.SetSigma(fx["sigma_direct"])
+    rng = np.random.default_rng(8)
+    Q = rng.uniform(-1.0, 1.0, (4000, 3))
+    P = Q[np.abs(np.linalg.norm(Q, axis=1) - 1) > 0.08][:400]
+    direct = ctx.ElectricFieldAndPotential(P)
+    errs = []
+    for deg in (4, 8, 12):
+        ctx.ConfigureFFTM(degree=deg, maximum_tree_depth=3)
+        errs.append(np.abs(ctx.FFTMField(P) - direct).max() / np.abs(direct).max())
+    assert errs[0] > errs[1] > errs[2]
+    assert errs[1] < 5e-4 and errs[2] < 1e-4, errs
+
+
+def test_fftm_state_and_argument_errors():
+    ctx = K.CUDAElectrostaticContext(0)
+    ctx.SetGeometry(G.icosphere(1))
+    ctx.SetSigma(np.ones(80) * 1e-9)
+    with pytest.raises(K.KemcuError):
+        ctx.FFTMField(np.zeros((4, 3)))  # not configured
+    for bad in ({"divisions": 3}, {"zeromask": 2}, {"degree": 0}, {"degree": 16}, {"maximum_tree_depth": 11}):
+        with pytest.raises(K.KemcuError):
+            ctx.ConfigureFFTM(**bad)
+    ax = K.CUDAElectrostaticContext(0)
+    ax.SetGeometry(G.conic_sphere(20))
+    with pytest.raises(K.KemcuError):
+        ax.ConfigureFFTM()
