@@ -79,9 +79,14 @@ enum kemcu_solve_mode {
     KEMCU_SOLVE_ASSEMBLED_FP64 = 3, /* GMRES on the assembled FP64 operator alone (no FP32 copy,
                                   no refinement): the plain algorithm with the same assembly,
                                   which separates the gain of assembly from that of precision */
-    KEMCU_SOLVE_FP32 = 4       /* iterative refinement, matrix-free: inner GMRES on the FP32
+    KEMCU_SOLVE_FP32 = 4,      /* iterative refinement, matrix-free: inner GMRES on the FP32
                                   far-field operator (KEMCU_FP32), FP64 matrix-free residual and
                                   correction; FP64-accurate charge densities */
+    KEMCU_SOLVE_FFTM = 5       /* GMRES on the fast multipole operator of kemcu_fftm_configure
+                                  (the operator of KKrylovChargeDensitySolver with
+                                  KFastMultipoleMatrixGenerator): the residual is the FFTM
+                                  operator's, whose entries differ from the direct ones by the
+                                  expansion's truncation error */
 };
 
 typedef struct kemcu_ctx kemcu_ctx;
@@ -306,6 +311,11 @@ int kemcu_fftm_configure(kemcu_ctx* ctx, const kemcu_fftm_params* prm);
    (KFMElectrostaticFastMultipoleFieldSolver.cc:145-160) */
 int kemcu_fftm_field(kemcu_ctx* ctx, const double* P, size_t n, double* out4, int what);
 int kemcu_fftm_field_dev(kemcu_ctx* ctx, const double* dP, size_t n, double* dout4, int what);
+/* y = A x with the fast multipole operator (KFastMultipoleMatrixGenerator, KFastMultipoleMatrixGenerator.cc:
+   23-41): the local expansion of the leaf holding each row's collocation point (potential, or
+   field along the normal for a Neumann row) plus the direct entries, by the numeric policy as
+   kemcu_matvec, of the elements owned by the neighbours of that leaf's ancestors; x, y n_rhs x n */
+int kemcu_fftm_matvec(kemcu_ctx* ctx, const double* x, double* y, int n_rhs);
 /* tree summary: world4 = world cube centre and side; counts = {cells with moments, elements
    owned per level 0..maximum_tree_depth} (counts has room for 2 + maximum_tree_depth ints) */
 int kemcu_fftm_info(const kemcu_ctx* ctx, double* world4, int* counts);

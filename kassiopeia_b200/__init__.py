@@ -24,10 +24,10 @@ import numpy as np
 
 from . import _native as N
 from ._native import (FIELD, FIELD_AND_POTENTIAL, FP32, FP64, MIXED, POTENTIAL, SOLVE_ASSEMBLED, SOLVE_ASSEMBLED_FP64,
-                      SOLVE_FP32, SOLVE_MIXED, SOLVE_PLAIN, KemcuError)
+                      SOLVE_FFTM, SOLVE_FP32, SOLVE_MIXED, SOLVE_PLAIN, KemcuError)
 
 __all__ = ["CUDAElectrostaticContext", "KemcuError", "FP64", "MIXED", "FP32", "SOLVE_PLAIN", "SOLVE_MIXED",
-           "SOLVE_ASSEMBLED", "SOLVE_ASSEMBLED_FP64", "SOLVE_FP32", "FIELD_AND_POTENTIAL", "POTENTIAL", "FIELD"]
+           "SOLVE_ASSEMBLED", "SOLVE_ASSEMBLED_FP64", "SOLVE_FP32", "SOLVE_FFTM", "FIELD_AND_POTENTIAL", "POTENTIAL", "FIELD"]
 
 ONE_OVER_FOUR_PI_EPS0 = 1.0 / (4.0 * np.pi * 8.8541878128e-12)  # KEMConstants (KConst epoch 2021)
 EPS0 = 8.8541878128e-12
@@ -262,6 +262,14 @@ class CUDAElectrostaticContext:
         out = np.zeros((P.shape[0], 4))
         self._check(N.lib().kemcu_fftm_field(self._h, _d(P), P.shape[0], _d(out), what))
         return out
+
+    def FFTMMultiply(self, x):
+        """A x by the fast multipole operator (x: n, or n_rhs x n)."""
+        x = np.ascontiguousarray(x, np.float64)
+        nr = 1 if x.ndim == 1 else x.shape[0]
+        y = np.zeros_like(x)
+        self._check(N.lib().kemcu_fftm_matvec(self._h, _d(x), _d(y), nr))
+        return y
 
     def FFTMFieldDevice(self, d_points_ptr: int, n: int, d_out_ptr: int, what=FIELD_AND_POTENTIAL):
         self._check(N.lib().kemcu_fftm_field_dev(self._h, C.c_void_p(d_points_ptr), n, C.c_void_p(d_out_ptr), what))

@@ -17,7 +17,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "kemcu.h")
 OK, EINVAL, ECUDA, ENONFINITE, ENOTCONVERGED, ETIMEOUT, ENOMEM, ESTATE = 0, -1, -2, -3, -4, -5, -6, -7
 FP64, MIXED, FP32 = 0, 1, 2
 FIELD_AND_POTENTIAL, POTENTIAL, FIELD = 0, 1, 2
-SOLVE_PLAIN, SOLVE_MIXED, SOLVE_ASSEMBLED, SOLVE_ASSEMBLED_FP64, SOLVE_FP32 = 0, 1, 2, 3, 4
+SOLVE_PLAIN, SOLVE_MIXED, SOLVE_ASSEMBLED, SOLVE_ASSEMBLED_FP64, SOLVE_FP32, SOLVE_FFTM = 0, 1, 2, 3, 4, 5
 TRACK_ACTIVE, TRACK_HIT, TRACK_MAX_STEPS, TRACK_LEFT, TRACK_NONFINITE = 0, 1, 2, 3, 4
 
 _ERRNAMES = {EINVAL: "EINVAL", ECUDA: "ECUDA", ENONFINITE: "ENONFINITE", ENOTCONVERGED: "ENOTCONVERGED",
@@ -145,6 +145,7 @@ def lib():
     L.kemcu_fftm_field.argtypes = [vp, _dp, C.c_size_t, _dp, C.c_int]
     L.kemcu_fftm_field_dev.argtypes = [vp, C.c_void_p, C.c_size_t, C.c_void_p, C.c_int]
     L.kemcu_fftm_info.argtypes = [vp, _dp, _ip]
+    L.kemcu_fftm_matvec.argtypes = [vp, _dp, _dp, C.c_int]
     L.kemcu_fm_moments.argtypes = [vp, C.c_int, _dp, _dp]
     L.kemcu_fm_local_field.argtypes = [vp, C.c_int, _dp, _dp, C.c_size_t, _dp, _dp]
     L.kemcu_fm_response.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp]

@@ -447,6 +447,67 @@ __global__ void __launch_bounds__(128) fm_eval_kernel(const double* __restrict__
     }
 }
 
+// FFTM matrix-vector product (the reference's KFastMultipoleMatrixGenerator: the dense part from
+// the local expansions, KFMElectrostaticBoundaryIntegrator.hh:355-386, the sparse part from the
+// default numeric integrator on the direct-call lists): row t of y is the local expansion of the
+// leaf holding element t's collocation point (its potential, or for a Neumann row its field
+// along the normal) plus the matrix entries entry() of the elements owned by the neighbours of
+// the leaf's ancestors times x, in the order of fm_eval_kernel. One CTA per run of targets
+// sorted by leaf (tgt_order lists the elements).
+__global__ void __launch_bounds__(128) fm_matvec_kernel(const double* __restrict__ rec,
+                                                        const TargetRec* __restrict__ tgt,
+                                                        const int* __restrict__ tgt_order,
+                                                        const int* __restrict__ run_key, const int* __restrict__ run_off,
+                                                        const int* __restrict__ run_cnt, FmTreeView T, int p,
+                                                        const double* __restrict__ Lx, const double* __restrict__ x,
+                                                        double* __restrict__ y)
+{
+    extern __shared__ double fm_x[];
+    const int b = blockIdx.x;
+    const int key = run_key[b] - 1;
+    const int off = run_off[b], cnt = run_cnt[b];
+    const int K = (p + 1) * (p + 1);
+    const FmLevel& Ld = T.lv[T.depth];
+    for (int i = threadIdx.x; i < K; i += blockDim.x)
+        fm_x[i] = Lx[(Ld.base + key) * K + i];
+    __syncthreads();
+    const int lz = key % Ld.n, ly = (key / Ld.n) % Ld.n, lx = key / (Ld.n * Ld.n);
+    const double cx = T.wx + (lx + .5) * Ld.side, cy = T.wy + (ly + .5) * Ld.side, cz = T.wz + (lz + .5) * Ld.side;
+    const double inv_side = 1. / Ld.side;
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+        const int ti = tgt_order[off + k];
+        const TargetRec t = tgt[ti];
+        const V3 C = v3(t.cen[0], t.cen[1], t.cen[2]);
+        double far[4];
+        fm_l2p(fm_x, p, (C.x - cx) * inv_side, (C.y - cy) * inv_side, (C.z - cz) * inv_side, inv_side, far);
+        const double fv = t.neumann == 0. ? far[3] : far[0] * t.normal[0] + far[1] * t.normal[1] + far[2] * t.normal[2];
+        double s = 0., c = 0.;
+        for (int l = 0; l <= T.depth; l++) {
+            const FmLevel& L = T.lv[l];
+            int ax = lx, ay = ly, az = lz;
+            for (int q = T.depth; q > l; q--) {
+                ax /= T.lv[q].div;
+                ay /= T.lv[q].div;
+                az /= T.lv[q].div;
+            }
+            for (int sx = max(0, ax - T.zm); sx <= min(L.n - 1, ax + T.zm); sx++)
+                for (int sy = max(0, ay - T.zm); sy <= min(L.n - 1, ay + T.zm); sy++)
+                    for (int sz = max(0, az - T.zm); sz <= min(L.n - 1, az + T.zm); sz++) {
+                        const long long ci = fm_cell(L, sx, sy, sz);
+                        const int e0 = T.own_ptr[ci], e1 = T.own_ptr[ci + 1];
+                        for (int j = e0; j < e1; j++) {
+                            const int e = T.own_elem[j];
+                            const double yk = entry<false>(rec + (size_t) e * rRecSize, t, C) * x[e] - c;
+                            const double tt = s + yk;
+                            c = (tt - s) - yk;
+                            s = tt;
+                        }
+                    }
+        }
+        y[ti] = s + fv;
+    }
+}
+
 // leaf key (leaf index + 1, or 0 outside the world cube) and index of every point
 __global__ void fm_leaf_kernel(const double* __restrict__ P, int n, double wx, double wy, double wz, double side,
                                int nd, int* __restrict__ key, int* __restrict__ idx)

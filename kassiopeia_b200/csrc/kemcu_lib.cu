@@ -94,6 +94,7 @@ struct kemcu_ctx
 };
 
 void fm_release(kemcu_ctx* ctx);
+int fm_apply(kemcu_ctx* ctx, const double* d_x, double* d_y, int nrhs);
 
 namespace
 {
@@ -579,12 +580,15 @@ enum OpKind
     kFreeMixed,
     kDense64,
     kDense32,
-    kFree32  // matrix-free with the FP32 far-field form
+    kFree32,  // matrix-free with the FP32 far-field form
+    kFftm     // the fast multipole operator (kemcu_fftm_configure)
 };
 
 int apply_op(kemcu_ctx* ctx, int op, const double* d_x, double* d_y, int nrhs)
 {
     const int n = (int) ctx->n;
+    if (op == kFftm)
+        return fm_apply(ctx, d_x, d_y, nrhs);
     if ((op == kFree64 || op == kFreeMixed || op == kFree32) && ctx->axisym) {
         const int split = axisym_split(ctx->num_sms, n, n);
         double* partial = nullptr;
@@ -1441,8 +1445,10 @@ int kemcu_gmres(kemcu_ctx* ctx, const double* b, double* x, int n_rhs, double re
     if (rc)
         return rc;
     if (!x || n_rhs < 1 || n_rhs > kMaxRhs || (b == nullptr && n_rhs != 1) || !(rel_tol > 0.) || max_iter < 1 ||
-        mode < 0 || mode > KEMCU_SOLVE_FP32)
+        mode < 0 || mode > KEMCU_SOLVE_FFTM)
         return fail(ctx, KEMCU_EINVAL, "invalid gmres arguments");
+    if (mode == KEMCU_SOLVE_FFTM && !ctx->fm)
+        return fail(ctx, KEMCU_ESTATE, "KEMCU_SOLVE_FFTM needs kemcu_fftm_configure first");
     KC(cudaSetDevice(ctx->device));
     if ((rc = clear_pipe_flag(ctx)))
         return rc;
@@ -1467,8 +1473,8 @@ int kemcu_gmres(kemcu_ctx* ctx, const double* b, double* x, int n_rhs, double re
     auto t0 = std::chrono::steady_clock::now();
     int iters = 0, fp64 = 0, low = 0;
     double est = 0., rel = 0.;
-    if (mode == KEMCU_SOLVE_PLAIN || mode == KEMCU_SOLVE_ASSEMBLED_FP64) {
-        int op = kFree64;
+    if (mode == KEMCU_SOLVE_PLAIN || mode == KEMCU_SOLVE_ASSEMBLED_FP64 || mode == KEMCU_SOLVE_FFTM) {
+        int op = mode == KEMCU_SOLVE_FFTM ? kFftm : kFree64;
         if (mode == KEMCU_SOLVE_ASSEMBLED_FP64) {
             if ((rc = assemble(ctx, false)))
                 return rc;

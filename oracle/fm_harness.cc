@@ -11,6 +11,10 @@
 //   kemref_fm_response   the M2M, M2L and L2L response functions of the 3D Laplace kernel
 //                        (KFMResponseKernel_3DLaplaceM2M.cc, ...M2L.cc, ...L2L.cc) between two
 //                        origins, as a dense (degree+1)^2 x (degree+1)^2 complex matrix
+//   kemref_fm_matvec     y = A x with the reference's fast-multipole matrix (KFastMultipoleMatrixGenerator,
+//                        KFastMultipoleMatrixGenerator.cc:23-41: dense far part from the local
+//                        expansions, sparse near part by the numeric integrator), x and y in
+//                        container order
 //   kemref_fm_field      the whole reference FFTM field solver on a container made by
 //                        ref_harness.cc's kemref_create: KFMElectrostaticTreeConstructor with the
 //                        single-threaded field mapper, then KFMElectrostaticFastMultipoleFieldSolver
@@ -26,9 +30,15 @@
 #include "KFMResponseKernel_3DLaplaceL2L.hh"
 #include "KFMResponseKernel_3DLaplaceM2L.hh"
 #include "KFMResponseKernel_3DLaplaceM2M.hh"
+#include "KEMFileInterface.hh"
+#include "KFastMultipoleMatrixGenerator.hh"
+#include "KSimpleVector.hh"
 #include "KSurfaceContainer.hh"
 
 #include <complex>
+#include <cstdlib>
+#include <filesystem>
+#include <string>
 #include <vector>
 
 using namespace KEMField;
@@ -126,6 +136,42 @@ int kemref_fm_response(int kind, int degree, const double* source_origin, const 
             out[2 * (t * S + s)] = v.real();
             out[2 * (t * S + s) + 1] = v.imag();
         }
+    return 0;
+}
+
+// ip, dp as kemref_fm_field; the matrix's tree estimates its world cube the same way. The sparse
+// part keeps its blocks in files of KEMFileInterface's active directory: a temporary directory,
+// removed afterwards.
+int kemref_fm_matvec(void* h, const int* ip, const double* dp, const double* x, double* y)
+{
+    auto* container = static_cast<KSurfaceContainer*>(kemref_container(h));
+    char tmpl[] = "/tmp/kemref_fmXXXXXX";
+    if (!mkdtemp(tmpl))
+        return -1;
+    const std::string dir(tmpl);
+    KEMFileInterface::GetInstance()->ActiveDirectory(dir);
+    KFastMultipoleMatrixGenerator gen;
+    gen.SetStrategy(KFMSubdivisionStrategy::Aggressive);
+    gen.SetDegree(ip[0]);
+    gen.SetTopLevelDivisions(ip[1]);
+    gen.SetDivisions(ip[2]);
+    gen.SetZeromask(ip[3]);
+    gen.SetMaximumTreeDepth(ip[4]);
+    gen.SetInsertionRatio(dp[0]);
+    gen.SetRegionExpansionFactor(dp[1]);
+    gen.SetUseRegionEstimation(true);
+    gen.SetUseCaching(false);
+    gen.SetVerbosity(0);
+    auto A = gen.Build(*container);
+    const unsigned n = container->size();
+    KSimpleVector<double> xv(n), yv(n);
+    for (unsigned i = 0; i < n; i++)
+        xv[i] = x[i];
+    A->Multiply(xv, yv);
+    for (unsigned i = 0; i < n; i++)
+        y[i] = yv[i];
+    A.reset();
+    std::filesystem::remove_all(dir);
     return 0;
 }
 

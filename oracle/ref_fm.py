@@ -40,6 +40,7 @@ def lib():
         L.kemref_fm_l2p.argtypes = [C.c_int, _dp, C.c_double, _dp, C.c_int, _dp, _dp]
         L.kemref_fm_response.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp]
         L.kemref_fm_field.argtypes = [C.c_void_p, _ip, _dp, C.c_int, _dp, _dp, _dp]
+        L.kemref_fm_matvec.argtypes = [C.c_void_p, _ip, _dp, _dp, _dp]
         _lib = L
     return _lib
 
@@ -114,6 +115,19 @@ class FmRefProblem:
         s[self.cidx] = np.asarray(sigma, np.float64)
         s = _c(s)
         lib().kemref_set_sigma(self.h, _d(s))
+
+    def matvec(self, x, degree=8, top_level_divisions=2, divisions=2, zeromask=1, maximum_tree_depth=3,
+               insertion_ratio=4.0 / 3.0, region_expansion_factor=1.1):
+        """A x with the reference's fast-multipole matrix (caller order)."""
+        ipar = np.ascontiguousarray([degree, top_level_divisions, divisions, zeromask, maximum_tree_depth],
+                                    np.int32)
+        dpar = _c([insertion_ratio, region_expansion_factor])
+        xc = np.empty(self.n)
+        xc[self.cidx] = np.asarray(x, np.float64)
+        xc = _c(xc)
+        yc = np.zeros(self.n)
+        lib().kemref_fm_matvec(self.h, ipar.ctypes.data_as(_ip), _d(dpar), _d(xc), _d(yc))
+        return np.ascontiguousarray(yc[self.cidx])
 
     def field(self, P, degree=8, top_level_divisions=2, divisions=2, zeromask=1, maximum_tree_depth=3,
               insertion_ratio=4.0 / 3.0, region_expansion_factor=1.1):

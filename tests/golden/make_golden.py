@@ -53,7 +53,10 @@ Fixtures:
                  M2M, M2L and L2L response matrices (degree 6) between fixed origins; and the
                  FFTM field (KFMElectrostaticFastMultipoleFieldSolver, degree 8, divisions 2,
                  zeromask 1, depths 3 and 4) of the coax_small density at 300 gap points, with
-                 the world cube it estimated
+                 the world cube it estimated; the fast-multipole matrix
+                 (KFastMultipoleMatrixGenerator, degree 8, depth 3) times the coax_small density
+                 and times a seeded vector on mixed_small (Neumann rows and wires), with the world
+                 cubes of those trees
 
 Usage: python tests/golden/make_golden.py [fixture ...]   (default: all)
 """
@@ -506,9 +509,15 @@ def fftm():
     fr.set_sigma(sigma)
     f3, w3 = fr.field(pts, degree=8, maximum_tree_depth=3)
     f4, w4 = fr.field(pts, degree=8, maximum_tree_depth=4)
+    coax_Ax = fr.matvec(sigma, degree=8, maximum_tree_depth=3)
+    fm = ref_fm.FmRefProblem(mx)
+    xv = np.load(os.path.join(HERE, "mixed_small.npz"))["xv"]
+    mixed_Ax = fm.matvec(xv, degree=8, maximum_tree_depth=3)
+    _, mixed_world = fm.field(np.zeros((1, 3)), degree=8, maximum_tree_depth=3)
     save("fftm", mixed_origins=origins, mixed_moments=moments, l2p_degree=np.array(deg), l2p_coeff=coeff,
          l2p_origin=l2p_origin, l2p_points=l2p_points, l2p=l2p, resp_src=src, resp_tgt=tgt, resp_far=far,
-         resp=resp, coax_points=pts, coax_field_d3=f3, coax_world_d3=w3, coax_field_d4=f4, coax_world_d4=w4)
+         resp=resp, coax_points=pts, coax_field_d3=f3, coax_world_d3=w3, coax_field_d4=f4, coax_world_d4=w4,
+         coax_Ax_d3=coax_Ax, mixed_Ax_d3=mixed_Ax, mixed_world_d3=mixed_world)
 
 
 def golden_mesh(name):

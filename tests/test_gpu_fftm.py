@@ -152,3 +152,51 @@ def test_fftm_state_and_argument_errors():
     ax.SetGeometry(G.conic_sphere(20))
     with pytest.raises(K.KemcuError):
         ax.ConfigureFFTM()
+
+
+@pytest.mark.parametrize("case", ["coax_small", "mixed_small"])
+def test_fftm_matvec_equals_reference_fixture(case):
+    # KFastMultipoleMatrixGenerator's matrix (dense far part from the local expansions, sparse near
+    # part by the numeric integrator) times a vector: Dirichlet rows (coax), Neumann rows and
+    # wires (mixed)
+    fx = golden.load("fftm")
+    g = golden.load(case)
+    x = g["sigma"] if case == "coax_small" else g["xv"]
+    w = fx["coax_world_d3" if case == "coax_small" else "mixed_world_d3"]
+    want = fx["coax_Ax_d3" if case == "coax_small" else "mixed_Ax_d3"]
+    ctx = K.CUDAElectrostaticContext(0)
+    ctx.SetGeometry(mesh_from(g))
+    ctx.ConfigureFFTM(degree=8, maximum_tree_depth=3, world_center=w[:3], world_length=w[3])
+    got = ctx.FFTMMultiply(x)
+    assert np.abs(got - want).max() <= 1e-11 * np.abs(want).max()
+
+
+@needs_ref_fm
+def test_fftm_matvec_equals_live_reference_on_sphere():
+    fx = golden.load("c1_sphere")
+    sph = G.icosphere(3)
+    fr = ref_fm.FmRefProblem(sph)
+    want = fr.matvec(fx["sigma_direct"], degree=8, maximum_tree_depth=3)
+    _, world = fr.field(np.zeros((1, 3)), degree=8, maximum_tree_depth=3)
+    ctx = K.CUDAElectrostaticContext(0)
+    ctx.SetGeometry(sph)
+    ctx.ConfigureFFTM(degree=8, maximum_tree_depth=3, world_center=world[:3], world_length=world[3])
+    got = ctx.FFTMMultiply(fx["sigma_direct"])
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+    # and the FFTM operator is the direct one to its truncation error
+    direct = ctx.Multiply(fx["sigma_direct"])
+    assert np.abs(got - direct).max() <= 2e-5 * np.abs(direct).max()
+
+
+def test_fftm_solve_reaches_direct_density():
+    # GMRES on the fast-multipole operator (KKrylovChargeDensitySolver with
+    # KFastMultipoleMatrixGenerator): its residual is the FFTM operator's; the density differs from
+    # the direct solution by the operator's truncation error
+    fx = golden.load("c1_sphere")
+    ctx = K.CUDAElectrostaticContext(0)
+    ctx.SetGeometry(G.icosphere(3))
+    ctx.ConfigureFFTM(degree=10, maximum_tree_depth=3)
+    sigma, st = ctx.Solve(tol=1e-10, mode=K.SOLVE_FFTM)
+    assert st["rel_residual"] <= 1e-10
+    ref = fx["sigma_direct"]
+    assert np.abs(sigma - ref).max() <= 1e-4 * np.abs(ref).max()
