@@ -116,6 +116,30 @@ def cpu_reference_rate(mesh, sigma, pts, workers, seconds_target=12.0):
             sample, values)
 
 
+def reference_fftm_rate(mesh, sigma, P, degree=8, depth=5):
+    """one-core timing of the reference FFTM field solver (tree build, field mapping, evaluation)
+    on 200 and 2,000 of the gap points; None where oracle/_ref/libkemref_fm.so is not built"""
+    try:
+        from oracle import ref_fm
+    except ImportError:
+        return None
+    if not ref_fm.available():
+        return None
+    fr = ref_fm.FmRefProblem(mesh)
+    fr.set_sigma(sigma)
+    t = []
+    for n in (200, 2000):
+        t0 = time.perf_counter()
+        fr.field(P[:n], degree=degree, maximum_tree_depth=depth)
+        t.append(time.perf_counter() - t0)
+    per_point = max(t[1] - t[0], 1e-9) / 1800
+    fr.close()
+    return {"setup_s": t[0] - 200 * per_point, "evaluation_points_per_s": 1.0 / per_point, "cores": 1,
+            "parameters": f"degree {degree}, divisions 2, zeromask 1, depth {depth}, insertion ratio 4/3",
+            "sample": "tree + field map, then 200 and 2,000 gap points (two calls)",
+            "points_per_s_1M_incl_setup": 1e6 / (t[0] - 200 * per_point + 1e6 * per_point)}
+
+
 def accuracy_vs(out, ref):
     """max per-point relative error of |E| and of phi, and max error relative to the largest
     value of each quantity"""
@@ -360,6 +384,40 @@ def run_native(args, rank, world, dist):
             Os = torch.empty((100_000, 4), dtype=torch.float64, device="cuda")
             v, ms = sc.TuneField(Ps.data_ptr(), 100_000, Os.data_ptr(), precision=K.MIXED)
             extra["autotune_sphere20k_100k_points_mixed"] = {**sc.FieldVariantInfo(v), "k1_ms_per_shape": ms}
+        # the fast multipole method (the reference's FFTM, KFMElectrostaticFastMultipoleFieldSolver
+        # and KFastMultipoleMatrixGenerator) on the benched coax density: field at the 1,000,000
+        # gap points (device-resident, as the value above), its accuracy against the FP64 direct
+        # sum, and GMRES on the FFTM operator
+        fm = {}
+        for deg, depth in ((8, 5), (10, 5)):
+            t0 = time.perf_counter()
+            ctx.ConfigureFFTM(degree=deg, maximum_tree_depth=depth)
+            build_s = time.perf_counter() - t0
+            ctx.FFTMFieldDevice(dP.data_ptr(), N_POINTS, dOut.data_ptr())
+            ms = []
+            for _ in range(max(1, args.steps)):
+                ctx.FFTMFieldDevice(dP.data_ptr(), N_POINTS, dOut.data_ptr())
+                ms.append(ctx.last_kernel_ms)
+            acc = accuracy_vs(ctx.FFTMField(sub), o64)
+            info = ctx.FFTMInfo(depth)
+            fm[f"degree{deg}_depth{depth}"] = {
+                "tree_build_s": build_s, "ms_per_1M_points": float(np.median(ms)),
+                "points_per_s": N_POINTS / (float(np.median(ms)) * 1e-3),
+                "speedup_over_mixed_direct": (ms_mixed / args.steps) / float(np.median(ms)),
+                "accuracy_vs_fp64_direct": acc, "world_length": info["world_length"],
+                "occupied_cells": info["occupied_cells"], "elements_owned_per_level": info["owned_per_level"]}
+        ctx.ConfigureFFTM(degree=8, maximum_tree_depth=5)
+        xf, sf = ctx.Solve(tol=TOL, max_iter=300, mode=K.SOLVE_FFTM)
+        bnorm = np.linalg.norm(ctx.RHS())
+        fm["gmres_fftm_degree8_depth5"] = {
+            "seconds": sf["seconds"], "iterations": sf["iterations"], "fftm_rel_residual": sf["rel_residual"],
+            "true_rel_residual_direct_operator": float(np.linalg.norm(ctx.Multiply(xf) - ctx.RHS()) / bnorm),
+            "sigma_vs_assembled_solution": float(np.max(np.abs(xf - x_asm)) / np.max(np.abs(x_asm))),
+            "fftm_matvec_ms": None}
+        ctx.FFTMMultiply(xf)
+        fm["gmres_fftm_degree8_depth5"]["fftm_matvec_ms"] = ctx.last_kernel_ms
+        ctx.SetSigma(x_asm)
+        extra["fftm_coax44k"] = fm
         # configuration 5: 100,000 jittered triangles on 8 stacked rings, 8 right-hand sides:
         # one matrix-free FP64 matvec for 8 RHS, and the assembled solve (120 GB operator; the
         # coax context is re-used so that its 23 GB operator is released first)
@@ -379,6 +437,20 @@ def run_native(args, rank, world, dist):
             "matrix_free_fp64_matvec_ms_1rhs": t1, "matrix_free_fp64_matvec_ms_8rhs": t8,
             "assembled_solve_s": s5["seconds"], "assembled_solve_repeat_s": s5r["seconds"],
             "krylov_iterations": s5["iterations"], "rel_residual": s5["rel_residual"]}
+        # the same 8 right-hand sides on the FFTM operator (no assembled operator: it is released
+        # with the geometry's other buffers when the tree is built on a fresh context)
+        with K.CUDAElectrostaticContext(dev) as fc:
+            fc.SetGeometry(rings)
+            t0 = time.perf_counter()
+            fc.ConfigureFFTM(degree=8, maximum_tree_depth=6)
+            build_s = time.perf_counter() - t0
+            Xf, sfm = fc.Solve(B, tol=TOL, mode=K.SOLVE_FFTM, raise_on_failure=False)
+            R = fc.Multiply(Xf, precision=K.FP64) - B
+            extra["c5_stacked_rings_100k_8rhs"]["fftm_degree8_depth6"] = {
+                "tree_build_s": build_s, "solve_s": sfm["seconds"], "krylov_iterations": sfm["iterations"],
+                "fftm_rel_residual": sfm["rel_residual"], "converged": sfm["status"] == 0,
+                "true_rel_residual_direct_operator": float(max(np.linalg.norm(R[i]) / np.linalg.norm(B[i])
+                                                               for i in range(len(B))))}
 
     res = dict(
         ms_mixed=ms_mixed, ms_fp64=ms_fp64, ms_fp32=ms_fp32, err_fp32=err_fp32, wall_mixed=wall_mixed, e2e_s=e2e_s, launches=int(launches),
@@ -430,6 +502,27 @@ def profile_tracker():
         _, _, _, ts = ctx.TrackRK8(E, 1e-11, 10000, step_budget=8, sphere_radius=1.0, precision=prec)
         print(json.dumps({"tracker": name, "tracks": len(E), "steps": ts["steps"], "seconds": ts["seconds"],
                           "track_steps_per_s": ts["steps"] / ts["seconds"]}), flush=True)
+
+
+def profile_fftm():
+    """profiling case for ncu: the fast multipole field (degree 8, depth 5) of the coax density
+    at 1,000,000 gap points, two evaluations"""
+    import torch
+
+    import kassiopeia_b200 as K
+    from kassiopeia_b200 import geometry as G
+
+    ctx = K.CUDAElectrostaticContext(int(os.environ.get("LOCAL_RANK", 0)), autotune=False)
+    mesh = G.coax()
+    ctx.SetGeometry(mesh)
+    ctx.SetSigma(G.coax_density(mesh))
+    ctx.ConfigureFFTM(degree=8, maximum_tree_depth=5)
+    P = torch.from_numpy(G.gap_points(1_000_000, seed=7)).cuda()
+    out = torch.empty((1_000_000, 4), dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        ctx.FFTMFieldDevice(P.data_ptr(), 1_000_000, out.data_ptr())
+        print(json.dumps({"fftm_field": "degree 8, depth 5", "points": 1_000_000, "ms": ctx.last_kernel_ms}),
+              flush=True)
 
 
 def profile_axisym():
@@ -517,6 +610,8 @@ def main():
     ap.add_argument("--profile-axisym", action="store_true",
                     help="profiling case for ncu: axisymmetric coax (4,416 conic sections and rings), field and "
                          "potential at 10,000 gap points, two launches; prints points/s")
+    ap.add_argument("--profile-fftm", action="store_true",
+                    help="profiling case for ncu: fast multipole field of the coax at 1,000,000 points, two launches")
     ap.add_argument("--tracking-c3", action="store_true",
                     help="configuration 3 as configured: 65,536 electrons to the end of every track (hit or "
                          "10,000 steps) in launches of --c3-chunk steps; prints one JSON line (several minutes)")
@@ -529,6 +624,9 @@ def main():
         return
     if args.profile_axisym:
         profile_axisym()
+        return
+    if args.profile_fftm:
+        profile_fftm()
         return
     if args.profile_operator:
         profile_operator()
@@ -580,6 +678,12 @@ def main():
             # the single-core figure beside it (one process, a ~5 s sample)
             rate1, sample1, _, _ = cpu_reference_rate(r["mesh"], r["sigma"], r["P"], 1, seconds_target=5.0)
             cpu["one_core"] = {"value": rate1, "sample": sample1}
+            # the reference's own fast multipole field solver (oracle/_ref/libkemref_fm.so), one
+            # core, same density and parameters (degree 8, depth 5): each call builds its tree and
+            # maps the field; two sample sizes separate that set-up from the per-point evaluation
+            fm_ref = reference_fftm_rate(r["mesh"], r["sigma"], r["P"])
+            if fm_ref is not None:
+                cpu["fftm_reference_one_core"] = fm_ref
             if r["axisym"] is not None:
                 # the axisymmetric model's field on the reference CPU code, one core
                 am, ax_sigma, ax_pts = r["axisym"]

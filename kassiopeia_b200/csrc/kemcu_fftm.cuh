@@ -133,9 +133,12 @@ __global__ void fm_p2m_kernel(const double* __restrict__ rec, const double* __re
     }
 }
 
-// Sum of the element moments of every occupied owner cell, in element order: one warp per cell,
-// lanes over the K coefficients. run[c] = (first, count) of owner cell key[c] in em.
-__global__ void fm_cell_sum_kernel(const double* __restrict__ em, const int* __restrict__ key,
+// Moments of every occupied owner cell for the sources src: the sum over its elements, in
+// element order, of src times the element's unit-density moments (em, from fm_p2m_kernel with
+// unit sources, kept from the tree's construction: the geometry fixes them). One warp per cell,
+// lanes over the K coefficients; run[c] = (first, count) of owner cell key[c] in em / order.
+__global__ void fm_cell_sum_kernel(const double* __restrict__ em, const double* __restrict__ src,
+                                   const int* __restrict__ order, const int* __restrict__ key,
                                    const int2* __restrict__ run, int ncells, int K, double* __restrict__ M)
 {
     const int c = (int) ((blockIdx.x * (size_t) blockDim.x + threadIdx.x) >> 5);
@@ -147,9 +150,16 @@ __global__ void fm_cell_sum_kernel(const double* __restrict__ em, const int* __r
     for (int i = lane; i < K; i += 32) {
         double s = 0.;
         for (int j = 0; j < rg.y; j++)
-            s += em[(size_t) (rg.x + j) * K + i];
+            s += src[order[rg.x + j]] * em[(size_t) (rg.x + j) * K + i];
         dst[i] = s;
     }
+}
+
+__global__ void fm_fill_kernel(double* __restrict__ x, int n, double v)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        x[i] = v;
 }
 
 // ------------------------------------------------------------------------- translations
