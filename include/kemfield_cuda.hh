@@ -458,7 +458,19 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
         KCUDAChargeDensitySolverBase(tolerance, device),
         fMaxIterations(max_iterations),
         fMode(mode)
-    {}
+    {
+        kemcu_fftm_default_params(&fFftm);
+    }
+    // the tree of KEMCU_SOLVE_FFTM (GMRES on the fast multipole operator, the device form of
+    // KKrylovChargeDensitySolver with KFastMultipoleMatrixGenerator)
+    void SetFastMultipoleParameters(const kemcu_fftm_params& prm)
+    {
+        fFftm = prm;
+    }
+    const kemcu_fftm_params& GetFastMultipoleParameters() const
+    {
+        return fFftm;
+    }
     void SetMaxIterations(int n)
     {
         fMaxIterations = n;
@@ -475,7 +487,7 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
     {
         return fMode;
     }
-    // XML form: "plain", "mixed", "assembled", "assembled_fp64" or "fp32" (kemcu_solve_mode)
+    // XML form: "plain", "mixed", "assembled", "assembled_fp64", "fp32" or "fftm" (kemcu_solve_mode)
     void SetModeName(const std::string& name)
     {
         if (name == "plain")
@@ -488,15 +500,19 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
             fMode = KEMCU_SOLVE_ASSEMBLED_FP64;
         else if (name == "fp32")
             fMode = KEMCU_SOLVE_FP32;
+        else if (name == "fftm")
+            fMode = KEMCU_SOLVE_FFTM;
         else
             throw KEMSimpleException("kemcu: unknown solve mode <" + name +
-                                     "> (plain, mixed, assembled, assembled_fp64, fp32)");
+                                     "> (plain, mixed, assembled, assembled_fp64, fp32, fftm)");
     }
     // solves A sigma = b for the boundary values and writes sigma into the container
     kemcu_solve_stats Solve(KCUDASurfaceContainer& container) const
     {
         std::vector<double> x(container.size());
         kemcu_solve_stats st{};
+        if (fMode == KEMCU_SOLVE_FFTM)
+            KCUDACheck(container.Context(), kemcu_fftm_configure(container.Context(), &fFftm));
         KCUDACheck(container.Context(),
                    kemcu_gmres(container.Context(), nullptr, x.data(), 1, fTolerance, fMaxIterations, fMode, &st));
         container.ReadBasisData();
@@ -513,6 +529,7 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
         fStats = Solve(container);
     }
     int fMaxIterations, fMode;
+    kemcu_fftm_params fFftm;
     kemcu_solve_stats fStats{};
 };
 

@@ -8,6 +8,7 @@
 //
 //   <cuda_krylov_charge_density_solver tolerance max_iterations mode device/>
 //       KCUDAChargeDensitySolver: GMRES on the device; mode = plain | mixed | assembled | assembled_fp64 | fp32
+//       | fftm (the fast multipole operator, default tree parameters)
 //   <cuda_robin_hood_charge_density_solver tolerance check_sub_interval cache_matrix_elements device/>
 //       KCUDARobinHoodChargeDensitySolver (attribute names of the reference's robin_hood element)
 //   <cuda_field_solver precision device/>

@@ -463,14 +463,16 @@ __global__ void __launch_bounds__(128) fm_eval_kernel(const double* __restrict__
 // leaf holding element t's collocation point (its potential, or for a Neumann row its field
 // along the normal) plus the matrix entries entry() of the elements owned by the neighbours of
 // the leaf's ancestors times x, in the order of fm_eval_kernel. One CTA per run of targets
-// sorted by leaf (tgt_order lists the elements).
+// sorted by leaf (tgt_order lists the elements). NR right-hand sides (nrhs of them used) share
+// every entry: x, y are nrhs x n, the local expansions of right-hand side r at Lx + r * lstride.
+template<int NR>
 __global__ void __launch_bounds__(128) fm_matvec_kernel(const double* __restrict__ rec,
                                                         const TargetRec* __restrict__ tgt,
                                                         const int* __restrict__ tgt_order,
                                                         const int* __restrict__ run_key, const int* __restrict__ run_off,
                                                         const int* __restrict__ run_cnt, FmTreeView T, int p,
-                                                        const double* __restrict__ Lx, const double* __restrict__ x,
-                                                        double* __restrict__ y)
+                                                        const double* __restrict__ Lx, size_t lstride, int n,
+                                                        int nrhs, const double* __restrict__ x, double* __restrict__ y)
 {
     extern __shared__ double fm_x[];
     const int b = blockIdx.x;
@@ -478,8 +480,9 @@ __global__ void __launch_bounds__(128) fm_matvec_kernel(const double* __restrict
     const int off = run_off[b], cnt = run_cnt[b];
     const int K = (p + 1) * (p + 1);
     const FmLevel& Ld = T.lv[T.depth];
-    for (int i = threadIdx.x; i < K; i += blockDim.x)
-        fm_x[i] = Lx[(Ld.base + key) * K + i];
+    for (int r = 0; r < nrhs; r++)
+        for (int i = threadIdx.x; i < K; i += blockDim.x)
+            fm_x[r * K + i] = Lx[r * lstride + (Ld.base + key) * K + i];
     __syncthreads();
     const int lz = key % Ld.n, ly = (key / Ld.n) % Ld.n, lx = key / (Ld.n * Ld.n);
     const double cx = T.wx + (lx + .5) * Ld.side, cy = T.wy + (ly + .5) * Ld.side, cz = T.wz + (lz + .5) * Ld.side;
@@ -488,10 +491,10 @@ __global__ void __launch_bounds__(128) fm_matvec_kernel(const double* __restrict
         const int ti = tgt_order[off + k];
         const TargetRec t = tgt[ti];
         const V3 C = v3(t.cen[0], t.cen[1], t.cen[2]);
-        double far[4];
-        fm_l2p(fm_x, p, (C.x - cx) * inv_side, (C.y - cy) * inv_side, (C.z - cz) * inv_side, inv_side, far);
-        const double fv = t.neumann == 0. ? far[3] : far[0] * t.normal[0] + far[1] * t.normal[1] + far[2] * t.normal[2];
-        double s = 0., c = 0.;
+        double s[NR], c[NR];
+#pragma unroll
+        for (int r = 0; r < NR; r++)
+            s[r] = c[r] = 0.;
         for (int l = 0; l <= T.depth; l++) {
             const FmLevel& L = T.lv[l];
             int ax = lx, ay = ly, az = lz;
@@ -507,14 +510,28 @@ __global__ void __launch_bounds__(128) fm_matvec_kernel(const double* __restrict
                         const int e0 = T.own_ptr[ci], e1 = T.own_ptr[ci + 1];
                         for (int j = e0; j < e1; j++) {
                             const int e = T.own_elem[j];
-                            const double yk = entry<false>(rec + (size_t) e * rRecSize, t, C) * x[e] - c;
-                            const double tt = s + yk;
-                            c = (tt - s) - yk;
-                            s = tt;
+                            const double a = entry<false>(rec + (size_t) e * rRecSize, t, C);
+#pragma unroll
+                            for (int r = 0; r < NR; r++)
+                                if (r < nrhs) {
+                                    const double yk = a * x[(size_t) r * n + e] - c[r];
+                                    const double tt = s[r] + yk;
+                                    c[r] = (tt - s[r]) - yk;
+                                    s[r] = tt;
+                                }
                         }
                     }
         }
-        y[ti] = s + fv;
+        const double ux = (C.x - cx) * inv_side, uy = (C.y - cy) * inv_side, uz = (C.z - cz) * inv_side;
+#pragma unroll
+        for (int r = 0; r < NR; r++)
+            if (r < nrhs) {
+                double far[4];
+                fm_l2p(fm_x + r * K, p, ux, uy, uz, inv_side, far);
+                const double fv =
+                    t.neumann == 0. ? far[3] : far[0] * t.normal[0] + far[1] * t.normal[1] + far[2] * t.normal[2];
+                y[(size_t) r * n + ti] = s[r] + fv;
+            }
     }
 }
 

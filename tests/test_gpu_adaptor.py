@@ -1,4 +1,5 @@
-"""The C++ KEMField adaptors (include/kemfield_cuda.hh) on a real device: the reference's own
+"""The C++ KEMField adaptors (include/kemfield_cuda.hh, kemfield_cuda_fftm.hh, kassiopeia_cuda.hh,
+kemfield_cuda_bindings.hh) on a real device: the reference's own
 KSurfaceContainer is solved on the GPU, and the reference CPU field solver, matrix and GMRES
 driver are compared with the CUDA adaptors (tests/cxx/adaptor_check.cc, built by
 `make -C oracle adaptor` where the reference tree exists)."""
@@ -45,6 +46,21 @@ def test_xml_bindings_configure_the_gpu_solvers():
     # Kommon tokenizer configures the CUDA solvers (and the use_cuda switch) of boundary fields
     # whose fields then match the reference CPU field solver (tests/cxx/bindings_check.cc)
     r = subprocess.run([XML], capture_output=True, text=True, timeout=600)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "OK" in r.stdout
+
+
+FFTM = os.path.join(ROOT, "oracle", "_ref", "fftm_check")
+
+
+@pytest.mark.skipif(not os.path.exists(FFTM), reason="FFTM check not built (needs the reference tree)")
+def test_fast_multipole_drop_ins_against_reference_classes():
+    # include/kemfield_cuda_fftm.hh: the reference's KKrylovChargeDensitySolver solving with
+    # KCUDAFastMultipoleMatrixGenerator against it solving with its own
+    # KFastMultipoleMatrixGenerator, the device FFTM solve, and KCUDAFastMultipoleFieldSolver
+    # against KElectricFastMultipoleFieldSolver (tests/cxx/fftm_check.cc)
+    r = subprocess.run([FFTM], capture_output=True, text=True, timeout=900)
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "OK" in r.stdout

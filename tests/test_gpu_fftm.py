@@ -200,3 +200,17 @@ def test_fftm_solve_reaches_direct_density():
     assert st["rel_residual"] <= 1e-10
     ref = fx["sigma_direct"]
     assert np.abs(sigma - ref).max() <= 1e-4 * np.abs(ref).max()
+
+
+def test_fftm_matvec_several_rhs_equal_single_products():
+    # the direct entries are evaluated once for all right-hand sides; every row equals the
+    # product with that right-hand side alone
+    cs = golden.load("coax_small")
+    ctx = K.CUDAElectrostaticContext(0)
+    ctx.SetGeometry(mesh_from(cs))
+    ctx.ConfigureFFTM(degree=6, maximum_tree_depth=3)
+    X = np.random.default_rng(11).normal(size=(5, len(cs["sigma"]))) * 1e-9
+    Y = ctx.FFTMMultiply(X)
+    for r in range(len(X)):
+        y1 = ctx.FFTMMultiply(X[r])
+        assert np.abs(Y[r] - y1).max() <= 1e-14 * np.abs(y1).max()
