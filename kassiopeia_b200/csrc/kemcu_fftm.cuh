@@ -386,8 +386,15 @@ struct FmTreeView
     const int* own_elem;  // elements in owner order
 };
 
+//
+// Register budget: the analytic integrals (rwg64) take up to 255 registers unbounded, which left
+// two CTAs per SM; bounded for 4 resident CTAs they spill a little and the kernel runs 18 %
+// faster (coax, 10^6 points, degree 8: 24.8 ms at depth 5, 17.6 ms at depth 6, against 30.2 and
+// 22.3; 3 and 5 CTAs measured 25.5 / 18.8 and 25.8 / 17.2 ms; results bit-identical).
+constexpr int kFmEvalMinBlocks = 4, kFmMatvecMinBlocks = 5;
+
 template<bool POT, bool FIELD, bool ANALYTIC>
-__global__ void __launch_bounds__(128) fm_eval_kernel(const double* __restrict__ rec, const double* __restrict__ src,
+__global__ void __launch_bounds__(128, kFmEvalMinBlocks) fm_eval_kernel(const double* __restrict__ rec, const double* __restrict__ src,
                                                       const double* __restrict__ P, const int* __restrict__ run_key,
                                                       const int* __restrict__ run_off, const int* __restrict__ run_cnt,
                                                       int first_run, FmTreeView T, int p,
@@ -465,8 +472,9 @@ __global__ void __launch_bounds__(128) fm_eval_kernel(const double* __restrict__
 // the leaf's ancestors times x, in the order of fm_eval_kernel. One CTA per run of targets
 // sorted by leaf (tgt_order lists the elements). NR right-hand sides (nrhs of them used) share
 // every entry: x, y are nrhs x n, the local expansions of right-hand side r at Lx + r * lstride.
+// (bounded for 5 resident CTAs: 7.35 ms per coax matvec against 8.9 ms unbounded, 7.6 at 4)
 template<int NR>
-__global__ void __launch_bounds__(128) fm_matvec_kernel(const double* __restrict__ rec,
+__global__ void __launch_bounds__(128, kFmMatvecMinBlocks) fm_matvec_kernel(const double* __restrict__ rec,
                                                         const TargetRec* __restrict__ tgt,
                                                         const int* __restrict__ tgt_order,
                                                         const int* __restrict__ run_key, const int* __restrict__ run_off,
