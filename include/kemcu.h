@@ -287,12 +287,14 @@ int kemcu_fma_peak(kemcu_ctx* ctx, double* fp64_tflops, double* fp32_tflops);
    about the owner cells, M2M up, M2L between the cells of each level that are not neighbours
    (within `zeromask` cells) but whose parents are, L2L down; a point is the local expansion of
    its leaf plus the direct sum over the elements owned by the neighbours of its leaf's
-   ancestors. Only divisions == 2 and zeromask == 1 are built. */
+   ancestors. Divisions 2..8 and zeromask 1..3; the M2L operators (one per offset of the
+   interaction lists, ((2 (zeromask+1) divisions - 1)^3 - (2 zeromask + 1)^3) matrices of
+   (degree+1)^4 doubles) must fit in 8 GB. */
 typedef struct {
     int degree;                     /* expansion degree p, 1..15 (KFMElectrostaticParameters::degree) */
     int top_level_divisions;        /* divisions of the root per dimension, 1..8 */
-    int divisions;                  /* divisions of every further level per dimension (2) */
-    int zeromask;                   /* neighbour order: cells within it are summed directly (1) */
+    int divisions;                  /* divisions of every further level per dimension, 2..8 (2) */
+    int zeromask;                   /* neighbour order: cells within it are summed directly, 1..3 (1) */
     int maximum_tree_depth;         /* level of the leaves, 1..10 */
     double insertion_ratio;         /* insertion condition's ratio (4/3) */
     double region_expansion_factor; /* world cube side over the elements' extent (1.1) */

@@ -17,7 +17,7 @@
 // world cube is the one given and the tree is the reference's; with it on, the library estimates
 // the cube from the elements' bounding box (the reference from their minimal bounding ball), so
 // the two trees, and their truncation errors, can differ. Only the aggressive subdivision
-// strategy, divisions 2 and zeromask 1 are built (kemcu_fftm_configure rejects the others).
+// strategy is built; divisions 2..8 and zeromask 1..3 (kemcu_fftm_configure rejects others).
 #pragma once
 
 #include "KBoundaryMatrixGenerator.hh"

@@ -145,7 +145,8 @@ def test_fftm_state_and_argument_errors():
     ctx.SetSigma(np.ones(80) * 1e-9)
     with pytest.raises(K.KemcuError):
         ctx.FFTMField(np.zeros((4, 3)))  # not configured
-    for bad in ({"divisions": 3}, {"zeromask": 2}, {"degree": 0}, {"degree": 16}, {"maximum_tree_depth": 11}):
+    for bad in ({"divisions": 1}, {"divisions": 9}, {"zeromask": 0}, {"zeromask": 4}, {"degree": 0}, {"degree": 16},
+                {"maximum_tree_depth": 11}):
         with pytest.raises(K.KemcuError):
             ctx.ConfigureFFTM(**bad)
     ax = K.CUDAElectrostaticContext(0)
@@ -214,3 +215,25 @@ def test_fftm_matvec_several_rhs_equal_single_products():
     for r in range(len(X)):
         y1 = ctx.FFTMMultiply(X[r])
         assert np.abs(Y[r] - y1).max() <= 1e-14 * np.abs(y1).max()
+
+
+@needs_ref_fm
+@pytest.mark.parametrize("t,d,zm,depth", [(2, 3, 1, 3), (4, 4, 1, 2), (3, 4, 1, 3), (2, 2, 2, 3), (2, 4, 2, 2)])
+def test_fftm_other_divisions_and_zeromask_equal_live_reference(t, d, zm, depth):
+    # top-level divisions, division ratio and neighbour order of the reference's parameters
+    fx = golden.load("c1_sphere")
+    sph = G.icosphere(3)
+    rng = np.random.default_rng(3)
+    Q = rng.uniform(-1.0, 1.0, (4000, 3))
+    P = Q[np.abs(np.linalg.norm(Q, axis=1) - 1) > 0.08][:200]
+    fr = ref_fm.FmRefProblem(sph)
+    fr.set_sigma(fx["sigma_direct"])
+    want, world = fr.field(P, degree=8, top_level_divisions=t, divisions=d, zeromask=zm, maximum_tree_depth=depth)
+    ctx = K.CUDAElectrostaticContext(0)
+    ctx.SetGeometry(sph)
+    ctx.SetSigma(fx["sigma_direct"])
+    ctx.ConfigureFFTM(degree=8, top_level_divisions=t, divisions=d, zeromask=zm, maximum_tree_depth=depth,
+                      world_center=world[:3], world_length=world[3])
+    got = ctx.FFTMField(P)
+    err = np.abs(got - want).max(axis=0) / np.abs(want).max(axis=0)
+    assert np.all(err[:3] <= 1e-11) and err[3] <= 1e-13, err
