@@ -466,10 +466,26 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
     void SetFastMultipoleParameters(const kemcu_fftm_params& prm)
     {
         fFftm = prm;
+        fFftmEstimate = prm.world_length <= 0.;
+        fFftmWorldLength = prm.world_length;
+    }
+    kemcu_fftm_params& FastMultipoleParameters()
+    {
+        return fFftm;
     }
     const kemcu_fftm_params& GetFastMultipoleParameters() const
     {
         return fFftm;
+    }
+    // the world cube: estimated from the elements (true, the default) or the centre in
+    // FastMultipoleParameters().world_center with this side length
+    void SetFastMultipoleRegionEstimation(bool choice)
+    {
+        fFftmEstimate = choice;
+    }
+    void SetFastMultipoleWorldLength(double length)
+    {
+        fFftmWorldLength = length;
     }
     void SetMaxIterations(int n)
     {
@@ -511,8 +527,11 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
     {
         std::vector<double> x(container.size());
         kemcu_solve_stats st{};
-        if (fMode == KEMCU_SOLVE_FFTM)
-            KCUDACheck(container.Context(), kemcu_fftm_configure(container.Context(), &fFftm));
+        if (fMode == KEMCU_SOLVE_FFTM) {
+            kemcu_fftm_params q = fFftm;
+            q.world_length = fFftmEstimate ? 0. : fFftmWorldLength;
+            KCUDACheck(container.Context(), kemcu_fftm_configure(container.Context(), &q));
+        }
         KCUDACheck(container.Context(),
                    kemcu_gmres(container.Context(), nullptr, x.data(), 1, fTolerance, fMaxIterations, fMode, &st));
         container.ReadBasisData();
@@ -530,6 +549,8 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
     }
     int fMaxIterations, fMode;
     kemcu_fftm_params fFftm;
+    bool fFftmEstimate = true;
+    double fFftmWorldLength = 0.;
     kemcu_solve_stats fStats{};
 };
 

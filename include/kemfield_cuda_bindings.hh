@@ -13,6 +13,13 @@
 //       KCUDARobinHoodChargeDensitySolver (attribute names of the reference's robin_hood element)
 //   <cuda_field_solver precision device/>
 //       KCUDAElectricFieldSolver; precision = fp64 | mixed | fp32
+//   <cuda_fast_multipole_field_solver expansion_degree top_level_divisions tree_level_divisions
+//           neighbor_order maximum_tree_depth region_expansion_factor use_region_size_estimation
+//           world_cube_center_x/y/z world_cube_length insertion_ratio use_caching verbosity device
+//           near_field_analytic/>
+//       KCUDAFastMultipoleFieldSolver, with the attribute names of the reference's
+//       fast_multipole_field_solver element (KElectricFastMultipoleFieldSolverBuilder.hh:16-75);
+//       cuda_krylov_charge_density_solver takes the same tree attributes for mode="fftm"
 //   <integrating_field_solver integrator use_opencl use_cuda cuda_precision cuda_device/>
 //       KIntegratingElectrostaticFieldSolverCUDA: the reference's integrating field solver with a
 //       use_cuda switch beside use_opencl (KIntegratingElectrostaticFieldSolverBuilder.cc:20-21);
@@ -26,6 +33,7 @@
 #include "KElectrostaticBoundaryIntegratorAttributeProcessor.hh"
 #include "KIntegratingElectrostaticFieldSolver.hh"
 #include "kemfield_cuda.hh"
+#include "kemfield_cuda_fftm.hh"
 
 #include <memory>
 #include <string>
@@ -124,6 +132,83 @@ using KCUDAChargeDensitySolverBuilder = KComplexElement<KEMField::KCUDAChargeDen
 using KCUDARobinHoodChargeDensitySolverBuilder = KComplexElement<KEMField::KCUDARobinHoodChargeDensitySolver>;
 using KCUDAElectricFieldSolverBuilder = KComplexElement<KEMField::KCUDAElectricFieldSolver>;
 using KIntegratingElectrostaticFieldSolverCUDABuilder = KComplexElement<KEMField::KIntegratingElectrostaticFieldSolverCUDA>;
+using KCUDAFastMultipoleFieldSolverBuilder = KComplexElement<KEMField::KCUDAFastMultipoleFieldSolver>;
+
+// the tree attributes of the reference's fast_multipole_field_solver element
+// (KElectricFastMultipoleFieldSolverBuilder.hh:16-75) onto KFMElectrostaticParameters
+inline bool KEMCUFastMultipoleAttribute(KEMField::KFMElectrostaticParameters& p, KContainer* c)
+{
+    const std::string& n = c->GetName();
+    if (n == "top_level_divisions")
+        p.top_level_divisions = c->AsReference<unsigned int>();
+    else if (n == "tree_level_divisions")
+        p.divisions = c->AsReference<unsigned int>();
+    else if (n == "expansion_degree")
+        p.degree = c->AsReference<unsigned int>();
+    else if (n == "neighbor_order")
+        p.zeromask = c->AsReference<unsigned int>();
+    else if (n == "maximum_tree_depth")
+        p.maximum_tree_depth = c->AsReference<unsigned int>();
+    else if (n == "region_expansion_factor")
+        p.region_expansion_factor = c->AsReference<double>();
+    else if (n == "use_region_size_estimation")
+        p.use_region_estimation = c->AsReference<bool>();
+    else if (n == "world_cube_center_x")
+        p.world_center_x = c->AsReference<double>();
+    else if (n == "world_cube_center_y")
+        p.world_center_y = c->AsReference<double>();
+    else if (n == "world_cube_center_z")
+        p.world_center_z = c->AsReference<double>();
+    else if (n == "world_cube_length")
+        p.world_length = c->AsReference<double>();
+    else if (n == "insertion_ratio")
+        p.insertion_ratio = c->AsReference<double>();
+    else if (n == "use_caching")
+        p.use_caching = c->AsReference<bool>();
+    else if (n == "verbosity")
+        p.verbosity = c->AsReference<unsigned int>();
+    else
+        return false;
+    return true;
+}
+
+// the same attributes onto the device solver's FFTM tree (mode="fftm")
+inline bool KEMCUFastMultipoleAttribute(KEMField::KCUDAChargeDensitySolver& s, KContainer* c)
+{
+    kemcu_fftm_params& q = s.FastMultipoleParameters();
+    const std::string& n = c->GetName();
+    if (n == "top_level_divisions")
+        q.top_level_divisions = (int) c->AsReference<unsigned int>();
+    else if (n == "tree_level_divisions")
+        q.divisions = (int) c->AsReference<unsigned int>();
+    else if (n == "expansion_degree")
+        q.degree = (int) c->AsReference<unsigned int>();
+    else if (n == "neighbor_order")
+        q.zeromask = (int) c->AsReference<unsigned int>();
+    else if (n == "maximum_tree_depth")
+        q.maximum_tree_depth = (int) c->AsReference<unsigned int>();
+    else if (n == "region_expansion_factor")
+        q.region_expansion_factor = c->AsReference<double>();
+    else if (n == "insertion_ratio")
+        q.insertion_ratio = c->AsReference<double>();
+    else if (n == "use_region_size_estimation")
+        s.SetFastMultipoleRegionEstimation(c->AsReference<bool>());
+    else if (n == "world_cube_center_x")
+        q.world_center[0] = c->AsReference<double>();
+    else if (n == "world_cube_center_y")
+        q.world_center[1] = c->AsReference<double>();
+    else if (n == "world_cube_center_z")
+        q.world_center[2] = c->AsReference<double>();
+    else if (n == "world_cube_length")
+        s.SetFastMultipoleWorldLength(c->AsReference<double>());
+    else if (n == "use_caching" || n == "verbosity") {
+        // accepted for the reference's attribute set; the device tree is rebuilt per solve and
+        // reports nothing
+    }
+    else
+        return false;
+    return true;
+}
 
 template<> inline bool KCUDAChargeDensitySolverBuilder::AddAttribute(KContainer* aContainer)
 {
@@ -144,7 +229,19 @@ template<> inline bool KCUDAChargeDensitySolverBuilder::AddAttribute(KContainer*
         }
     }
     else
-        return false;
+        return KEMCUFastMultipoleAttribute(*fObject, aContainer);
+    return true;
+}
+
+template<> inline bool KCUDAFastMultipoleFieldSolverBuilder::AddAttribute(KContainer* aContainer)
+{
+    const std::string& name = aContainer->GetName();
+    if (name == "device")
+        aContainer->CopyTo(fObject, &KEMField::KCUDAFastMultipoleFieldSolver::SetDevice);
+    else if (name == "near_field_analytic")
+        aContainer->CopyTo(fObject, &KEMField::KCUDAFastMultipoleFieldSolver::SetNearFieldAnalytic);
+    else
+        return KEMCUFastMultipoleAttribute(*fObject->GetParameters(), aContainer);
     return true;
 }
 
@@ -207,7 +304,7 @@ template<> inline bool KIntegratingElectrostaticFieldSolverCUDABuilder::AddAttri
     return true;
 }
 
-// Registers the attributes of the four builders and the four elements under the parent builder
+// Registers the attributes of the five builders and the five elements under the parent builder
 // (KElectrostaticBoundaryFieldBuilder in a KEMField build, whose AddElement takes any
 // KChargeDensitySolver and KElectricFieldSolver). Call once, e.g.
 //   STATICINT sKEMCU = katrin::RegisterKEMCUBuilders<katrin::KElectrostaticBoundaryFieldBuilder>();
@@ -231,7 +328,25 @@ template<class XParentBuilder> int RegisterKEMCUBuilders()
     XParentBuilder::template ComplexElement<KEMField::KCUDAChargeDensitySolver>("cuda_krylov_charge_density_solver");
     XParentBuilder::template ComplexElement<KEMField::KCUDARobinHoodChargeDensitySolver>(
         "cuda_robin_hood_charge_density_solver");
+    for (const char* a : {"top_level_divisions", "tree_level_divisions", "expansion_degree", "neighbor_order",
+                          "maximum_tree_depth", "verbosity"}) {
+        KCUDAChargeDensitySolverBuilder::Attribute<unsigned int>(a);
+        KCUDAFastMultipoleFieldSolverBuilder::Attribute<unsigned int>(a);
+    }
+    for (const char* a : {"region_expansion_factor", "world_cube_center_x", "world_cube_center_y",
+                          "world_cube_center_z", "world_cube_length", "insertion_ratio"}) {
+        KCUDAChargeDensitySolverBuilder::Attribute<double>(a);
+        KCUDAFastMultipoleFieldSolverBuilder::Attribute<double>(a);
+    }
+    for (const char* a : {"use_region_size_estimation", "use_caching"}) {
+        KCUDAChargeDensitySolverBuilder::Attribute<bool>(a);
+        KCUDAFastMultipoleFieldSolverBuilder::Attribute<bool>(a);
+    }
+    KCUDAFastMultipoleFieldSolverBuilder::Attribute<int>("device");
+    KCUDAFastMultipoleFieldSolverBuilder::Attribute<bool>("near_field_analytic");
     XParentBuilder::template ComplexElement<KEMField::KCUDAElectricFieldSolver>("cuda_field_solver");
+    XParentBuilder::template ComplexElement<KEMField::KCUDAFastMultipoleFieldSolver>(
+        "cuda_fast_multipole_field_solver");
     XParentBuilder::template ComplexElement<KEMField::KIntegratingElectrostaticFieldSolverCUDA>(
         "integrating_field_solver");
     return 0;

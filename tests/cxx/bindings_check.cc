@@ -5,7 +5,8 @@
 // (KEMField/Source/Bindings/Fields/Electric/include/KElectrostaticBoundaryFieldBuilder.hh), then
 // drives a KElectrostaticBoundaryField with them on a 320-triangle sphere at 1 V; the field is
 // compared with the reference's KIntegratingElectrostaticFieldSolver on the same charge
-// densities, and the parsed settings with the XML. Exit status 0 when everything agrees. With the
+// densities (a fourth field solves on the fast multipole operator and evaluates with the CUDA FFTM
+// field solver), and the parsed settings with the XML. Exit status 0 when everything agrees. With the
 // argument --parse-only the check stops after the settings (no device needed).
 #include "KComplexElement.hh"
 #include "KElectrostaticBoundaryField.hh"
@@ -121,6 +122,15 @@ static const char* kXML = R"(
     <cuda_krylov_charge_density_solver tolerance="1.e-12" mode="plain"/>
     <integrating_field_solver integrator="numeric" use_opencl="false" use_cuda="false"/>
 </test_electrostatic_field>
+<test_electrostatic_field>
+    <cuda_krylov_charge_density_solver tolerance="1.e-10" mode="fftm" expansion_degree="10" top_level_divisions="2"
+        tree_level_divisions="2" neighbor_order="1" maximum_tree_depth="3" use_region_size_estimation="true"
+        verbosity="0"/>
+    <cuda_fast_multipole_field_solver expansion_degree="10" top_level_divisions="2" tree_level_divisions="2"
+        neighbor_order="2" maximum_tree_depth="3" region_expansion_factor="1.1" use_region_size_estimation="false"
+        world_cube_center_x="0.001" world_cube_center_y="-0.002" world_cube_center_z="0.0" world_cube_length="6.4"
+        insertion_ratio="1.3333333333333333" verbosity="0"/>
+</test_electrostatic_field>
 )";
 
 // the boundary field with the parsed solvers, against the reference CPU field solver
@@ -172,7 +182,7 @@ int main(int argc, char** argv)
         file.AddToNames(xml);
         tokenizer.ProcessFile(&file);
         std::printf("parsed %zu field elements\n", gFields.size());
-        if (gFields.size() != 3)
+        if (gFields.size() != 4)
             return 1;
         // settings as written in the XML
         auto* k0 = dynamic_cast<KCUDAChargeDensitySolver*>(gFields[0].cds.get());
@@ -181,23 +191,35 @@ int main(int argc, char** argv)
         auto* f1 = dynamic_cast<KCUDAElectricFieldSolver*>(gFields[1].fs.get());
         auto* k2 = dynamic_cast<KCUDAChargeDensitySolver*>(gFields[2].cds.get());
         auto* f2 = dynamic_cast<KIntegratingElectrostaticFieldSolverCUDA*>(gFields[2].fs.get());
+        auto* k3 = dynamic_cast<KCUDAChargeDensitySolver*>(gFields[3].cds.get());
+        auto* f3 = dynamic_cast<KCUDAFastMultipoleFieldSolver*>(gFields[3].fs.get());
         const bool settings = k0 && f0 && r1 && f1 && k2 && f2 && k0->GetTolerance() == 1e-11 &&
                               k0->GetMaxIterations() == 250 && k0->GetMode() == KEMCU_SOLVE_ASSEMBLED &&
                               f0->UsesCUDA() && f0->CUDASolver().GetPrecision() == KEMCU_MIXED &&
                               r1->GetTolerance() == 1e-9 && r1->GetCheckSubInterval() == 64 &&
                               r1->MatrixElementsCached() && f1->GetPrecision() == KEMCU_FP64 &&
-                              k2->GetMode() == KEMCU_SOLVE_PLAIN && !f2->UsesCUDA();
+                              k2->GetMode() == KEMCU_SOLVE_PLAIN && !f2->UsesCUDA() && k3 && f3 &&
+                              k3->GetMode() == KEMCU_SOLVE_FFTM && k3->GetFastMultipoleParameters().degree == 10 &&
+                              k3->GetFastMultipoleParameters().maximum_tree_depth == 3 &&
+                              f3->GetParameters()->degree == 10 && f3->GetParameters()->zeromask == 2 &&
+                              f3->GetParameters()->maximum_tree_depth == 3 &&
+                              !f3->GetParameters()->use_region_estimation &&
+                              f3->GetParameters()->world_length == 6.4 &&
+                              f3->GetParameters()->world_center_y == -0.002;
         std::printf("settings from the XML: %s\n", settings ? "as written" : "WRONG");
         fail += !settings;
         if (settings && !parse_only) {
             const double d0 = field_difference(gFields[0], gScratch + "/0");
             const double d1 = field_difference(gFields[1], gScratch + "/1");
             const double d2 = field_difference(gFields[2], gScratch + "/2");
+            const double d3 = field_difference(gFields[3], gScratch + "/3");
             std::printf("field vs the reference CPU solver: GMRES assembled + CUDA mixed %.3e, Robin Hood + CUDA "
-                        "FP64 %.3e, GMRES plain + reference field solver (use_cuda=false) %.3e\n", d0, d1, d2);
+                        "FP64 %.3e, GMRES plain + reference field solver (use_cuda=false) %.3e, FFTM GMRES + CUDA "
+                        "FFTM field %.3e\n", d0, d1, d2, d3);
             // the densities differ by the solve tolerance (1e-11 GMRES, 1e-9 Robin Hood): the CPU
-            // comparison solver sees the same densities, so only the field arithmetic differs
-            fail += !(d0 < 1e-9 && d1 < 1e-12 && d2 < 1e-14);
+            // comparison solver sees the same densities, so only the field arithmetic differs; the
+            // FFTM field differs by its truncation error (degree 10, neighbour order 2)
+            fail += !(d0 < 1e-9 && d1 < 1e-12 && d2 < 1e-14 && d3 < 1e-5);
         }
     }
     catch (std::exception& e) {
