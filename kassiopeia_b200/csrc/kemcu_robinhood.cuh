@@ -21,10 +21,13 @@
 // CTA that stops arriving makes every other one return within the limit.
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "kemcu_kernels.cuh"
 
 namespace kemcu
 {
+namespace cg = cooperative_groups;
 
 constexpr int kRhThreads = 256;
 
@@ -215,7 +218,12 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& gen, int* 
 // (double-buffered by exchange parity); bar: {arrivals, generation}, zero arrivals on entry
 // (every CTA reads the generation before it first arrives, so all start from the same value);
 // flag |= 2 when a barrier wait gave up (bar must then be cleared before the next launch).
-template<bool ASSEMBLED>
+//
+// CLUSTER: the grid is one thread-block cluster (up to 16 CTAs holding all rows of the system);
+// the per-correction exchange is each CTA's best row in its shared memory, the hardware cluster
+// barrier, and a read of every CTA's result through distributed shared memory (double-buffered by
+// parity) instead of `part` and the software grid barrier; it has no wait that could time out.
+template<bool ASSEMBLED, bool CLUSTER>
 __global__ void __launch_bounds__(kRhThreads) robin_hood_kernel(const double* __restrict__ rec, const TargetRec* __restrict__ tgt,
                                                                 int n, const double* __restrict__ A, size_t ld,
                                                                 const long long* __restrict__ near_ptr,
@@ -231,6 +239,7 @@ __global__ void __launch_bounds__(kRhThreads) robin_hood_kernel(const double* __
     __shared__ double s_rec[rRecSize];
     __shared__ RhPart s_part[32];
     __shared__ RhPart s_best;
+    __shared__ RhPart s_slot[2];  // CLUSTER: this CTA's best row, read by the cluster's CTAs
     __shared__ int s_ok;
     const int tid = threadIdx.x, G = (int) gridDim.x;
     const int per = (n + G - 1) / G;
@@ -265,6 +274,26 @@ __global__ void __launch_bounds__(kRhThreads) robin_hood_kernel(const double* __
     // publish this CTA's best, wait for all, reduce the published results (every CTA alike)
     auto exchange = [&](RhPart mine) -> bool {
         mine = rh_cta_best(mine, s_part);
+        if (CLUSTER) {
+            if (tid == 0)
+                s_slot[parity] = mine;
+            cg::this_cluster().sync();
+            if (tid < 32) {
+                RhPart a = rh_none();
+                for (int q = tid; q < G; q += 32)
+                    rh_better(a, *cg::this_cluster().map_shared_rank(&s_slot[parity], q));
+                a = rh_warp_best(a);
+                if (tid == 0)
+                    s_best = a;
+            }
+            __syncthreads();
+            S.rmax = s_best.v;
+            S.k = s_best.i;
+            S.rk = s_best.r;
+            S.dk = s_best.d;
+            parity ^= 1;
+            return true;
+        }
         if (tid == 0)
             part[parity * G + blockIdx.x] = mine;
         if (G > 1 && !grid_barrier(bar, gen, &s_ok))
@@ -346,6 +375,8 @@ __global__ void __launch_bounds__(kRhThreads) robin_hood_kernel(const double* __
     __syncthreads();
     for (int q = tid; q < nr; q += blockDim.x)
         bit[r0 + q] = s_bit[q];
+    if (CLUSTER)
+        cg::this_cluster().sync();  // no CTA leaves while another may still read its slots
     if (!ok && tid == 0)
         atomicOr(flag, 2);
     if (blockIdx.x == 0 && tid == 0) {
