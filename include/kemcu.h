@@ -321,6 +321,60 @@ int kemcu_fftm_matvec(kemcu_ctx* ctx, const double* x, double* y, int n_rhs);
 /* tree summary: world4 = world cube centre and side; counts = {cells with moments, elements
    owned per level 0..maximum_tree_depth} (counts has room for 2 + maximum_tree_depth ints) */
 int kemcu_fftm_info(const kemcu_ctx* ctx, double* world4, int* counts);
+/* a second tree whose operator serves as the implicit Krylov preconditioner's matrix
+   (KEMCU_SOLVE_FFTM as kemcu_krylov_params.preconditioner_mode): the solver's parameters with
+   degree = preconditioner_degree for the reference's "implicit_krylov" (a lower-degree
+   operator on the same tree, KFMElectrostaticFastMultipoleBoundaryValueSolver.cc:726-745), or
+   the preconditioner_electrostatic_parameters for "independent_implicit_krylov" (:831-848).
+   Degree 1..15 (the reference's default preconditioner_degree 0 is refused with
+   KEMCU_EINVAL). Replaces the previous preconditioner tree. */
+int kemcu_fftm_configure_preconditioner(kemcu_ctx* ctx, const kemcu_fftm_params* prm);
+
+/* ---- Krylov charge-density solves with restarts and right preconditioners: the solver
+        dispatch of KKrylovSolverFactory.hh:110-150 and of the fast-multipole boundary-value
+        solver (KFMElectrostaticFastMultipoleBoundaryValueSolver.cc:189-233) ----
+   GMRES as KGeneralizedMinimalResidual / KPreconditionedGeneralizedMinimalResidual
+   (KPreconditionedGeneralizedMinimalResidual.hh: right preconditioning, the preconditioned basis
+   kept when the preconditioner is not stationary) and BiCGStab as
+   KBiconjugateGradientStabilized / KPreconditionedBiconjugateGradientStabilized; the iteration
+   loop of KSimpleIterativeKrylovSolver.hh:139-194 / KPreconditionedIterativeKrylovSolver.hh
+   (convergence when the solver's residual norm over |b| is <= tolerance; a restart every
+   iterations_between_restarts iterations, KIterativeKrylovRestartCondition.hh, recomputes the
+   residual b - A x and starts a new Krylov space from the current solution). Preconditioners:
+   Jacobi (KJacobiPreconditioner.hh: 1 / A(i, i)) and implicit Krylov
+   (KImplicitKrylovPreconditioner.hh: an inner GMRES from zero on the preconditioner's operator to
+   preconditioner_tolerance, at most max_preconditioner_iterations iterations).
+   b: n_rhs x n or NULL (boundary values, one RHS); x: n_rhs x n solution from x0 = 0 (also the
+   context's sigma for one RHS). Stats: iterations = Krylov iterations, outer = cycles (1 +
+   restarts), fp64_matvecs = applications of the system's operator, low_matvecs = of the
+   preconditioner's, rel_residual = max over RHS of |b - A x| / |b| recomputed at the end with the
+   system's operator, rel_residual_estimate = the solver's own residual norm over |b|. Returns
+   KEMCU_ENOTCONVERGED when the solver's residual norm is above the tolerance at the end. */
+enum kemcu_krylov_solver { KEMCU_KRYLOV_GMRES = 0, KEMCU_KRYLOV_BICGSTAB = 1 };
+enum kemcu_preconditioner { KEMCU_PRECON_NONE = 0, KEMCU_PRECON_JACOBI = 1, KEMCU_PRECON_IMPLICIT_KRYLOV = 2 };
+typedef struct {
+    int solver;                         /* kemcu_krylov_solver ("solver_name": gmres, bicgstab) */
+    int mode;                           /* the system's operator: KEMCU_SOLVE_PLAIN (FP64 matrix-free),
+                                           KEMCU_SOLVE_ASSEMBLED_FP64 or KEMCU_SOLVE_FFTM */
+    double tolerance;                   /* "tolerance" */
+    int max_iterations;                 /* "max_iterations" (bounds the GMRES basis kept on the device) */
+    int iterations_between_restarts;    /* "iterations_between_restarts"; 0 = never */
+    int preconditioner;                 /* kemcu_preconditioner ("preconditioner") */
+    int preconditioner_mode;            /* operator of the implicit Krylov preconditioner:
+                                           KEMCU_SOLVE_FFTM = the tree of kemcu_fftm_configure_preconditioner;
+                                           KEMCU_SOLVE_FP32 / KEMCU_SOLVE_MIXED = the FP32 / MIXED
+                                           matrix-free operator; KEMCU_SOLVE_ASSEMBLED = the FP32 copy
+                                           of the assembled operator; KEMCU_SOLVE_PLAIN /
+                                           KEMCU_SOLVE_ASSEMBLED_FP64 = the FP64 one */
+    double preconditioner_tolerance;    /* "preconditioner_tolerance" */
+    int max_preconditioner_iterations;  /* "max_preconditioner_iterations" */
+} kemcu_krylov_params;
+/* gmres, KEMCU_SOLVE_PLAIN, tolerance 1e-8, 500 iterations, no restart, no preconditioner;
+   implicit Krylov defaults: KEMCU_SOLVE_FFTM, tolerance 0.01, 30 iterations (the reference's
+   example configurations) */
+void kemcu_krylov_default_params(kemcu_krylov_params* prm);
+int kemcu_krylov_solve(kemcu_ctx* ctx, const double* b, double* x, int n_rhs, const kemcu_krylov_params* prm,
+                       kemcu_solve_stats* stats);
 /* multipole moments of every element of the context, for unit total charge, about the origins
    (n x 3), as KFMElectrostaticMultipoleCalculatorAnalytic::ConstructExpansion gives them:
    out n x (degree+1)^2 complex (re, im) in the index l(l+1)+m */

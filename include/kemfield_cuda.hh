@@ -41,6 +41,7 @@
 #include "KSurfaceTypes.hh"
 #include "kemcu.h"
 
+#include <climits>
 #include <memory>
 #include <string>
 #include <utility>
@@ -448,8 +449,18 @@ class KCUDAChargeDensitySolverBase : public KChargeDensitySolver
     bool fFromCache = false;
 };
 
-// KKrylovChargeDensitySolver analogue for the direct operator: the whole GMRES solve
-// (KSimpleIterativeKrylovSolver<double, KGeneralizedMinimalResidual>) on the device
+// the library's default fast multipole parameters (kemcu_fftm_default_params)
+inline kemcu_fftm_params KCUDADefaultFastMultipoleParameters()
+{
+    kemcu_fftm_params p;
+    kemcu_fftm_default_params(&p);
+    return p;
+}
+
+// KKrylovChargeDensitySolver analogue: the whole Krylov solve on the device, GMRES by default
+// (KSimpleIterativeKrylovSolver<double, KGeneralizedMinimalResidual>) on the direct operator or
+// (mode fftm) on the fast multipole one; with the solver / preconditioner / restart choices of
+// krylov_bem_solver (KKrylovChargeDensitySolverOld with KFMElectrostaticFastMultipoleBoundaryValueSolver)
 class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
 {
   public:
@@ -503,6 +514,100 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
     {
         return fMode;
     }
+    // the solver and preconditioner choices of the reference's Krylov solvers (the attributes
+    // solver_name, preconditioner, iterations_between_restarts, preconditioner_tolerance,
+    // max_preconditioner_iterations and preconditioner_degree of krylov_bem_solver,
+    // KKrylovChargeDensitySolverOldBuilder.hh, and the dispatch of
+    // KFMElectrostaticFastMultipoleBoundaryValueSolver.cc:189-233). Plain GMRES without restarts
+    // runs kemcu_gmres (every mode); any other choice runs kemcu_krylov_solve on the modes plain,
+    // assembled_fp64 and fftm.
+    void SetSolverName(const std::string& name)
+    {
+        if (name == "gmres")
+            fSolver = KEMCU_KRYLOV_GMRES;
+        else if (name == "bicgstab")
+            fSolver = KEMCU_KRYLOV_BICGSTAB;
+        else
+            throw KEMSimpleException("kemcu: unknown Krylov solver <" + name + "> (gmres, bicgstab)");
+    }
+    // "none", "jacobi", "implicit_krylov" (an inner GMRES on the solver's tree at
+    // preconditioner_degree, or on SetPreconditionerMode's operator for a direct system) or
+    // "independent_implicit_krylov" (an inner GMRES on the tree of
+    // SetPreconditionerFastMultipoleParameters)
+    void SetPreconditionerName(const std::string& name)
+    {
+        if (name == "none")
+            fPrecon = KEMCU_PRECON_NONE;
+        else if (name == "jacobi")
+            fPrecon = KEMCU_PRECON_JACOBI;
+        else if (name == "implicit_krylov" || name == "independent_implicit_krylov")
+            fPrecon = KEMCU_PRECON_IMPLICIT_KRYLOV;
+        else
+            throw KEMSimpleException("kemcu: unknown preconditioner <" + name +
+                                     "> (none, jacobi, implicit_krylov, independent_implicit_krylov)");
+        fIndependent = name == "independent_implicit_krylov";
+    }
+    void SetIterationsBetweenRestart(unsigned int n)
+    {
+        fRestart = n >= (unsigned int) INT_MAX ? 0 : (int) n;
+    }
+    void SetPreconditionerTolerance(double t)
+    {
+        fPreTolerance = t;
+    }
+    void SetMaxPreconditionerIterations(unsigned int n)
+    {
+        fPreMaxIterations = n >= (unsigned int) INT_MAX ? INT_MAX : (int) n;
+    }
+    // the degree of the implicit_krylov preconditioner's tree (1..15)
+    void SetPreconditionerDegree(unsigned int d)
+    {
+        fPreDegree = (int) d;
+    }
+    // the tree of independent_implicit_krylov (preconditioner_electrostatic_parameters); a world
+    // length <= 0 estimates the world cube
+    void SetPreconditionerFastMultipoleParameters(const kemcu_fftm_params& prm)
+    {
+        fPreFftm = prm;
+    }
+    // the operator of the implicit Krylov preconditioner for a direct system (kemcu_solve_mode;
+    // default KEMCU_SOLVE_FP32, the FP32 far-field matrix-free operator)
+    void SetPreconditionerMode(int mode)
+    {
+        fPreMode = mode;
+    }
+    int GetSolver() const
+    {
+        return fSolver;
+    }
+    int GetPreconditioner() const
+    {
+        return fPrecon;
+    }
+    bool IndependentPreconditioner() const
+    {
+        return fIndependent;
+    }
+    int GetIterationsBetweenRestart() const
+    {
+        return fRestart;
+    }
+    double GetPreconditionerTolerance() const
+    {
+        return fPreTolerance;
+    }
+    int GetMaxPreconditionerIterations() const
+    {
+        return fPreMaxIterations;
+    }
+    int GetPreconditionerDegree() const
+    {
+        return fPreDegree;
+    }
+    const kemcu_fftm_params& GetPreconditionerFastMultipoleParameters() const
+    {
+        return fPreFftm;
+    }
     // XML form: "plain", "mixed", "assembled", "assembled_fp64", "fp32" or "fftm" (kemcu_solve_mode)
     void SetModeName(const std::string& name)
     {
@@ -527,13 +632,39 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
     {
         std::vector<double> x(container.size());
         kemcu_solve_stats st{};
-        if (fMode == KEMCU_SOLVE_FFTM) {
-            kemcu_fftm_params q = fFftm;
-            q.world_length = fFftmEstimate ? 0. : fFftmWorldLength;
+        kemcu_fftm_params q = fFftm;
+        q.world_length = fFftmEstimate ? 0. : fFftmWorldLength;
+        if (fMode == KEMCU_SOLVE_FFTM)
             KCUDACheck(container.Context(), kemcu_fftm_configure(container.Context(), &q));
+        if (fSolver == KEMCU_KRYLOV_GMRES && fPrecon == KEMCU_PRECON_NONE && fRestart == 0) {
+            KCUDACheck(container.Context(),
+                       kemcu_gmres(container.Context(), nullptr, x.data(), 1, fTolerance, fMaxIterations, fMode, &st));
         }
-        KCUDACheck(container.Context(),
-                   kemcu_gmres(container.Context(), nullptr, x.data(), 1, fTolerance, fMaxIterations, fMode, &st));
+        else {
+            kemcu_krylov_params p;
+            kemcu_krylov_default_params(&p);
+            p.solver = fSolver;
+            p.mode = fMode;
+            p.tolerance = fTolerance;
+            p.max_iterations = fMaxIterations;
+            p.iterations_between_restarts = fRestart;
+            p.preconditioner = fPrecon;
+            p.preconditioner_tolerance = fPreTolerance;
+            p.max_preconditioner_iterations = fPreMaxIterations;
+            p.preconditioner_mode = fPreMode;
+            if (fPrecon == KEMCU_PRECON_IMPLICIT_KRYLOV && fMode == KEMCU_SOLVE_FFTM) {
+                // implicit_krylov: the solver's tree at the preconditioner's degree
+                // (KFMElectrostaticFastMultipoleBoundaryValueSolver.cc:731-737); independent: its own
+                kemcu_fftm_params pq = q;
+                if (fIndependent)
+                    pq = fPreFftm;
+                else
+                    pq.degree = fPreDegree;
+                KCUDACheck(container.Context(), kemcu_fftm_configure_preconditioner(container.Context(), &pq));
+                p.preconditioner_mode = KEMCU_SOLVE_FFTM;
+            }
+            KCUDACheck(container.Context(), kemcu_krylov_solve(container.Context(), nullptr, x.data(), 1, &p, &st));
+        }
         container.ReadBasisData();
         return st;
     }
@@ -551,6 +682,11 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
     kemcu_fftm_params fFftm;
     bool fFftmEstimate = true;
     double fFftmWorldLength = 0.;
+    int fSolver = KEMCU_KRYLOV_GMRES, fPrecon = KEMCU_PRECON_NONE, fRestart = 0;
+    bool fIndependent = false;
+    double fPreTolerance = 0.01;
+    int fPreMaxIterations = 30, fPreDegree = 1, fPreMode = KEMCU_SOLVE_FP32;
+    kemcu_fftm_params fPreFftm = KCUDADefaultFastMultipoleParameters();
     kemcu_solve_stats fStats{};
 };
 

@@ -6,9 +6,18 @@
 // Elements (children of the electrostatic boundary field element, registered by
 // RegisterKEMCUBuilders<KElectrostaticBoundaryFieldBuilder>() in one source file of the build):
 //
-//   <cuda_krylov_charge_density_solver tolerance max_iterations mode device/>
-//       KCUDAChargeDensitySolver: GMRES on the device; mode = plain | mixed | assembled | assembled_fp64 | fp32
-//       | fftm (the fast multipole operator, default tree parameters)
+//   <cuda_krylov_charge_density_solver tolerance max_iterations mode device solver_name preconditioner
+//           iterations_between_restarts preconditioner_tolerance max_preconditioner_iterations
+//           preconditioner_degree>
+//       KCUDAChargeDensitySolver: the Krylov solve on the device; mode = plain | mixed | assembled |
+//       assembled_fp64 | fp32 | fftm (the fast multipole operator); solver_name = gmres | bicgstab,
+//       preconditioner = none | jacobi | implicit_krylov | independent_implicit_krylov, with the
+//       meaning of the reference's krylov_bem_solver (KKrylovChargeDensitySolverOldBuilder.hh);
+//       children <fftm_multiplication .../> (the solver's tree; selects mode fftm) and
+//       <preconditioner_electrostatic_parameters .../> (the independent preconditioner's tree),
+//       built by the reference's KFMElectrostaticParametersBuilder
+//   <cuda_krylov_bem_solver .../>
+//       the same element under the name of the reference's krylov_bem_solver
 //   <cuda_robin_hood_charge_density_solver tolerance check_sub_interval cache_matrix_elements device/>
 //       KCUDARobinHoodChargeDensitySolver (attribute names of the reference's robin_hood element)
 //   <cuda_field_solver precision device/>
@@ -31,6 +40,7 @@
 
 #include "KComplexElement.hh"
 #include "KElectrostaticBoundaryIntegratorAttributeProcessor.hh"
+#include "KFMElectrostaticParametersBuilder.hh"
 #include "KIntegratingElectrostaticFieldSolver.hh"
 #include "kemfield_cuda.hh"
 #include "kemfield_cuda_fftm.hh"
@@ -219,18 +229,57 @@ template<> inline bool KCUDAChargeDensitySolverBuilder::AddAttribute(KContainer*
         aContainer->CopyTo(fObject, &KEMField::KCUDAChargeDensitySolver::SetMaxIterations);
     else if (name == "device")
         aContainer->CopyTo(fObject, &KEMField::KCUDAChargeDensitySolver::SetDevice);
-    else if (name == "mode") {
+    else if (name == "mode" || name == "solver_name" || name == "preconditioner") {
         try {
-            fObject->SetModeName(aContainer->AsString());
+            if (name == "mode")
+                fObject->SetModeName(aContainer->AsString());
+            else if (name == "solver_name")
+                fObject->SetSolverName(aContainer->AsString());
+            else
+                fObject->SetPreconditionerName(aContainer->AsString());
         }
         catch (KEMField::KEMSimpleException& e) {
             BINDINGMSG(eWarning) << e.what() << eom;
             return false;
         }
     }
+    else if (name == "iterations_between_restarts")
+        aContainer->CopyTo(fObject, &KEMField::KCUDAChargeDensitySolver::SetIterationsBetweenRestart);
+    else if (name == "preconditioner_tolerance")
+        aContainer->CopyTo(fObject, &KEMField::KCUDAChargeDensitySolver::SetPreconditionerTolerance);
+    else if (name == "max_preconditioner_iterations")
+        aContainer->CopyTo(fObject, &KEMField::KCUDAChargeDensitySolver::SetMaxPreconditionerIterations);
+    else if (name == "preconditioner_degree")
+        aContainer->CopyTo(fObject, &KEMField::KCUDAChargeDensitySolver::SetPreconditionerDegree);
+    else if (name == "intermediate_save_interval" || name == "use_display" || name == "show_plot" ||
+             name == "use_timer" || name == "time_limit_in_seconds" || name == "time_check_interval") {
+        // accepted for the reference's attribute set: the device solve keeps no checkpoints and
+        // shows no display (the iteration callback of kemcu_set_iteration_callback serves both)
+    }
     else
         return KEMCUFastMultipoleAttribute(*fObject, aContainer);
     return true;
+}
+
+// the children of the reference's krylov_bem_solver (KKrylovChargeDensitySolverOldBuilder.hh:
+// AddElement): fftm_multiplication, the solver's tree (it selects mode fftm), and
+// preconditioner_electrostatic_parameters, the tree of independent_implicit_krylov
+template<> inline bool KCUDAChargeDensitySolverBuilder::AddElement(KContainer* anElement)
+{
+    if (!anElement->Is<KEMField::KFMElectrostaticParameters>())
+        return false;
+    const kemcu_fftm_params q =
+        KEMField::KCUDAFastMultipoleParameters(anElement->AsReference<KEMField::KFMElectrostaticParameters>());
+    if (anElement->GetName() == "fftm_multiplication") {
+        fObject->SetFastMultipoleParameters(q);
+        fObject->SetMode(KEMCU_SOLVE_FFTM);
+        return true;
+    }
+    if (anElement->GetName() == "preconditioner_electrostatic_parameters") {
+        fObject->SetPreconditionerFastMultipoleParameters(q);
+        return true;
+    }
+    return false;
 }
 
 template<> inline bool KCUDAFastMultipoleFieldSolverBuilder::AddAttribute(KContainer* aContainer)
@@ -304,7 +353,7 @@ template<> inline bool KIntegratingElectrostaticFieldSolverCUDABuilder::AddAttri
     return true;
 }
 
-// Registers the attributes of the five builders and the five elements under the parent builder
+// Registers the attributes of the five builders and the six elements under the parent builder
 // (KElectrostaticBoundaryFieldBuilder in a KEMField build, whose AddElement takes any
 // KChargeDensitySolver and KElectricFieldSolver). Call once, e.g.
 //   STATICINT sKEMCU = katrin::RegisterKEMCUBuilders<katrin::KElectrostaticBoundaryFieldBuilder>();
@@ -314,6 +363,18 @@ template<class XParentBuilder> int RegisterKEMCUBuilders()
     KCUDAChargeDensitySolverBuilder::Attribute<int>("max_iterations");
     KCUDAChargeDensitySolverBuilder::Attribute<std::string>("mode");
     KCUDAChargeDensitySolverBuilder::Attribute<int>("device");
+    KCUDAChargeDensitySolverBuilder::Attribute<std::string>("solver_name");
+    KCUDAChargeDensitySolverBuilder::Attribute<std::string>("preconditioner");
+    KCUDAChargeDensitySolverBuilder::Attribute<double>("preconditioner_tolerance");
+    KCUDAChargeDensitySolverBuilder::Attribute<double>("time_limit_in_seconds");
+    for (const char* a : {"iterations_between_restarts", "max_preconditioner_iterations", "preconditioner_degree",
+                          "intermediate_save_interval", "time_check_interval"})
+        KCUDAChargeDensitySolverBuilder::Attribute<unsigned int>(a);
+    for (const char* a : {"use_display", "show_plot", "use_timer"})
+        KCUDAChargeDensitySolverBuilder::Attribute<bool>(a);
+    KCUDAChargeDensitySolverBuilder::ComplexElement<KEMField::KFMElectrostaticParameters>("fftm_multiplication");
+    KCUDAChargeDensitySolverBuilder::ComplexElement<KEMField::KFMElectrostaticParameters>(
+        "preconditioner_electrostatic_parameters");
     KCUDARobinHoodChargeDensitySolverBuilder::Attribute<double>("tolerance");
     KCUDARobinHoodChargeDensitySolverBuilder::Attribute<unsigned int>("check_sub_interval");
     KCUDARobinHoodChargeDensitySolverBuilder::Attribute<bool>("cache_matrix_elements");
@@ -326,6 +387,7 @@ template<class XParentBuilder> int RegisterKEMCUBuilders()
     KIntegratingElectrostaticFieldSolverCUDABuilder::Attribute<std::string>("cuda_precision");
     KIntegratingElectrostaticFieldSolverCUDABuilder::Attribute<int>("cuda_device");
     XParentBuilder::template ComplexElement<KEMField::KCUDAChargeDensitySolver>("cuda_krylov_charge_density_solver");
+    XParentBuilder::template ComplexElement<KEMField::KCUDAChargeDensitySolver>("cuda_krylov_bem_solver");
     XParentBuilder::template ComplexElement<KEMField::KCUDARobinHoodChargeDensitySolver>(
         "cuda_robin_hood_charge_density_solver");
     for (const char* a : {"top_level_divisions", "tree_level_divisions", "expansion_degree", "neighbor_order",

@@ -14,10 +14,11 @@
 //                                      kemcu_fftm_matvec
 //
 // Parameters map one to one (KCUDAFastMultipoleParameters). With use_region_estimation off the
-// world cube is the one given and the tree is the reference's; with it on, the library estimates
-// the cube from the elements' bounding box (the reference from their minimal bounding ball), so
-// the two trees, and their truncation errors, can differ. Only the aggressive subdivision
-// strategy is built; divisions 2..8 and zeromask 1..3 (kemcu_fftm_configure rejects others).
+// world cube is the one given; with it on, the library forms the reference's estimate (the
+// minimal bounding ball of the element balls, KFMElectrostaticRegionSizeEstimator, in the
+// surface container's order), so either way the tree is the reference's. Only the aggressive
+// subdivision strategy is built; divisions 2..8 and zeromask 1..3 (kemcu_fftm_configure rejects
+// others).
 #pragma once
 
 #include "KBoundaryMatrixGenerator.hh"

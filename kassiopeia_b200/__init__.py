@@ -200,6 +200,41 @@ class CUDAElectrostaticContext:
             self._check(rc)
         return x, stats
 
+    def KrylovSolve(self, b=None, solver="gmres", mode=SOLVE_PLAIN, tol=1e-8, max_iter=500, restart=0,
+                    preconditioner="none", preconditioner_mode=SOLVE_FFTM, preconditioner_tol=0.01,
+                    max_preconditioner_iter=30, raise_on_failure=True):
+        """Krylov charge-density solve with the reference's solver and preconditioner choices
+        (KKrylovSolverFactory, KFMElectrostaticFastMultipoleBoundaryValueSolver): solver "gmres" or
+        "bicgstab"; mode: the system's operator (SOLVE_PLAIN, SOLVE_ASSEMBLED_FP64, SOLVE_FFTM);
+        restart: iterations between restarts (0 = never); preconditioner "none", "jacobi" or
+        "implicit_krylov" (an inner GMRES on preconditioner_mode's operator, SOLVE_FFTM = the tree of
+        ConfigureFFTMPreconditioner). Returns (x, stats dict); b as for Solve."""
+        solvers = {"gmres": N.KRYLOV_GMRES, "bicgstab": N.KRYLOV_BICGSTAB}
+        precons = {"none": N.PRECON_NONE, "jacobi": N.PRECON_JACOBI, "implicit_krylov": N.PRECON_IMPLICIT_KRYLOV}
+        if solver not in solvers or preconditioner not in precons:
+            raise ValueError(f"solver must be one of {sorted(solvers)} and preconditioner one of {sorted(precons)}")
+        prm = N.KrylovParams()
+        N.lib().kemcu_krylov_default_params(C.byref(prm))
+        prm.solver, prm.mode, prm.tolerance, prm.max_iterations = solvers[solver], mode, tol, max_iter
+        prm.iterations_between_restarts, prm.preconditioner = restart, precons[preconditioner]
+        prm.preconditioner_mode, prm.preconditioner_tolerance = preconditioner_mode, preconditioner_tol
+        prm.max_preconditioner_iterations = max_preconditioner_iter
+        if b is None:
+            x = np.zeros(self.n)
+            bp, nr = None, 1
+        else:
+            bb = np.ascontiguousarray(b, np.float64)
+            nr = 1 if bb.ndim == 1 else bb.shape[0]
+            x = np.zeros_like(bb)
+            bp = _d(bb)
+        st = N.SolveStats()
+        rc = N.lib().kemcu_krylov_solve(self._h, bp, _d(x), nr, C.byref(prm), C.byref(st))
+        stats = {k: getattr(st, k) for k, _ in N.SolveStats._fields_}
+        stats["status"] = rc
+        if rc != N.OK and raise_on_failure:
+            self._check(rc)
+        return x, stats
+
     def SolveRobinHood(self, b=None, tol=1e-8, x0=None, check_interval=0, max_subiterations=0, assembled=False,
                        raise_on_failure=True):
         """Robin Hood charge-density solve (KRobinHood<double>::Solve); returns (x, stats dict).
@@ -244,6 +279,15 @@ class CUDAElectrostaticContext:
         fields of kemcu_fftm_params (degree, top_level_divisions, divisions, zeromask,
         maximum_tree_depth, insertion_ratio, region_expansion_factor, world_center,
         world_length, near_analytic); the others keep their defaults."""
+        self._check(N.lib().kemcu_fftm_configure(self._h, C.byref(self._fftm_params(params))))
+
+    def ConfigureFFTMPreconditioner(self, **params):
+        """Builds the tree whose operator the implicit Krylov preconditioner inverts
+        (KrylovSolve with preconditioner_mode=SOLVE_FFTM); keyword arguments as ConfigureFFTM."""
+        self._check(N.lib().kemcu_fftm_configure_preconditioner(self._h, C.byref(self._fftm_params(params))))
+
+    @staticmethod
+    def _fftm_params(params):
         prm = N.FftmParams()
         N.lib().kemcu_fftm_default_params(C.byref(prm))
         for k, v in params.items():
@@ -254,7 +298,7 @@ class CUDAElectrostaticContext:
                 setattr(prm, k, float(v))
             else:
                 setattr(prm, k, int(v))
-        self._check(N.lib().kemcu_fftm_configure(self._h, C.byref(prm)))
+        return prm
 
     def FFTMField(self, P, what=FIELD_AND_POTENTIAL):
         """n x 4 (Ex, Ey, Ez, phi) by the fast multipole method."""

@@ -19,6 +19,8 @@ FP64, MIXED, FP32 = 0, 1, 2
 FIELD_AND_POTENTIAL, POTENTIAL, FIELD = 0, 1, 2
 SOLVE_PLAIN, SOLVE_MIXED, SOLVE_ASSEMBLED, SOLVE_ASSEMBLED_FP64, SOLVE_FP32, SOLVE_FFTM = 0, 1, 2, 3, 4, 5
 TRACK_ACTIVE, TRACK_HIT, TRACK_MAX_STEPS, TRACK_LEFT, TRACK_NONFINITE = 0, 1, 2, 3, 4
+KRYLOV_GMRES, KRYLOV_BICGSTAB = 0, 1
+PRECON_NONE, PRECON_JACOBI, PRECON_IMPLICIT_KRYLOV = 0, 1, 2
 
 _ERRNAMES = {EINVAL: "EINVAL", ECUDA: "ECUDA", ENONFINITE: "ENONFINITE", ENOTCONVERGED: "ENOTCONVERGED",
              ETIMEOUT: "ETIMEOUT", ENOMEM: "ENOMEM", ESTATE: "ESTATE"}
@@ -59,6 +61,14 @@ class FftmParams(C.Structure):
                 ("zeromask", C.c_int), ("maximum_tree_depth", C.c_int), ("insertion_ratio", C.c_double),
                 ("region_expansion_factor", C.c_double), ("world_center", C.c_double * 3),
                 ("world_length", C.c_double), ("near_analytic", C.c_int)]
+
+
+
+class KrylovParams(C.Structure):
+    _fields_ = [("solver", C.c_int), ("mode", C.c_int), ("tolerance", C.c_double), ("max_iterations", C.c_int),
+                ("iterations_between_restarts", C.c_int), ("preconditioner", C.c_int),
+                ("preconditioner_mode", C.c_int), ("preconditioner_tolerance", C.c_double),
+                ("max_preconditioner_iterations", C.c_int)]
 
 
 ITER_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_double)
@@ -142,6 +152,10 @@ def lib():
     L.kemcu_fftm_default_params.argtypes = [C.POINTER(FftmParams)]
     L.kemcu_fftm_default_params.restype = None
     L.kemcu_fftm_configure.argtypes = [vp, C.POINTER(FftmParams)]
+    L.kemcu_fftm_configure_preconditioner.argtypes = [vp, C.POINTER(FftmParams)]
+    L.kemcu_krylov_default_params.argtypes = [C.POINTER(KrylovParams)]
+    L.kemcu_krylov_default_params.restype = None
+    L.kemcu_krylov_solve.argtypes = [vp, _dp, _dp, C.c_int, C.POINTER(KrylovParams), C.POINTER(SolveStats)]
     L.kemcu_fftm_field.argtypes = [vp, _dp, C.c_size_t, _dp, C.c_int]
     L.kemcu_fftm_field_dev.argtypes = [vp, C.c_void_p, C.c_size_t, C.c_void_p, C.c_int]
     L.kemcu_fftm_info.argtypes = [vp, _dp, _ip]

@@ -73,7 +73,7 @@ struct kemcu_ctx
     int* d_near_row = nullptr;
     double* d_near_val = nullptr;
     // grow-only scratch
-    DevBuf scratch[9];
+    DevBuf scratch[16];
     unsigned* d_counter = nullptr;
     int* d_flag = nullptr;
     double* noalloc_scratch = nullptr;  // device address of g_noalloc_scratch on this context's device
@@ -91,10 +91,11 @@ struct kemcu_ctx
     int pending_key = -1, pending_variant = -1;
     cudaEvent_t tv0 = nullptr, tv1 = nullptr;
     FmState* fm = nullptr;  // the fast multipole tree of the current geometry (kemcu_fftm_configure)
+    FmState* fm_pre = nullptr;  // the preconditioner's tree (kemcu_fftm_configure_preconditioner)
 };
 
 void fm_release(kemcu_ctx* ctx);
-int fm_apply(kemcu_ctx* ctx, const double* d_x, double* d_y, int nrhs);
+int fm_apply(kemcu_ctx* ctx, FmState* S, const double* d_x, double* d_y, int nrhs);
 
 namespace
 {
@@ -108,8 +109,13 @@ enum Scratch
     sVec2,
     sBasis,
     sMisc,
-    sSort  // Morton-ordering workspace of kemcu_field_dev (never aliases a caller's staging slot)
+    sSort,  // Morton-ordering workspace of kemcu_field_dev (never aliases a caller's staging slot)
+    sZ,     // preconditioned Krylov basis (flexible GMRES) or the Jacobi-scaled vector
+    sKry,   // BiCGStab vectors
+    sInBasis, sInW, sInMisc, sInK,  // the inner GMRES of the implicit Krylov preconditioner
+    kNumScratch
 };
+static_assert(kNumScratch <= 16, "kemcu_ctx::scratch holds 16 slots");
 
 int fail(kemcu_ctx* c, int code, const char* fmt, ...)
 {
@@ -581,14 +587,15 @@ enum OpKind
     kDense64,
     kDense32,
     kFree32,  // matrix-free with the FP32 far-field form
-    kFftm     // the fast multipole operator (kemcu_fftm_configure)
+    kFftm,    // the fast multipole operator (kemcu_fftm_configure)
+    kFftmPre  // the preconditioner's fast multipole operator (kemcu_fftm_configure_preconditioner)
 };
 
 int apply_op(kemcu_ctx* ctx, int op, const double* d_x, double* d_y, int nrhs)
 {
     const int n = (int) ctx->n;
-    if (op == kFftm)
-        return fm_apply(ctx, d_x, d_y, nrhs);
+    if (op == kFftm || op == kFftmPre)
+        return fm_apply(ctx, op == kFftm ? ctx->fm : ctx->fm_pre, d_x, d_y, nrhs);
     if ((op == kFree64 || op == kFreeMixed || op == kFree32) && ctx->axisym) {
         const int split = axisym_split(ctx->num_sms, n, n);
         double* partial = nullptr;
@@ -743,163 +750,275 @@ int assemble(kemcu_ctx* ctx, bool want32)
 }
 
 // ------------------------------------------------------------------------------- GMRES
-// GMRES(m) without restart from x0 = 0, as KGeneralizedMinimalResidual (x = V y, residual
-// estimate |p_{j+1}| relative to |b|). Orthogonalisation is classical Gram-Schmidt applied
-// twice (CGS2), which is as accurate as the reference's modified Gram-Schmidt and reads the
-// basis with two batched passes instead of j sequential ones. The j x j triangular solve
-// uses back-substitution (KGeneralizedMinimalResidual::UseBackSubstitution).
+// GMRES from x0 = 0, as KGeneralizedMinimalResidual (x = V y, residual estimate |p_{j+1}|
+// relative to |b|), with the restarts of KIterativeKrylovRestartCondition (every `restart`
+// iterations: x += V y, r = b - A x, a new Krylov space from r; 0 = never) and the right
+// preconditioning of KPreconditionedGeneralizedMinimalResidual (w = A P v_j; x += P V y for a
+// stationary P, x += Z y with the kept Z_j = P v_j otherwise). The reference forms x from the
+// last cycle's basis alone (KGeneralizedMinimalResidual.hh UpdateSolution clears x), which after
+// a restart drops the earlier cycles' part; here every cycle adds its correction, so a restarted
+// solve converges to the same solution as an unrestarted one. Orthogonalisation is classical
+// Gram-Schmidt applied twice (CGS2), which is as accurate as the reference's modified
+// Gram-Schmidt and reads the basis with two batched passes instead of j sequential ones. The
+// j x j triangular solve uses back-substitution (KGeneralizedMinimalResidual::UseBackSubstitution).
 // basis entries (n x (j+1)) up to which one CTA per RHS orthogonalises (arnoldi_small_kernel)
 constexpr size_t kArnoldiSmall = (size_t) 1 << 16;
 
+// Right preconditioner of a Krylov solve (KPreconditioner, KEMField/Source/LinearAlgebra/
+// Preconditioners): Jacobi scales by the inverse diagonal (KJacobiPreconditioner.hh,
+// stationary); the implicit Krylov form runs an inner GMRES from zero on its own operator to a
+// relative tolerance (KImplicitKrylovPreconditioner.hh:50-54, not stationary).
+struct Precond
+{
+    int kind = KEMCU_PRECON_NONE;
+    const double* dinv = nullptr;  // Jacobi: 1 / A(i, i), n values
+    int op = kFree64;              // implicit Krylov: the inner operator, tolerance and iterations
+    double tol = 0.01;
+    int max_iter = 30;
+    int inner_iters = 0;           // accumulated over the applications
+    int inner_matvecs = 0;
+};
+
+// workspace slots of one GMRES: the outer solve's, or those of the implicit Krylov
+// preconditioner's inner solve (which runs inside an outer iteration)
+struct KrylovSlots
+{
+    int basis, w, misc, k;
+};
+constexpr KrylovSlots kOuterSlots{sBasis, sVec2, sMisc, sVec1};
+constexpr KrylovSlots kInnerSlots{sInBasis, sInW, sInMisc, sInK};
+
+int apply_precond(kemcu_ctx* ctx, Precond& pc, const double* d_in, double* d_out, int nrhs);
+
 int gmres_core(kemcu_ctx* ctx, int op, const double* d_b, double* d_x, int nrhs, double tol, int max_iter,
-               int& iters, double& est, int& matvecs)
+               int& iters, double& est, int& matvecs, int restart = 0, Precond* pc = nullptr,
+               const KrylovSlots& sl = kOuterSlots)
 {
     const int n = (int) ctx->n;
-    const int m = std::max(1, max_iter);
+    const int m = std::max(1, restart > 0 ? std::min(restart, max_iter) : max_iter);  // iterations per cycle
     const int hs = m + 2;
-    void *pV, *pW, *pH, *pP;
+    const bool flexible = pc && pc->kind == KEMCU_PRECON_IMPLICIT_KRYLOV;
+    const bool jacobi = pc && pc->kind == KEMCU_PRECON_JACOBI;
+    const bool outer = sl.basis == sBasis;
+    void *pV, *pW, *pH, *pZ = nullptr;
     int rc;
-    if ((rc = ensure(ctx, sBasis, (size_t) (m + 1) * nrhs * n * sizeof(double), &pV)))
+    if ((rc = ensure(ctx, sl.basis, (size_t) (m + 1) * nrhs * n * sizeof(double), &pV)))
         return rc;
-    if ((rc = ensure(ctx, sVec2, (size_t) nrhs * n * sizeof(double), &pW)))
+    if ((rc = ensure(ctx, sl.w, (size_t) nrhs * n * sizeof(double), &pW)))
         return rc;
-    if ((rc = ensure(ctx, sMisc, (size_t) nrhs * hs * 3 * sizeof(double) + 64 * (size_t) nrhs * kDotBlocks * sizeof(double), &pH)))
+    if ((rc = ensure(ctx, sl.misc, (size_t) nrhs * hs * 3 * sizeof(double) + 64 * (size_t) nrhs * kDotBlocks * sizeof(double), &pH)))
+        return rc;
+    // the preconditioned basis (flexible), or one vector for the Jacobi-scaled v_j and P V y
+    if ((flexible || jacobi) && (rc = ensure(ctx, sZ, (size_t) (flexible ? m : 1) * nrhs * n * sizeof(double), &pZ)))
         return rc;
     double* V = (double*) pV;
     double* w = (double*) pW;
+    double* Z = (double*) pZ;
     double* h = (double*) pH;             // [nrhs][hs] first projection
     double* h2 = h + (size_t) nrhs * hs;  // [nrhs][hs] second projection / norms
     double* yv = h2 + (size_t) nrhs * hs; // [nrhs][hs] solution coefficients
     double* part = yv + (size_t) nrhs * hs;
-    (void) pP;
+    void* pk;
+    if ((rc = ensure(ctx, sl.k, (size_t) nrhs * sizeof(int) + 256, &pk)))
+        return rc;
+    int* d_k = (int*) pk;
     const dim3 vg((n + 255) / 256, nrhs);
-    // |b| and v0 = b / |b|
-    KC(cudaMemcpyAsync(V, d_b, (size_t) nrhs * n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-    multi_dot_kernel<<<dim3(kDotBlocks, nrhs), kDotThreads, 0, ctx->stream>>>(V, V, n, nrhs, 0, 1, part, ctx->d_counter, h2, hs);
-    KCHECK_LAUNCH();
-    scale_kernel<<<vg, 256, 0, ctx->stream>>>(V, V, n, h2, hs, 0);
-    KCHECK_LAUNCH();
+    const size_t vec = (size_t) nrhs * n;
+    // x0 = 0, r0 = b
+    KC(cudaMemsetAsync(d_x, 0, vec * sizeof(double), ctx->stream));
+    KC(cudaMemcpyAsync(V, d_b, vec * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     std::vector<double> hb((size_t) nrhs * hs);
-    KC(cudaMemcpyAsync(hb.data(), h2, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    KC(cudaStreamSynchronize(ctx->stream));
-    std::vector<double> bnorm(nrhs), p((size_t) nrhs * hs, 0.), cs((size_t) nrhs * hs), sn((size_t) nrhs * hs);
+    std::vector<double> bnorm(nrhs, 0.), p((size_t) nrhs * hs, 0.), cs((size_t) nrhs * hs), sn((size_t) nrhs * hs);
     std::vector<std::vector<double>> H(nrhs);  // column-major R, one column of hs added per iteration
     std::vector<int> kfin(nrhs, 0);
     std::vector<char> done(nrhs, 0);
-    for (int r = 0; r < nrhs; r++) {
-        bnorm[r] = std::sqrt(hb[(size_t) r * hs]);
-        p[(size_t) r * hs] = bnorm[r];
-        if (!(bnorm[r] > 0.))
-            done[r] = 1;
-    }
+    std::vector<double> hcol((size_t) nrhs * hs), hcol2((size_t) nrhs * hs), b2((size_t) nrhs * hs);
+    std::vector<double> y((size_t) nrhs * hs);
     iters = 0;
     est = 0.;
-    std::vector<double> hcol((size_t) nrhs * hs), hcol2((size_t) nrhs * hs);
-    for (int j = 0; j < m; j++) {
+    bool stop = false;
+    for (int cycle = 0;; cycle++) {
+        // |r| and v0 = r / |r|
+        multi_dot_kernel<<<dim3(kDotBlocks, nrhs), kDotThreads, 0, ctx->stream>>>(V, V, n, nrhs, 0, 1, part, ctx->d_counter, h2, hs);
+        KCHECK_LAUNCH();
+        scale_kernel<<<vg, 256, 0, ctx->stream>>>(V, V, n, h2, hs, 0);
+        KCHECK_LAUNCH();
+        KC(cudaMemcpyAsync(hb.data(), h2, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        KC(cudaStreamSynchronize(ctx->stream));
+        std::fill(p.begin(), p.end(), 0.);
+        double worst0 = 0.;
+        for (int r = 0; r < nrhs; r++) {
+            const double rn = std::sqrt(hb[(size_t) r * hs]);
+            if (cycle == 0)
+                bnorm[r] = rn;
+            p[(size_t) r * hs] = rn;
+            kfin[r] = 0;
+            H[r].clear();
+            if (cycle > 0 && !done[r] && bnorm[r] > 0.)
+                worst0 = std::max(worst0, rn / bnorm[r]);
+            if (!(bnorm[r] > 0.) || (cycle > 0 && rn <= tol * bnorm[r]))
+                done[r] = 1;
+        }
+        if (cycle > 0)
+            est = worst0;  // the restarted residual, until the new cycle's first estimate
+        for (int j = 0; j < m && iters < max_iter; j++) {
+            bool all = true;
+            for (int r = 0; r < nrhs; r++)
+                all = all && done[r];
+            if (all)
+                break;
+            double* vj = V + (size_t) j * vec;
+            double* vn = V + (size_t) (j + 1) * vec;
+            const double* src = vj;
+            if (jacobi) {
+                diag_scale_kernel<<<vg, 256, 0, ctx->stream>>>(pc->dinv, vj, Z, n, 0);
+                KCHECK_LAUNCH();
+                src = Z;
+            }
+            else if (flexible) {
+                double* zj = Z + (size_t) j * vec;
+                if ((rc = apply_precond(ctx, *pc, vj, zj, nrhs)))
+                    return rc;
+                src = zj;
+            }
+            if ((rc = apply_op(ctx, op, src, w, nrhs)))
+                return rc;
+            matvecs++;
+            if ((size_t) n * (size_t) (j + 1) <= kArnoldiSmall) {
+                // one CTA per RHS: both Gram-Schmidt passes, the norm and the new basis vector
+                arnoldi_small_kernel<<<nrhs, kArnoldiThreads, 0, ctx->stream>>>(V, w, n, nrhs, j, h, hs);
+                KCHECK_LAUNCH();
+                KC(cudaMemcpyAsync(hcol.data(), h, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+                KC(cudaStreamSynchronize(ctx->stream));
+                for (int r = 0; r < nrhs; r++) {
+                    const double beta = hcol[(size_t) r * hs + hs - 1];
+                    b2[(size_t) r * hs] = beta * beta;
+                    for (int k = 0; k <= j; k++)
+                        hcol2[(size_t) r * hs + k] = 0.;
+                }
+            }
+            else {
+                for (int pass = 0; pass < 2; pass++) {
+                    double* hh = pass == 0 ? h : h2;
+                    for (int k0 = 0; k0 <= j; k0 += 64) {
+                        const int nk = std::min(64, j + 1 - k0);
+                        multi_dot_kernel<<<dim3(kDotBlocks, nrhs), kDotThreads, 0, ctx->stream>>>(V, w, n, nrhs, k0, nk,
+                                                                                                 part, ctx->d_counter, hh, hs);
+                        KCHECK_LAUNCH();
+                    }
+                    for (int k0 = 0; k0 <= j; k0 += 64) {
+                        const int nk = std::min(64, j + 1 - k0);
+                        gs_update_kernel<<<vg, 256, 0, ctx->stream>>>(V, w, n, nrhs, k0, nk, hh, hs, nullptr);
+                        KCHECK_LAUNCH();
+                    }
+                }
+                // beta^2 into yv[r][0]
+                multi_dot_kernel<<<dim3(kDotBlocks, nrhs), kDotThreads, 0, ctx->stream>>>(w, w, n, nrhs, 0, 1, part,
+                                                                                         ctx->d_counter, yv, hs);
+                KCHECK_LAUNCH();
+                scale_kernel<<<vg, 256, 0, ctx->stream>>>(w, vn, n, yv, hs, 0);
+                KCHECK_LAUNCH();
+                KC(cudaMemcpyAsync(hcol.data(), h, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+                KC(cudaMemcpyAsync(hcol2.data(), h2, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+                KC(cudaMemcpyAsync(b2.data(), yv, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+                KC(cudaStreamSynchronize(ctx->stream));
+            }
+            iters++;
+            double worst = 0.;
+            for (int r = 0; r < nrhs; r++) {
+                if (done[r])
+                    continue;
+                H[r].resize((size_t) (j + 1) * hs, 0.);
+                double* col = H[r].data() + (size_t) j * hs;
+                for (int k = 0; k <= j; k++)
+                    col[k] = hcol[(size_t) r * hs + k] + hcol2[(size_t) r * hs + k];
+                const double beta = std::sqrt(b2[(size_t) r * hs]);
+                // apply previous Givens rotations (KGeneralizedMinimalResidual.hh:240-246)
+                for (int k = 0; k < j; k++) {
+                    const double a = col[k], b = col[k + 1];
+                    col[k] = cs[(size_t) r * hs + k] * a + sn[(size_t) r * hs + k] * b;
+                    col[k + 1] = -sn[(size_t) r * hs + k] * a + cs[(size_t) r * hs + k] * b;
+                }
+                const double gam = std::sqrt(col[j] * col[j] + beta * beta);
+                cs[(size_t) r * hs + j] = col[j] / gam;
+                sn[(size_t) r * hs + j] = beta / gam;
+                col[j] = gam;
+                p[(size_t) r * hs + j + 1] = -sn[(size_t) r * hs + j] * p[(size_t) r * hs + j];
+                p[(size_t) r * hs + j] = cs[(size_t) r * hs + j] * p[(size_t) r * hs + j];
+                const double rel = std::fabs(p[(size_t) r * hs + j + 1]) / bnorm[r];
+                kfin[r] = j + 1;
+                if (rel <= tol || !(beta > 0.))
+                    done[r] = 1;
+                worst = std::max(worst, rel);
+            }
+            est = worst;
+            if (outer && ctx->cb && ctx->cb(ctx->cb_user, iters, worst)) {
+                stop = true;
+                break;
+            }
+        }
+        // y = R^-1 p; x += V y (P V y for Jacobi, Z y for the flexible form)
+        std::fill(y.begin(), y.end(), 0.);
+        for (int r = 0; r < nrhs; r++) {
+            const int k = kfin[r];
+            for (int i = k - 1; i >= 0; i--) {
+                double s = p[(size_t) r * hs + i];
+                for (int c = i + 1; c < k; c++)
+                    s -= H[r][(size_t) c * hs + i] * y[(size_t) r * hs + c];
+                y[(size_t) r * hs + i] = s / H[r][(size_t) i * hs + i];
+            }
+        }
+        KC(cudaMemcpyAsync(yv, y.data(), (size_t) nrhs * hs * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        KC(cudaMemcpyAsync(d_k, kfin.data(), (size_t) nrhs * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        if (flexible) {
+            combine_kernel<<<vg, 256, 0, ctx->stream>>>(Z, yv, hs, n, nrhs, d_k, d_x);
+            KCHECK_LAUNCH();
+        }
+        else if (jacobi) {
+            KC(cudaMemsetAsync(Z, 0, vec * sizeof(double), ctx->stream));
+            combine_kernel<<<vg, 256, 0, ctx->stream>>>(V, yv, hs, n, nrhs, d_k, Z);
+            KCHECK_LAUNCH();
+            diag_scale_kernel<<<vg, 256, 0, ctx->stream>>>(pc->dinv, Z, d_x, n, 1);
+            KCHECK_LAUNCH();
+        }
+        else {
+            combine_kernel<<<vg, 256, 0, ctx->stream>>>(V, yv, hs, n, nrhs, d_k, d_x);
+            KCHECK_LAUNCH();
+        }
         bool all = true;
         for (int r = 0; r < nrhs; r++)
             all = all && done[r];
-        if (all)
+        if (all || stop || iters >= max_iter || restart <= 0)
             break;
-        double* vj = V + (size_t) j * nrhs * n;
-        double* vn = V + (size_t) (j + 1) * nrhs * n;
-        if ((rc = apply_op(ctx, op, vj, w, nrhs)))
+        // restart from the current solution: r = b - A x into V[0]
+        if ((rc = apply_op(ctx, op, d_x, V, nrhs)))
             return rc;
         matvecs++;
-        std::vector<double> b2(nrhs * (size_t) hs);
-        if ((size_t) n * (size_t) (j + 1) <= kArnoldiSmall) {
-            // one CTA per RHS: both Gram-Schmidt passes, the norm and the new basis vector
-            arnoldi_small_kernel<<<nrhs, kArnoldiThreads, 0, ctx->stream>>>(V, w, n, nrhs, j, h, hs);
-            KCHECK_LAUNCH();
-            KC(cudaMemcpyAsync(hcol.data(), h, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-            KC(cudaStreamSynchronize(ctx->stream));
-            for (int r = 0; r < nrhs; r++) {
-                const double beta = hcol[(size_t) r * hs + hs - 1];
-                b2[(size_t) r * hs] = beta * beta;
-                for (int k = 0; k <= j; k++)
-                    hcol2[(size_t) r * hs + k] = 0.;
-            }
-        }
-        else {
-            for (int pass = 0; pass < 2; pass++) {
-                double* hh = pass == 0 ? h : h2;
-                for (int k0 = 0; k0 <= j; k0 += 64) {
-                    const int nk = std::min(64, j + 1 - k0);
-                    multi_dot_kernel<<<dim3(kDotBlocks, nrhs), kDotThreads, 0, ctx->stream>>>(V, w, n, nrhs, k0, nk,
-                                                                                             part, ctx->d_counter, hh, hs);
-                    KCHECK_LAUNCH();
-                }
-                for (int k0 = 0; k0 <= j; k0 += 64) {
-                    const int nk = std::min(64, j + 1 - k0);
-                    gs_update_kernel<<<vg, 256, 0, ctx->stream>>>(V, w, n, nrhs, k0, nk, hh, hs, nullptr);
-                    KCHECK_LAUNCH();
-                }
-            }
-            // beta^2 into yv[r][0]
-            multi_dot_kernel<<<dim3(kDotBlocks, nrhs), kDotThreads, 0, ctx->stream>>>(w, w, n, nrhs, 0, 1, part,
-                                                                                     ctx->d_counter, yv, hs);
-            KCHECK_LAUNCH();
-            scale_kernel<<<vg, 256, 0, ctx->stream>>>(w, vn, n, yv, hs, 0);
-            KCHECK_LAUNCH();
-            KC(cudaMemcpyAsync(hcol.data(), h, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-            KC(cudaMemcpyAsync(hcol2.data(), h2, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-            KC(cudaMemcpyAsync(b2.data(), yv, (size_t) nrhs * hs * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-            KC(cudaStreamSynchronize(ctx->stream));
-        }
-        iters = j + 1;
-        double worst = 0.;
-        for (int r = 0; r < nrhs; r++) {
-            if (done[r])
-                continue;
-            H[r].resize((size_t) (j + 1) * hs, 0.);
-            double* col = H[r].data() + (size_t) j * hs;
-            for (int k = 0; k <= j; k++)
-                col[k] = hcol[(size_t) r * hs + k] + hcol2[(size_t) r * hs + k];
-            const double beta = std::sqrt(b2[(size_t) r * hs]);
-            // apply previous Givens rotations (KGeneralizedMinimalResidual.hh:240-246)
-            for (int k = 0; k < j; k++) {
-                const double a = col[k], b = col[k + 1];
-                col[k] = cs[(size_t) r * hs + k] * a + sn[(size_t) r * hs + k] * b;
-                col[k + 1] = -sn[(size_t) r * hs + k] * a + cs[(size_t) r * hs + k] * b;
-            }
-            const double gam = std::sqrt(col[j] * col[j] + beta * beta);
-            cs[(size_t) r * hs + j] = col[j] / gam;
-            sn[(size_t) r * hs + j] = beta / gam;
-            col[j] = gam;
-            p[(size_t) r * hs + j + 1] = -sn[(size_t) r * hs + j] * p[(size_t) r * hs + j];
-            p[(size_t) r * hs + j] = cs[(size_t) r * hs + j] * p[(size_t) r * hs + j];
-            const double rel = std::fabs(p[(size_t) r * hs + j + 1]) / bnorm[r];
-            kfin[r] = j + 1;
-            if (rel <= tol || !(beta > 0.))
-                done[r] = 1;
-            worst = std::max(worst, rel);
-        }
-        est = worst;
-        if (ctx->cb && ctx->cb(ctx->cb_user, iters, worst))
-            break;
+        residual_kernel<<<(unsigned) ((vec + 255) / 256), 256, 0, ctx->stream>>>(d_b, V, vec);
+        KCHECK_LAUNCH();
     }
-    // y = R^-1 p, x = V y
-    std::vector<double> y((size_t) nrhs * hs, 0.);
-    for (int r = 0; r < nrhs; r++) {
-        const int k = kfin[r];
-        for (int i = k - 1; i >= 0; i--) {
-            double s = p[(size_t) r * hs + i];
-            for (int c = i + 1; c < k; c++)
-                s -= H[r][(size_t) c * hs + i] * y[(size_t) r * hs + c];
-            y[(size_t) r * hs + i] = s / H[r][(size_t) i * hs + i];
-        }
-    }
-    int* d_k;
-    void* pk;
-    if ((rc = ensure(ctx, sVec1, (size_t) nrhs * sizeof(int) + 256, &pk)))
-        return rc;
-    d_k = (int*) pk;
-    KC(cudaMemcpyAsync(yv, y.data(), (size_t) nrhs * hs * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    KC(cudaMemcpyAsync(d_k, kfin.data(), (size_t) nrhs * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-    KC(cudaMemsetAsync(d_x, 0, (size_t) nrhs * n * sizeof(double), ctx->stream));
-    combine_kernel<<<vg, 256, 0, ctx->stream>>>(V, yv, hs, n, nrhs, d_k, d_x);
-    KCHECK_LAUNCH();
     KC(cudaStreamSynchronize(ctx->stream));
+    return KEMCU_OK;
+}
+
+// z = P v: Jacobi scaling, or the implicit Krylov preconditioner's inner GMRES from zero
+int apply_precond(kemcu_ctx* ctx, Precond& pc, const double* d_in, double* d_out, int nrhs)
+{
+    const int n = (int) ctx->n;
+    if (pc.kind == KEMCU_PRECON_JACOBI) {
+        diag_scale_kernel<<<dim3((n + 255) / 256, nrhs), 256, 0, ctx->stream>>>(pc.dinv, d_in, d_out, n, 0);
+        KCHECK_LAUNCH();
+        return KEMCU_OK;
+    }
+    if (pc.kind == KEMCU_PRECON_IMPLICIT_KRYLOV) {
+        int it = 0, mv = 0;
+        double e = 0.;
+        int rc = gmres_core(ctx, pc.op, d_in, d_out, nrhs, pc.tol, pc.max_iter, it, e, mv, 0, nullptr, kInnerSlots);
+        pc.inner_iters += it;
+        pc.inner_matvecs += mv;
+        return rc;
+    }
+    KC(cudaMemcpyAsync(d_out, d_in, (size_t) nrhs * n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     return KEMCU_OK;
 }
 
@@ -1659,3 +1778,4 @@ int kemcu_rule_nodes(int which, double* out)
 #include "kemcu_adjoint_host.inc"
 #include "kemcu_robinhood_host.inc"
 #include "kemcu_fftm_host.inc"
+#include "kemcu_krylov_host.inc"

@@ -213,6 +213,121 @@ __global__ void __launch_bounds__(kArnoldiThreads) arnoldi_small_kernel(double* 
         vn[i] = beta > 0. ? wr[i] * (1. / beta) : 0.;
 }
 
+// y[r][i] = d[i] x[r][i], or y[r][i] += d[i] x[r][i] when accumulate (the Jacobi
+// preconditioner, KJacobiPreconditioner.hh:40-45, and its use in forming the GMRES solution);
+// grid (ceil(n/256), nrhs)
+__global__ void diag_scale_kernel(const double* __restrict__ d, const double* __restrict__ x, double* __restrict__ y,
+                                  int n, int accumulate)
+{
+    const int r = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const double v = d[i] * x[(size_t) r * n + i];
+    y[(size_t) r * n + i] = accumulate ? y[(size_t) r * n + i] + v : v;
+}
+
+// d[i] = 1 / d[i]
+__global__ void invert_kernel(double* __restrict__ d, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        d[i] = 1. / d[i];
+}
+
+// up to three inner products per right-hand side in one launch (BiCGStab's scalars):
+// out[r][q] = sum_i a_q[r][i] b_q[r][i] for q < np, out row stride 4. grid (kDotBlocks, nrhs);
+// partial[r][q][blk]; counter[r] starts at 0 and is reset. Each CTA sums a slice of the rows,
+// the last CTA of a right-hand side sums the slices in block order (scheduling-independent).
+struct DotPairs
+{
+    const double* a[3];
+    const double* b[3];
+    int np;
+};
+__global__ void __launch_bounds__(kDotThreads) pair_dot_kernel(DotPairs dp, int n, double* __restrict__ partial,
+                                                               unsigned* __restrict__ counter, double* __restrict__ out)
+{
+    __shared__ double sh[32];
+    __shared__ bool last;
+    const int r = blockIdx.y;
+    const int per = (n + gridDim.x - 1) / gridDim.x;
+    const int i0 = blockIdx.x * per, i1 = min(n, i0 + per);
+    double acc[3] = {0., 0., 0.};
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        const size_t k = (size_t) r * n + i;
+#pragma unroll
+        for (int q = 0; q < 3; q++)
+            if (q < dp.np)
+                acc[q] = fma(dp.a[q][k], dp.b[q][k], acc[q]);
+    }
+    for (int q = 0; q < dp.np; q++) {
+        const double s = block_sum(acc[q], sh);
+        if (threadIdx.x == 0)
+            partial[((size_t) r * 4 + q) * gridDim.x + blockIdx.x] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0)
+        last = atomicAdd(counter + r, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last)
+        return;
+    __threadfence();
+    if (threadIdx.x < dp.np) {
+        double s = 0.;
+        for (int b = 0; b < (int) gridDim.x; b++)
+            s += __ldcg(partial + ((size_t) r * 4 + threadIdx.x) * gridDim.x + b);
+        out[(size_t) r * 4 + threadIdx.x] = s;
+    }
+    if (threadIdx.x == 0)
+        counter[r] = 0u;
+}
+
+// per-right-hand-side coefficients of a BiCGStab vector update
+struct RhsCoef
+{
+    double a[kMaxRhs], b[kMaxRhs];
+};
+
+// p = r + beta (p - omega v)  (a = beta, b = omega; KBiconjugateGradientStabilized.hh:162-164)
+__global__ void bicg_direction_kernel(const double* __restrict__ r, const double* __restrict__ v, double* __restrict__ p,
+                                      int n, RhsCoef c)
+{
+    const int q = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const size_t k = (size_t) q * n + i;
+    p[k] = r[k] + c.a[q] * (p[k] - c.b[q] * v[k]);
+}
+
+// s = r - alpha v  (a = alpha; :170-172)
+__global__ void bicg_half_kernel(const double* __restrict__ r, const double* __restrict__ v, double* __restrict__ s,
+                                 int n, RhsCoef c)
+{
+    const int q = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const size_t k = (size_t) q * n + i;
+    s[k] = r[k] - c.a[q] * v[k];
+}
+
+// x += alpha y + omega z, r = s - omega t  (a = alpha, b = omega; :178-181)
+__global__ void bicg_update_kernel(const double* __restrict__ y, const double* __restrict__ z,
+                                   const double* __restrict__ s, const double* __restrict__ t, double* __restrict__ x,
+                                   double* __restrict__ r, int n, RhsCoef c)
+{
+    const int q = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const size_t k = (size_t) q * n + i;
+    x[k] = x[k] + c.a[q] * y[k] + c.b[q] * z[k];
+    r[k] = s[k] - c.b[q] * t[k];
+}
+
 // non-finite check: flag[0] |= 1 when any value is NaN or Inf
 __global__ void finite_kernel(const double* __restrict__ v, size_t n, int* __restrict__ flag)
 {

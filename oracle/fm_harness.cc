@@ -15,10 +15,15 @@
 //                        KFastMultipoleMatrixGenerator.cc:23-41: dense far part from the local
 //                        expansions, sparse near part by the numeric integrator), x and y in
 //                        container order
+//   kemref_fm_bvs        the reference's fast-multipole charge-density solve
+//                        (KFMElectrostaticFastMultipoleBoundaryValueSolver.cc:189-233, the solver of
+//                        krylov_bem_solver): gmres or bicgstab, preconditioner none, jacobi,
+//                        implicit_krylov or independent_implicit_krylov, restarts
 //   kemref_fm_field      the whole reference FFTM field solver on a container made by
 //                        ref_harness.cc's kemref_create: KFMElectrostaticTreeConstructor with the
 //                        single-threaded field mapper, then KFMElectrostaticFastMultipoleFieldSolver
 //                        (KFMElectrostaticFastMultipoleFieldSolver.cc:47-163) at each point
+#include "KFMElectrostaticFastMultipoleBoundaryValueSolver.hh"
 #include "KFMElectrostaticFastMultipoleFieldSolver.hh"
 #include "KFMElectrostaticLocalCoefficientFieldCalculator.hh"
 #include "KFMElectrostaticLocalCoefficientSet.hh"
@@ -44,6 +49,8 @@
 using namespace KEMField;
 
 extern "C" void* kemref_container(void* h);
+extern "C" void kemref_set_sigma(void* h, const double* sigma);
+extern "C" void kemref_get_sigma(void* h, double* sigma);
 
 extern "C" {
 
@@ -212,6 +219,68 @@ int kemref_fm_field(void* h, const int* ip, const double* dp, int n, const doubl
         out4[4 * i + 2] = E[2];
         out4[4 * i + 3] = solver.Potential(p);
     }
+    return 0;
+}
+}
+
+namespace
+{
+KFMElectrostaticParameters fm_params(const int* ip, const double* dp)
+{
+    KFMElectrostaticParameters params;
+    params.strategy = KFMSubdivisionStrategy::Aggressive;
+    params.degree = ip[0];
+    params.top_level_divisions = ip[1];
+    params.divisions = ip[2];
+    params.zeromask = ip[3];
+    params.maximum_tree_depth = ip[4];
+    params.insertion_ratio = dp[0];
+    params.region_expansion_factor = dp[1];
+    params.use_region_estimation = true;
+    params.use_caching = false;
+    params.verbosity = 0;
+    return params;
+}
+}  // namespace
+
+extern "C" {
+// ip, dp: the solver tree's parameters as kemref_fm_matvec; solver "gmres" or "bicgstab";
+// precon "none", "jacobi", "implicit_krylov" (degree precon_degree on the solver's tree) or
+// "independent_implicit_krylov" (the tree of pip, pdp); restart 0 = never. x receives the
+// solution in container order (from zero charge densities), *resid the solver's residual norm
+// over |b|.
+int kemref_fm_bvs(void* h, const int* ip, const double* dp, const char* solver, const char* precon, double tol,
+                  int max_iter, int restart, double precon_tol, int precon_max_iter, int precon_degree,
+                  const int* pip, const double* pdp, double* x, double* resid)
+{
+    auto* container = static_cast<KSurfaceContainer*>(kemref_container(h));
+    const std::vector<double> zeros(container->size(), 0.);
+    kemref_set_sigma(h, zeros.data());
+    char tmpl[] = "/tmp/kemref_fmXXXXXX";
+    if (!mkdtemp(tmpl))
+        return -1;
+    const std::string dir(tmpl);
+    KEMFileInterface::GetInstance()->ActiveDirectory(dir);
+    {
+        KFMElectrostaticFastMultipoleBoundaryValueSolver bvs;
+        bvs.SetSolverElectrostaticParameters(fm_params(ip, dp));
+        if (pip && pdp)
+            bvs.SetPreconditionerElectrostaticParameters(fm_params(pip, pdp));
+        bvs.SetSolverType(solver);
+        bvs.SetPreconditionerType(precon);
+        bvs.SetTolerance(tol);
+        bvs.SetMaxIterations((unsigned) max_iter);
+        if (restart > 0)
+            bvs.SetRestart((unsigned) restart);
+        bvs.SetPreconditionerTolerance(precon_tol);
+        bvs.SetMaxPreconditionerIterations((unsigned) precon_max_iter);
+        bvs.SetPreconditionerDegree((unsigned) precon_degree);
+        bvs.Solve(*container);
+        if (resid)
+            *resid = bvs.GetResidualNorm();
+    }
+    kemref_get_sigma(h, x);
+    std::filesystem::remove_all(dir);
     return 0;
 }
 }

@@ -43,6 +43,9 @@ def lib():
         L.kemref_gmres.argtypes = [C.c_void_p, C.c_double, C.c_int, _dp, _dp]
         L.kemref_gmres.restype = C.c_int
         L.kemref_robinhood.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
+        L.kemref_krylov.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_double,
+                                    C.c_int, _dp, _dp]
+        L.kemref_krylov.restype = C.c_int
         L.kemref_robinhood.restype = C.c_int
         L.kemref_rk8_track.argtypes = [C.c_void_p, _dp, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, _dp]
         L.kemref_rk8_track.restype = C.c_int
@@ -154,6 +157,17 @@ class RefProblem:
         x = np.zeros(self.n)
         r = np.zeros(1)
         it = lib().kemref_gmres(self.h, tol, max_iter, _d(x), _d(r))
+        return self._from_c(x), it, float(r[0])
+
+    def krylov(self, solver="gmres", preconditioner="none", tol=1e-8, max_iter=500, restart=0,
+               preconditioner_tol=0.01, max_preconditioner_iter=30):
+        """The reference's Krylov solver factory on the direct system (KBuildKrylovSolver):
+        (x, iterations, residual norm over |b|)."""
+        x = np.zeros(self.n)
+        r = np.zeros(1)
+        pc = {"none": 0, "jacobi": 1, "implicit_krylov": 2}[preconditioner]
+        it = lib().kemref_krylov(self.h, int(solver == "bicgstab"), pc, tol, max_iter, restart, preconditioner_tol,
+                                 max_preconditioner_iter, _d(x), _d(r))
         return self._from_c(x), it, float(r[0])
 
     def robinhood(self, tol=1e-8):

@@ -41,6 +41,9 @@ def lib():
         L.kemref_fm_response.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp]
         L.kemref_fm_field.argtypes = [C.c_void_p, _ip, _dp, C.c_int, _dp, _dp, _dp]
         L.kemref_fm_matvec.argtypes = [C.c_void_p, _ip, _dp, _dp, _dp]
+        L.kemref_get_sigma.argtypes = [C.c_void_p, _dp]
+        L.kemref_fm_bvs.argtypes = [C.c_void_p, _ip, _dp, C.c_char_p, C.c_char_p, C.c_double, C.c_int, C.c_int,
+                                    C.c_double, C.c_int, C.c_int, _ip, _dp, _dp, _dp]
         _lib = L
     return _lib
 
@@ -140,3 +143,24 @@ class FmRefProblem:
         world = np.zeros(4)
         lib().kemref_fm_field(self.h, ipar.ctypes.data_as(_ip), _d(dpar), P.shape[0], _d(P), _d(out), _d(world))
         return out, world
+
+    def solve(self, solver="gmres", preconditioner="none", tol=1e-6, max_iter=500, restart=0, preconditioner_tol=0.01,
+              max_preconditioner_iter=30, preconditioner_degree=1, preconditioner_params=None, **tree):
+        """The reference's fast-multipole charge-density solve (KFMElectrostaticFastMultipoleBoundaryValueSolver,
+        the solver of krylov_bem_solver): (x in caller order, residual norm over |b|). tree: the
+        solver tree's parameters as matvec; preconditioner_params: those of the independent
+        preconditioner tree (independent_implicit_krylov)."""
+        def params(degree=8, top_level_divisions=2, divisions=2, zeromask=1, maximum_tree_depth=3,
+                   insertion_ratio=4.0 / 3.0, region_expansion_factor=1.1):
+            return (np.ascontiguousarray([degree, top_level_divisions, divisions, zeromask, maximum_tree_depth],
+                                         np.int32), _c([insertion_ratio, region_expansion_factor]))
+        ipar, dpar = params(**tree)
+        pip, pdp = params(**(preconditioner_params or tree))
+        x = np.zeros(self.n)
+        r = np.zeros(1)
+        rc = lib().kemref_fm_bvs(self.h, ipar.ctypes.data_as(_ip), _d(dpar), solver.encode(), preconditioner.encode(),
+                                 tol, max_iter, restart, preconditioner_tol, max_preconditioner_iter,
+                                 preconditioner_degree, pip.ctypes.data_as(_ip), _d(pdp), _d(x), _d(r))
+        if rc != 0:
+            raise RuntimeError(f"kemref_fm_bvs failed ({rc})")
+        return np.ascontiguousarray(x[self.cidx]), float(r[0])

@@ -32,6 +32,10 @@
 #include "KElectrostaticQuadratureLineSegmentIntegrator.hh"
 #include "KElectrostaticIntegratingFieldSolver.hh"
 #include "KGeneralizedMinimalResidual.hh"
+#include "KImplicitKrylovPreconditioner.hh"
+#include "KJacobiPreconditioner.hh"
+#include "KKrylovSolverConfiguration.hh"
+#include "KKrylovSolverFactory.hh"
 #include "KRobinHood.hh"
 #include "KSMathArray.h"
 #include "KSMathRK8.h"
@@ -309,6 +313,47 @@ int kemref_gmres(void* h, double tol, int max_iter, double* x, double* resid)
     if (resid)
         *resid = S.ResidualNorm();
     return (int) S.GetIteration();
+}
+
+// Krylov solve of the direct system through the reference's solver factory (KBuildKrylovSolver,
+// KKrylovSolverFactory.hh:83-155, as KKrylovChargeDensitySolver.cc:43-67 uses it): GMRES or
+// BiCGStab, a restart every `restart` iterations (0 = never), preconditioner 0 none, 1 Jacobi
+// (KJacobiPreconditioner), 2 implicit Krylov (KBuildKrylovPreconditioner: an inner GMRES on the
+// same direct matrix to precon_tol, at most precon_max_iter iterations). x from zero; returns
+// the iteration count, *resid = the solver's residual norm over |b|.
+int kemref_krylov(void* h, int bicgstab, int precon, double tol, int max_iter, int restart, double precon_tol,
+                  int precon_max_iter, double* x, double* resid)
+{
+    auto* ctx = static_cast<RefCtx*>(h);
+    auto A = std::make_shared<KBoundaryIntegralMatrix<KElectrostaticBoundaryIntegrator>>(ctx->container,
+                                                                                         ctx->integrator);
+    KBoundaryIntegralVector<KElectrostaticBoundaryIntegrator> b(ctx->container, ctx->integrator);
+    KBoundaryIntegralSolutionVector<KElectrostaticBoundaryIntegrator> xs(ctx->container, ctx->integrator);
+    for (unsigned i = 0; i < xs.Dimension(); i++)
+        xs[i] = 0.;
+    KKrylovSolverConfiguration cfg;
+    cfg.SetSolverName(bicgstab ? "bicgstab" : "gmres");
+    cfg.SetTolerance(tol);
+    cfg.SetMaxIterations((unsigned) max_iter);
+    if (restart > 0)
+        cfg.SetIterationsBetweenRestart((unsigned) restart);
+    std::shared_ptr<const KSquareMatrix<double>> P;
+    if (precon == 1)
+        P = std::make_shared<KJacobiPreconditioner<double>>(*A);
+    else if (precon == 2) {
+        KKrylovSolverConfiguration pc;
+        pc.SetSolverName("gmres");
+        pc.SetTolerance(precon_tol);
+        pc.SetMaxIterations((unsigned) precon_max_iter);
+        P = KBuildKrylovPreconditioner<double>(pc, A);
+    }
+    auto solver = KBuildKrylovSolver<double>(cfg, A, P);
+    solver->Solve(xs, b);
+    for (unsigned i = 0; i < xs.Dimension(); i++)
+        x[i] = xs(i);
+    if (resid)
+        *resid = solver->ResidualNorm();
+    return (int) solver->GetIteration();
 }
 
 int kemref_robinhood(void* h, double tol, double* x, double* resid)

@@ -6,7 +6,9 @@
 // drives a KElectrostaticBoundaryField with them on a 320-triangle sphere at 1 V; the field is
 // compared with the reference's KIntegratingElectrostaticFieldSolver on the same charge
 // densities (a fourth field solves on the fast multipole operator and evaluates with the CUDA FFTM
-// field solver), and the parsed settings with the XML. Exit status 0 when everything agrees. With the
+// field solver; a fifth and a sixth take krylov_bem_solver's solver and preconditioner choices and
+// its fftm_multiplication / preconditioner_electrostatic_parameters children, built by the
+// reference's KFMElectrostaticParametersBuilder), and the parsed settings with the XML. Exit status 0 when everything agrees. With the
 // argument --parse-only the check stops after the settings (no device needed).
 #include "KComplexElement.hh"
 #include "KElectrostaticBoundaryField.hh"
@@ -131,6 +133,28 @@ static const char* kXML = R"(
         world_cube_center_x="0.001" world_cube_center_y="-0.002" world_cube_center_z="0.0" world_cube_length="6.4"
         insertion_ratio="1.3333333333333333" verbosity="0"/>
 </test_electrostatic_field>
+<test_electrostatic_field>
+    <cuda_krylov_bem_solver solver_name="gmres" preconditioner="implicit_krylov" tolerance="1e-8"
+        preconditioner_tolerance="0.01" max_iterations="500" max_preconditioner_iterations="30"
+        iterations_between_restarts="250" preconditioner_degree="1" intermediate_save_interval="1"
+        use_display="true" show_plot="false" use_timer="true">
+        <fftm_multiplication verbosity="0" strategy="aggressive" top_level_divisions="2" tree_level_divisions="2"
+            expansion_degree="8" neighbor_order="1" maximum_tree_depth="3" use_region_size_estimation="true"
+            region_expansion_factor="1.1" insertion_ratio="1.3333333333333333"/>
+    </cuda_krylov_bem_solver>
+    <cuda_field_solver precision="fp64"/>
+</test_electrostatic_field>
+<test_electrostatic_field>
+    <cuda_krylov_charge_density_solver solver_name="bicgstab" preconditioner="independent_implicit_krylov"
+        tolerance="1e-8" preconditioner_tolerance="0.05" max_preconditioner_iterations="20">
+        <fftm_multiplication top_level_divisions="2" tree_level_divisions="2" expansion_degree="8" neighbor_order="1"
+            maximum_tree_depth="3" use_region_size_estimation="true" region_expansion_factor="1.1"/>
+        <preconditioner_electrostatic_parameters top_level_divisions="2" tree_level_divisions="2"
+            expansion_degree="2" neighbor_order="1" maximum_tree_depth="2" use_region_size_estimation="true"
+            region_expansion_factor="1.1"/>
+    </cuda_krylov_charge_density_solver>
+    <cuda_field_solver precision="fp64"/>
+</test_electrostatic_field>
 )";
 
 // the boundary field with the parsed solvers, against the reference CPU field solver
@@ -182,7 +206,7 @@ int main(int argc, char** argv)
         file.AddToNames(xml);
         tokenizer.ProcessFile(&file);
         std::printf("parsed %zu field elements\n", gFields.size());
-        if (gFields.size() != 4)
+        if (gFields.size() != 6)
             return 1;
         // settings as written in the XML
         auto* k0 = dynamic_cast<KCUDAChargeDensitySolver*>(gFields[0].cds.get());
@@ -206,6 +230,19 @@ int main(int argc, char** argv)
                               !f3->GetParameters()->use_region_estimation &&
                               f3->GetParameters()->world_length == 6.4 &&
                               f3->GetParameters()->world_center_y == -0.002;
+        auto* k4 = dynamic_cast<KCUDAChargeDensitySolver*>(gFields[4].cds.get());
+        auto* k5 = dynamic_cast<KCUDAChargeDensitySolver*>(gFields[5].cds.get());
+        const bool krylov = k4 && k5 && k4->GetMode() == KEMCU_SOLVE_FFTM && k4->GetSolver() == KEMCU_KRYLOV_GMRES &&
+                            k4->GetPreconditioner() == KEMCU_PRECON_IMPLICIT_KRYLOV && !k4->IndependentPreconditioner() &&
+                            k4->GetIterationsBetweenRestart() == 250 && k4->GetPreconditionerTolerance() == 0.01 &&
+                            k4->GetMaxPreconditionerIterations() == 30 && k4->GetPreconditionerDegree() == 1 &&
+                            k4->GetMaxIterations() == 500 && k4->GetFastMultipoleParameters().degree == 8 &&
+                            k5->GetMode() == KEMCU_SOLVE_FFTM && k5->GetSolver() == KEMCU_KRYLOV_BICGSTAB &&
+                            k5->IndependentPreconditioner() && k5->GetMaxPreconditionerIterations() == 20 &&
+                            k5->GetPreconditionerFastMultipoleParameters().degree == 2 &&
+                            k5->GetPreconditionerFastMultipoleParameters().maximum_tree_depth == 2;
+        std::printf("Krylov solver and preconditioner settings from the XML: %s\n", krylov ? "as written" : "WRONG");
+        fail += !krylov;
         std::printf("settings from the XML: %s\n", settings ? "as written" : "WRONG");
         fail += !settings;
         if (settings && !parse_only) {
@@ -220,6 +257,15 @@ int main(int argc, char** argv)
             // comparison solver sees the same densities, so only the field arithmetic differs; the
             // FFTM field differs by its truncation error (degree 10, neighbour order 2)
             fail += !(d0 < 1e-9 && d1 < 1e-12 && d2 < 1e-14 && d3 < 1e-5);
+            if (krylov) {
+                // fast multipole solves (degree 8) with the preconditioned solvers, the field of their
+                // densities by the direct sum: the densities carry the operator's truncation error
+                const double d4 = field_difference(gFields[4], gScratch + "/4");
+                const double d5 = field_difference(gFields[5], gScratch + "/5");
+                std::printf("field vs the reference CPU solver: FFTM GMRES + implicit Krylov (degree 1) %.3e, "
+                            "FFTM BiCGStab + independent implicit Krylov %.3e\n", d4, d5);
+                fail += !(d4 < 1e-5 && d5 < 1e-5);
+            }
         }
     }
     catch (std::exception& e) {

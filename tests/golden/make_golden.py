@@ -57,6 +57,17 @@ Fixtures:
                  (KFastMultipoleMatrixGenerator, degree 8, depth 3) times the coax_small density
                  and times a seeded vector on mixed_small (Neumann rows and wires), with the world
                  cubes of those trees
+  krylov         the reference's Krylov solvers on the coax_small system: the solver factory
+                 (KBuildKrylovSolver, the path of KKrylovChargeDensitySolver) with gmres and
+                 bicgstab, preconditioners none, jacobi and implicit_krylov (inner gmres on the
+                 same matrix to 0.1, at most 10 iterations), no restart and a restart every 7
+                 iterations, tolerance 1e-9: solution, iterations, residual norm, and the true
+                 residual of the solution; and the fast-multipole boundary-value solver
+                 (KFMElectrostaticFastMultipoleBoundaryValueSolver, the solver of krylov_bem_solver;
+                 degree 8, depth 3) with every solver / preconditioner pair but gmres / none
+                 (which does not initialise its tree and crashes), tolerance 1e-6, inner
+                 tolerance 0.01 and 30 iterations, preconditioner degree 1 (implicit_krylov) or
+                 the degree-2, depth-2 tree (independent_implicit_krylov): solution and residual
 
 Usage: python tests/golden/make_golden.py [fixture ...]   (default: all)
 """
@@ -520,6 +531,35 @@ def fftm():
          coax_Ax_d3=coax_Ax, mixed_Ax_d3=mixed_Ax, mixed_world_d3=mixed_world)
 
 
+def krylov():
+    from oracle import ref_fm
+
+    cx = golden_mesh("coax_small")
+    p = ref.RefProblem(cx)
+    A, b = p.matrix(), p.rhs()
+    out = {"direct_sigma": np.linalg.solve(A, b)}
+    for solver in ("gmres", "bicgstab"):
+        for pc in ("none", "jacobi", "implicit_krylov"):
+            for restart in (0, 7):
+                x, it, r = p.krylov(solver, pc, tol=1e-9, max_iter=300, restart=restart, preconditioner_tol=0.1,
+                                    max_preconditioner_iter=10)
+                key = f"{solver}_{pc}_r{restart}"
+                out[key + "_sigma"] = x
+                out[key + "_iterations"] = np.array(it)
+                out[key + "_residual"] = np.array(r)
+                out[key + "_true_residual"] = np.array(np.linalg.norm(b - A @ x) / np.linalg.norm(b))
+    fr = ref_fm.FmRefProblem(cx)
+    for solver, pc in (("gmres", "jacobi"), ("gmres", "implicit_krylov"), ("gmres", "independent_implicit_krylov"),
+                       ("bicgstab", "none"), ("bicgstab", "jacobi"), ("bicgstab", "implicit_krylov"),
+                       ("bicgstab", "independent_implicit_krylov")):
+        x, r = fr.solve(solver, pc, tol=1e-6, max_iter=200, preconditioner_tol=0.01, max_preconditioner_iter=30,
+                        preconditioner_degree=1, preconditioner_params=dict(degree=2, maximum_tree_depth=2), degree=8,
+                        maximum_tree_depth=3)
+        out[f"fftm_{solver}_{pc}_sigma"] = x
+        out[f"fftm_{solver}_{pc}_residual"] = np.array(r)
+    save("krylov", **out)
+
+
 def golden_mesh(name):
     from oracle.golden import mesh_from
 
@@ -527,7 +567,8 @@ def golden_mesh(name):
 
 
 FIXTURES = {f.__name__: f for f in (rules, integrators, lines, icosphere, mixed_small, coax_small, rk8, adjoint,
-                                     robinhood, axisym, c1_sphere, c2_coax, c3_tracks, c4_adjoint, c5_rings, fftm)}
+                                     robinhood, axisym, c1_sphere, c2_coax, c3_tracks, c4_adjoint, c5_rings, fftm,
+                                     krylov)}
 
 if __name__ == "__main__":
     for name in sys.argv[1:] or list(FIXTURES):

@@ -102,4 +102,5 @@ def test_xml_bindings_parse_without_a_device():
         pytest.skip("bindings check not built (needs the reference tree)")
     r = subprocess.run([binary, "--parse-only"], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert "parsed 4 field elements" in r.stdout and "settings from the XML: as written" in r.stdout
+    assert "parsed 6 field elements" in r.stdout and "settings from the XML: as written" in r.stdout
+    assert "Krylov solver and preconditioner settings from the XML: as written" in r.stdout
