@@ -417,6 +417,17 @@ def run_native(args, rank, world, dist):
             "fftm_matvec_ms": None}
         ctx.FFTMMultiply(xf)
         fm["gmres_fftm_degree8_depth5"]["fftm_matvec_ms"] = ctx.last_kernel_ms
+        # the solver of the reference's krylov_bem_solver in its example configurations (gmres,
+        # implicit_krylov on the degree-1 tree, inner tolerance 0.01 and 30 iterations, restarts
+        # every 250) and BiCGStab, on the same operator
+        ctx.ConfigureFFTMPreconditioner(degree=1, maximum_tree_depth=5)
+        for tag, kw in (("gmres_implicit_krylov_degree1", dict(preconditioner="implicit_krylov", restart=250,
+                                                                preconditioner_tol=0.01, max_preconditioner_iter=30)),
+                        ("bicgstab", dict(solver="bicgstab"))):
+            _, sk = ctx.KrylovSolve(mode=K.SOLVE_FFTM, tol=TOL, max_iter=300, raise_on_failure=False, **kw)
+            fm[tag] = {"seconds": sk["seconds"], "iterations": sk["iterations"],
+                       "operator_products": sk["fp64_matvecs"], "preconditioner_products": sk["low_matvecs"],
+                       "fftm_rel_residual": sk["rel_residual"], "converged": sk["status"] == 0}
         ctx.SetSigma(x_asm)
         extra["fftm_coax44k"] = fm
         # configuration 5: 100,000 jittered triangles on 8 stacked rings, 8 right-hand sides:
@@ -452,6 +463,13 @@ def run_native(args, rank, world, dist):
                 "fftm_rel_residual": sfm["rel_residual"], "converged": sfm["status"] == 0,
                 "true_rel_residual_direct_operator": float(max(np.linalg.norm(R[i]) / np.linalg.norm(B[i])
                                                                for i in range(len(B))))}
+            # the same solve with the Jacobi preconditioner (KJacobiPreconditioner, right-preconditioned GMRES)
+            Xj, sj = fc.KrylovSolve(B, mode=K.SOLVE_FFTM, tol=TOL, max_iter=400, preconditioner="jacobi",
+                                    raise_on_failure=False)
+            extra["c5_stacked_rings_100k_8rhs"]["fftm_degree8_depth6_jacobi"] = {
+                "solve_s": sj["seconds"], "krylov_iterations": sj["iterations"],
+                "fftm_rel_residual": sj["rel_residual"], "converged": sj["status"] == 0,
+                "speedup_over_unpreconditioned": sfm["seconds"] / sj["seconds"]}
 
     res = dict(
         ms_mixed=ms_mixed, ms_fp64=ms_fp64, ms_fp32=ms_fp32, err_fp32=err_fp32, wall_mixed=wall_mixed, e2e_s=e2e_s, launches=int(launches),
