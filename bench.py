@@ -390,7 +390,7 @@ def run_native(args, rank, world, dist):
         # sum, and GMRES on the FFTM operator
         fm = {}
         ctx.SetSigma(x_asm)  # the capped Robin Hood runs above leave their iterate on the context
-        for deg, depth in ((8, 5), (10, 5)):
+        for deg, depth in ((8, 6), (8, 5), (10, 6)):
             t0 = time.perf_counter()
             ctx.ConfigureFFTM(degree=deg, maximum_tree_depth=depth)
             build_s = time.perf_counter() - t0
