@@ -9,6 +9,11 @@
 //          reference GMRES's least-squares step by SVD leaves its iterate well above its residual
 //          estimate, so the two reference-GMRES residuals are compared with each other, the
 //          device GMRES with the tolerance);
+//   krylov the reference's krylov_bem_solver (KKrylovChargeDensitySolverOld with
+//          KFMElectrostaticFastMultipoleBoundaryValueSolver) with gmres + implicit_krylov (degree-1
+//          preconditioner tree, inner tolerance 0.01, 30 iterations, restarts every 250) and with
+//          bicgstab + jacobi, against KCUDAChargeDensitySolver with the same settings, each to 1e-8:
+//          residuals under the reference's FFTM matrix and the densities;
 //   field  the reference's KElectricFastMultipoleFieldSolver and KCUDAFastMultipoleFieldSolver
 //          (both KElectricFieldSolvers) on those densities, at points inside the world cube.
 // Exit status 0 when every comparison is within tolerance.
@@ -17,6 +22,8 @@
 #include "KElectrostaticBoundaryField.hh"
 #include "KFastMultipoleMatrixGenerator.hh"
 #include "KKrylovChargeDensitySolver.hh"
+#include "KKrylovChargeDensitySolverOld.hh"
+#include "KFMElectrostaticFastMultipoleBoundaryValueSolverConfiguration.hh"
 #include "KSimpleVector.hh"
 #include "KSurface.hh"
 #include "KSurfaceContainer.hh"
@@ -171,6 +178,67 @@ int main()
             dev.Solve(gpu);
             s_dev = densities(*container);
         }
+        // krylov_bem_solver: the reference's boundary-value solver and the device with its settings
+        const char* kry[2][2] = {{"gmres", "implicit_krylov"}, {"bicgstab", "jacobi"}};
+        std::vector<double> s_old[2], s_devk[2];
+        for (int c = 0; c < 2; c++) {
+            {
+                auto container = sphere();
+                const std::string sub = dir + "/old" + std::to_string(c);
+                std::filesystem::create_directories(sub);
+                KEMFileInterface::GetInstance()->ActiveDirectory(sub);
+                KKrylovChargeDensitySolverOld old;
+                auto* cfg = old.GetSolverConfig();
+                cfg->SetSolverName(kry[c][0]);
+                cfg->SetPreconditionerName(kry[c][1]);
+                cfg->SetSolverTolerance(1e-8);
+                cfg->SetMaxSolverIterations(200);
+                cfg->SetIterationsBetweenRestart(250);
+                cfg->SetPreconditionerTolerance(0.01);
+                cfg->SetMaxPreconditionerIterations(30);
+                cfg->SetPreconditionerDegree(1);
+                auto* prm = new KFMElectrostaticParameters();
+                prm->strategy = KFMSubdivisionStrategy::Aggressive;
+                prm->degree = 8;
+                prm->top_level_divisions = 2;
+                prm->divisions = 2;
+                prm->zeromask = 1;
+                prm->maximum_tree_depth = 3;
+                prm->insertion_ratio = 4. / 3.;
+                prm->use_region_estimation = false;
+                prm->world_center_x = wc[0];
+                prm->world_center_y = wc[1];
+                prm->world_center_z = wc[2];
+                prm->world_length = wl;
+                prm->use_caching = false;
+                prm->verbosity = 0;
+                cfg->SetFFTMParams(prm);  // owned by the configuration
+                old.Initialize(*container);
+                s_old[c] = densities(*container);
+            }
+            {
+                auto container = sphere();
+                KCUDASurfaceContainer gpu(*container);
+                KCUDAChargeDensitySolver dev(1e-8, 200, KEMCU_SOLVE_FFTM);
+                kemcu_fftm_params q;
+                kemcu_fftm_default_params(&q);
+                q.degree = 8;
+                q.maximum_tree_depth = 3;
+                q.world_center[0] = wc[0];
+                q.world_center[1] = wc[1];
+                q.world_center[2] = wc[2];
+                q.world_length = wl;
+                dev.SetFastMultipoleParameters(q);
+                dev.SetSolverName(kry[c][0]);
+                dev.SetPreconditionerName(kry[c][1]);
+                dev.SetIterationsBetweenRestart(250);
+                dev.SetPreconditionerTolerance(0.01);
+                dev.SetMaxPreconditionerIterations(30);
+                dev.SetPreconditionerDegree(1);
+                dev.Solve(gpu);
+                s_devk[c] = densities(*container);
+            }
+        }
         // the reference's FFTM matrix and the CUDA one on the same vector, and the residuals of the
         // three solutions under the reference's matrix
         {
@@ -214,6 +282,15 @@ int main()
                         r_ref, r_cuda, r_dev);
             fail += !(d_mat < 1e-11);
             fail += !(r_cuda <= 10. * r_ref + 1e-9 && r_dev <= 1e-9);
+            for (int c = 0; c < 2; c++) {
+                const double ro = residual(s_old[c]), rd = residual(s_devk[c]), ds = max_rel(s_devk[c], s_old[c]);
+                std::printf("krylov_bem_solver %s + %s: relative residual under the reference's FFTM matrix, reference "
+                            "%.3e, device %.3e; densities max difference / max value %.3e\n",
+                            kry[c][0], kry[c][1], ro, rd, ds);
+                // both solve the same system to 1e-8 (condition number ~30): the densities agree to
+                // a few 1e-7 at most
+                fail += !(ro <= 1e-8 && rd <= 1e-8 && ds <= 1e-6);
+            }
         }
 
         // field: the reference FFTM field solver and the CUDA one, each a KElectricFieldSolver

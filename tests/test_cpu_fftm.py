@@ -77,3 +77,23 @@ def test_fftm_parameters_rejected_on_cpu_paths():
     K._native.lib().kemcu_fftm_default_params(K._native.C.byref(prm))
     assert (prm.degree, prm.top_level_divisions, prm.divisions, prm.zeromask) == (8, 2, 2, 1)
     assert abs(prm.insertion_ratio - 4.0 / 3.0) < 1e-15 and prm.near_analytic == 1
+
+
+def test_krylov_defaults_and_host_side_errors():
+    # kemcu_krylov_default_params and the argument checks before any device work (no GPU): the
+    # documented defaults (gmres on the FP64 matrix-free operator, 1e-8, 500 iterations, no restart,
+    # no preconditioner; implicit Krylov on the preconditioner's tree to 0.01 in 30 iterations),
+    # and a null context refused with KEMCU_EINVAL
+    from kassiopeia_b200 import _native as N
+    L = N.lib()
+    p = N.KrylovParams()
+    L.kemcu_krylov_default_params(p)
+    assert (p.solver, p.mode, p.tolerance, p.max_iterations, p.iterations_between_restarts) == \
+        (N.KRYLOV_GMRES, K.SOLVE_PLAIN, 1e-8, 500, 0)
+    assert (p.preconditioner, p.preconditioner_mode, p.preconditioner_tolerance, p.max_preconditioner_iterations) == \
+        (N.PRECON_NONE, K.SOLVE_FFTM, 0.01, 30)
+    x = np.zeros(4)
+    assert L.kemcu_krylov_solve(None, None, x.ctypes.data_as(N._dp), 1, p, None) == N.EINVAL
+    fp = N.FftmParams()
+    L.kemcu_fftm_default_params(fp)
+    assert L.kemcu_fftm_configure_preconditioner(None, fp) == N.EINVAL
