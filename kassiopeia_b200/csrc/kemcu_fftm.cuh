@@ -243,10 +243,11 @@ __global__ void fm_l2l_kernel(const int* __restrict__ children, int nchildren, F
 // interaction list (children of its parent's neighbours that are not its own neighbours, the
 // neighbours being the cells within zm cells in every direction), in a fixed order. op_index
 // maps an offset (source - target, cell units, |o_i| <= R) to its operator, or -1.
+template<int NR>
 __global__ void fm_m2l_kernel(const int* __restrict__ targets, int ntargets, FmLevel L, int zm, int R,
                               const int* __restrict__ op_index, const unsigned char* __restrict__ occ,
                               const double* __restrict__ ops, int K, const double* __restrict__ M,
-                              double* __restrict__ Lx)
+                              double* __restrict__ Lx, int nrhs, size_t mstride, size_t lstride)
 {
     extern __shared__ double fm_x[];
     const int b = blockIdx.x;
@@ -269,7 +270,10 @@ __global__ void fm_m2l_kernel(const int* __restrict__ targets, int ntargets, FmL
         }
     }
     const int row = threadIdx.x;
-    double acc = 0.;
+    double acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+        acc[r] = 0.;
     const int W = 2 * R + 1;
     for (int sx = lo[0]; sx < hi[0]; sx++)
         for (int sy = lo[1]; sy < hi[1]; sy++)
@@ -282,17 +286,36 @@ __global__ void fm_m2l_kernel(const int* __restrict__ targets, int ntargets, FmL
                     continue;
                 const int oi = op_index[((ox + R) * W + (oy + R)) * W + (oz + R)];
                 __syncthreads();
-                for (int i = threadIdx.x; i < K; i += blockDim.x)
-                    fm_x[i] = M[si * K + i];
+                for (int r = 0; r < (NR == 1 ? 1 : nrhs); r++)
+                    for (int i = threadIdx.x; i < K; i += blockDim.x)
+                        fm_x[r * K + i] = M[r * mstride + si * K + i];
                 __syncthreads();
                 if (row < K && oi >= 0) {
                     const double* op = ops + (size_t) oi * K * K;
-                    for (int k = 0; k < K; k++)
-                        acc = fma(op[(size_t) k * K + row], fm_x[k], acc);
+                    if (NR == 1 || nrhs == NR) {
+                        for (int k = 0; k < K; k++) {
+                            const double o = op[(size_t) k * K + row];
+#pragma unroll
+                            for (int r = 0; r < NR; r++)
+                                acc[r] = fma(o, fm_x[r * K + k], acc[r]);
+                        }
+                    }
+                    else {
+                        for (int k = 0; k < K; k++) {
+                            const double o = op[(size_t) k * K + row];
+#pragma unroll
+                            for (int r = 0; r < NR; r++)
+                                if (r < nrhs)
+                                    acc[r] = fma(o, fm_x[r * K + k], acc[r]);
+                        }
+                    }
                 }
             }
     if (row < K)
-        Lx[(L.base + tc) * K + row] += acc;
+#pragma unroll
+        for (int r = 0; r < NR; r++)
+            if (NR == 1 || r < nrhs)
+                Lx[r * lstride + (L.base + tc) * K + row] += acc[r];
 }
 
 // ------------------------------------------------------------------------- L2P
@@ -531,6 +554,98 @@ __global__ void __launch_bounds__(128, kFmMatvecMinBlocks) fm_matvec_kernel(cons
                     }
         }
         const double ux = (C.x - cx) * inv_side, uy = (C.y - cy) * inv_side, uz = (C.z - cz) * inv_side;
+#pragma unroll
+        for (int r = 0; r < NR; r++)
+            if (r < nrhs) {
+                double far[4];
+                fm_l2p(fm_x + r * K, p, ux, uy, uz, inv_side, far);
+                const double fv =
+                    t.neumann == 0. ? far[3] : far[0] * t.normal[0] + far[1] * t.normal[1] + far[2] * t.normal[2];
+                y[(size_t) r * n + ti] = s[r] + fv;
+            }
+    }
+}
+
+// The near part of the matrix kept as a sparse matrix (fm_build_near): per run of targets (one
+// leaf) its direct elements, col[coloff[b] .. + ncol[b]], in fm_matvec_kernel's order, and the
+// entries of the run's cnt targets column-major at val[valoff[b] + j cnt + k].
+struct FmNear
+{
+    const long long* coloff;
+    const int* ncol;
+    const long long* valoff;
+    const int* col;
+    double* val;
+};
+
+// the entries entry() of every run's targets with its direct elements; one CTA per run, its
+// threads over the (element, target) pairs of the run
+__global__ void __launch_bounds__(256) fm_near_fill_kernel(const double* __restrict__ rec,
+                                                           const TargetRec* __restrict__ tgt,
+                                                           const int* __restrict__ tgt_order,
+                                                           const int* __restrict__ run_off,
+                                                           const int* __restrict__ run_cnt,
+                                                           const long long* __restrict__ coloff,
+                                                           const int* __restrict__ ncol,
+                                                           const long long* __restrict__ valoff,
+                                                           const int* __restrict__ col, double* __restrict__ val)
+{
+    const int b = blockIdx.x;
+    const int off = run_off[b], cnt = run_cnt[b], nc = ncol[b];
+    const int* cb = col + coloff[b];
+    double* vb = val + valoff[b];
+    const long long pairs = (long long) nc * cnt;
+    for (long long q = threadIdx.x; q < pairs; q += blockDim.x) {
+        const int j = (int) (q / cnt), k = (int) (q % cnt);
+        const TargetRec t = tgt[tgt_order[off + k]];
+        vb[q] = entry<false>(rec + (size_t) cb[j] * rRecSize, t, v3(t.cen[0], t.cen[1], t.cen[2]));
+    }
+}
+
+// fm_matvec_kernel with the near part read from the sparse matrix: the same sums in the same
+// order (compensated, over the run's columns), plus the local expansion of the leaf
+template<int NR>
+__global__ void __launch_bounds__(128, kFmMatvecMinBlocks) fm_matvec_near_kernel(
+    const TargetRec* __restrict__ tgt, const int* __restrict__ tgt_order, const int* __restrict__ run_key,
+    const int* __restrict__ run_off, const int* __restrict__ run_cnt, FmNear nr, FmTreeView T, int p,
+    const double* __restrict__ Lx, size_t lstride, int n, int nrhs, const double* __restrict__ x,
+    double* __restrict__ y)
+{
+    extern __shared__ double fm_x[];
+    const int b = blockIdx.x;
+    const int key = run_key[b] - 1;
+    const int off = run_off[b], cnt = run_cnt[b], nc = nr.ncol[b];
+    const int* cb = nr.col + nr.coloff[b];
+    const double* vb = nr.val + nr.valoff[b];
+    const int K = (p + 1) * (p + 1);
+    const FmLevel& Ld = T.lv[T.depth];
+    for (int r = 0; r < nrhs; r++)
+        for (int i = threadIdx.x; i < K; i += blockDim.x)
+            fm_x[r * K + i] = Lx[r * lstride + (Ld.base + key) * K + i];
+    __syncthreads();
+    const int lz = key % Ld.n, ly = (key / Ld.n) % Ld.n, lx = key / (Ld.n * Ld.n);
+    const double cx = T.wx + (lx + .5) * Ld.side, cy = T.wy + (ly + .5) * Ld.side, cz = T.wz + (lz + .5) * Ld.side;
+    const double inv_side = 1. / Ld.side;
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+        const int ti = tgt_order[off + k];
+        const TargetRec t = tgt[ti];
+        double s[NR], c[NR];
+#pragma unroll
+        for (int r = 0; r < NR; r++)
+            s[r] = c[r] = 0.;
+        for (int j = 0; j < nc; j++) {
+            const int e = cb[j];
+            const double a = vb[(size_t) j * cnt + k];
+#pragma unroll
+            for (int r = 0; r < NR; r++)
+                if (r < nrhs) {
+                    const double yk = a * x[(size_t) r * n + e] - c[r];
+                    const double tt = s[r] + yk;
+                    c[r] = (tt - s[r]) - yk;
+                    s[r] = tt;
+                }
+        }
+        const double ux = (t.cen[0] - cx) * inv_side, uy = (t.cen[1] - cy) * inv_side, uz = (t.cen[2] - cz) * inv_side;
 #pragma unroll
         for (int r = 0; r < NR; r++)
             if (r < nrhs) {
