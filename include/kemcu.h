@@ -316,7 +316,10 @@ int kemcu_fftm_field_dev(kemcu_ctx* ctx, const double* dP, size_t n, double* dou
 /* y = A x with the fast multipole operator (KFastMultipoleMatrixGenerator, KFastMultipoleMatrixGenerator.cc:
    23-41): the local expansion of the leaf holding each row's collocation point (potential, or
    field along the normal for a Neumann row) plus the direct entries, by the numeric policy as
-   kemcu_matvec, of the elements owned by the neighbours of that leaf's ancestors; x, y n_rhs x n */
+   kemcu_matvec, of the elements owned by the neighbours of that leaf's ancestors; x, y n_rhs x n.
+   The first product of a tree computes the near part's entries and keeps them on the device (as
+   the reference keeps the sparse part of its matrix) when they fit a quarter of the free device
+   memory and at most 8 GB; otherwise every product computes them. */
 int kemcu_fftm_matvec(kemcu_ctx* ctx, const double* x, double* y, int n_rhs);
 /* tree summary: world4 = world cube centre and side; counts = {cells with moments, elements
    owned per level 0..maximum_tree_depth} (counts has room for 2 + maximum_tree_depth ints) */
