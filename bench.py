@@ -544,6 +544,31 @@ def profile_fftm():
               flush=True)
 
 
+def profile_fftm_matvec():
+    """profiling case for ncu: the fast multipole operator's products, three on the coax (degree 8,
+    depth 5; the first one also keeps the near part) and two for configuration 5's 8 right-hand
+    sides (degree 8, depth 6)"""
+    import kassiopeia_b200 as K
+    from kassiopeia_b200 import geometry as G
+
+    ctx = K.CUDAElectrostaticContext(int(os.environ.get("LOCAL_RANK", 0)), autotune=False)
+    mesh = G.coax()
+    ctx.SetGeometry(mesh)
+    ctx.ConfigureFFTM(degree=8, maximum_tree_depth=5)
+    x = G.coax_density(mesh)
+    for _ in range(3):
+        ctx.FFTMMultiply(x)
+        print(json.dumps({"fftm_product": "coax, degree 8, depth 5", "ms": ctx.last_kernel_ms}), flush=True)
+    rings = G.stacked_rings()
+    ctx.SetGeometry(rings)
+    ctx.ConfigureFFTM(degree=8, maximum_tree_depth=6)
+    B = G.ring_potentials(rings, n_rhs=8) * 1e-12
+    for _ in range(2):
+        ctx.FFTMMultiply(B)
+        print(json.dumps({"fftm_product": "configuration 5, 8 right-hand sides, degree 8, depth 6",
+                          "ms": ctx.last_kernel_ms}), flush=True)
+
+
 def profile_axisym():
     import kassiopeia_b200 as K
     from kassiopeia_b200 import geometry as G
@@ -631,6 +656,9 @@ def main():
                          "potential at 10,000 gap points, two launches; prints points/s")
     ap.add_argument("--profile-fftm", action="store_true",
                     help="profiling case for ncu: fast multipole field of the coax at 1,000,000 points, two launches")
+    ap.add_argument("--profile-fftm-matvec", action="store_true",
+                    help="profiling case for ncu: fast multipole operator products (coax; configuration 5 with 8 "
+                         "right-hand sides)")
     ap.add_argument("--tracking-c3", action="store_true",
                     help="configuration 3 as configured: 65,536 electrons to the end of every track (hit or "
                          "10,000 steps) in launches of --c3-chunk steps; prints one JSON line (several minutes)")
@@ -646,6 +674,9 @@ def main():
         return
     if args.profile_fftm:
         profile_fftm()
+        return
+    if args.profile_fftm_matvec:
+        profile_fftm_matvec()
         return
     if args.profile_operator:
         profile_operator()

@@ -181,9 +181,10 @@ __device__ __forceinline__ long long fm_cell(const FmLevel& L, int x, int y, int
     return L.base + ((long long) x * L.n + y) * L.n + z;
 }
 
+template<int NR>
 __global__ void fm_m2m_kernel(const int* __restrict__ parents, int nparents, FmLevel Lp, FmLevel Lc,
                               const unsigned char* __restrict__ occ, const double* __restrict__ ops, int K,
-                              double* __restrict__ M)
+                              double* __restrict__ M, int nrhs, size_t mstride)
 {
     extern __shared__ double fm_x[];
     const int b = blockIdx.x;
@@ -192,8 +193,12 @@ __global__ void fm_m2m_kernel(const int* __restrict__ parents, int nparents, FmL
     const long long pc = parents[b];
     const int pz = (int) (pc % Lp.n), py = (int) ((pc / Lp.n) % Lp.n), px = (int) (pc / ((long long) Lp.n * Lp.n));
     const int d = Lc.div;
-    double acc = 0.;
+    double acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+        acc[r] = 0.;
     const int row = threadIdx.x;
+    const int nr = NR == 1 ? 1 : nrhs;
     for (int cx = 0; cx < d; cx++)
         for (int cy = 0; cy < d; cy++)
             for (int cz = 0; cz < d; cz++) {
@@ -201,22 +206,43 @@ __global__ void fm_m2m_kernel(const int* __restrict__ parents, int nparents, FmL
                 if (!occ[ci])
                     continue;
                 __syncthreads();
-                for (int i = threadIdx.x; i < K; i += blockDim.x)
-                    fm_x[i] = M[ci * K + i];
+                for (int r = 0; r < nr; r++)
+                    for (int i = threadIdx.x; i < K; i += blockDim.x)
+                        fm_x[r * K + i] = M[r * mstride + ci * K + i];
                 __syncthreads();
                 if (row < K) {
                     const double* op = ops + (size_t) ((cx * d + cy) * d + cz) * K * K;
-                    for (int k = 0; k < K; k++)
-                        acc = fma(op[(size_t) k * K + row], fm_x[k], acc);
+                    if (NR == 1 || nrhs == NR) {
+                        for (int k = 0; k < K; k++) {
+                            const double o = op[(size_t) k * K + row];
+#pragma unroll
+                            for (int r = 0; r < NR; r++)
+                                acc[r] = fma(o, fm_x[r * K + k], acc[r]);
+                        }
+                    }
+                    else {
+                        for (int k = 0; k < K; k++) {
+                            const double o = op[(size_t) k * K + row];
+#pragma unroll
+                            for (int r = 0; r < NR; r++)
+                                if (r < nrhs)
+                                    acc[r] = fma(o, fm_x[r * K + k], acc[r]);
+                        }
+                    }
                 }
             }
     if (row < K)
-        M[(Lp.base + pc) * K + row] += acc;
+#pragma unroll
+        for (int r = 0; r < NR; r++)
+            if (NR == 1 || r < nrhs)
+                M[r * mstride + (Lp.base + pc) * K + row] += acc[r];
 }
 
 // L2L: every flagged child of level Lc receives its parent's local expansion
+template<int NR>
 __global__ void fm_l2l_kernel(const int* __restrict__ children, int nchildren, FmLevel Lp, FmLevel Lc,
-                              const double* __restrict__ ops, int K, double* __restrict__ Lx)
+                              const double* __restrict__ ops, int K, double* __restrict__ Lx, int nrhs,
+                              size_t lstride)
 {
     extern __shared__ double fm_x[];
     const int b = blockIdx.x;
@@ -226,17 +252,30 @@ __global__ void fm_l2l_kernel(const int* __restrict__ children, int nchildren, F
     const int cz = (int) (cc % Lc.n), cy = (int) ((cc / Lc.n) % Lc.n), cx = (int) (cc / ((long long) Lc.n * Lc.n));
     const int d = Lc.div;
     const long long pi = fm_cell(Lp, cx / d, cy / d, cz / d);
-    for (int i = threadIdx.x; i < K; i += blockDim.x)
-        fm_x[i] = Lx[pi * K + i];
+    const int nr = NR == 1 ? 1 : nrhs;
+    for (int r = 0; r < nr; r++)
+        for (int i = threadIdx.x; i < K; i += blockDim.x)
+            fm_x[r * K + i] = Lx[r * lstride + pi * K + i];
     __syncthreads();
     const int row = threadIdx.x;
     if (row >= K)
         return;
     const double* op = ops + (size_t) (((cx % d) * d + (cy % d)) * d + (cz % d)) * K * K;
-    double acc = 0.;
-    for (int k = 0; k < K; k++)
-        acc = fma(op[(size_t) k * K + row], fm_x[k], acc);
-    Lx[(Lc.base + cc) * K + row] += acc;
+    double acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+        acc[r] = 0.;
+    for (int k = 0; k < K; k++) {
+        const double o = op[(size_t) k * K + row];
+#pragma unroll
+        for (int r = 0; r < NR; r++)
+            if (NR == 1 || r < nrhs)
+                acc[r] = fma(o, fm_x[r * K + k], acc[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+        if (NR == 1 || r < nrhs)
+            Lx[r * lstride + (Lc.base + cc) * K + row] += acc[r];
 }
 
 // M2L at one level: every flagged target cell receives the moments of the occupied cells of its
