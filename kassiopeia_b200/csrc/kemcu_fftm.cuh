@@ -181,6 +181,24 @@ __device__ __forceinline__ long long fm_cell(const FmLevel& L, int x, int y, int
     return L.base + ((long long) x * L.n + y) * L.n + z;
 }
 
+// sum_k op[k K + row] x[k]: one row of a column-major K x K operator times x, in four
+// independent chains over k mod 4 (a single accumulator is a 2K-step dependent chain, the
+// translation kernels' latency with one right-hand side)
+__device__ __forceinline__ double fm_op_row(const double* __restrict__ op, int row, int K, const double* x)
+{
+    double a0 = 0., a1 = 0., a2 = 0., a3 = 0.;
+    int k = 0;
+    for (; k + 3 < K; k += 4) {
+        a0 = fma(op[(size_t) k * K + row], x[k], a0);
+        a1 = fma(op[(size_t) (k + 1) * K + row], x[k + 1], a1);
+        a2 = fma(op[(size_t) (k + 2) * K + row], x[k + 2], a2);
+        a3 = fma(op[(size_t) (k + 3) * K + row], x[k + 3], a3);
+    }
+    for (; k < K; k++)
+        a0 = fma(op[(size_t) k * K + row], x[k], a0);
+    return (a0 + a1) + (a2 + a3);
+}
+
 template<int NR>
 __global__ void fm_m2m_kernel(const int* __restrict__ parents, int nparents, FmLevel Lp, FmLevel Lc,
                               const unsigned char* __restrict__ occ, const double* __restrict__ ops, int K,
@@ -212,7 +230,9 @@ __global__ void fm_m2m_kernel(const int* __restrict__ parents, int nparents, FmL
                 __syncthreads();
                 if (row < K) {
                     const double* op = ops + (size_t) ((cx * d + cy) * d + cz) * K * K;
-                    if (NR == 1 || nrhs == NR) {
+                    if (NR == 1)
+                        acc[0] += fm_op_row(op, row, K, fm_x);
+                    else if (nrhs == NR) {
                         for (int k = 0; k < K; k++) {
                             const double o = op[(size_t) k * K + row];
 #pragma unroll
@@ -261,21 +281,25 @@ __global__ void fm_l2l_kernel(const int* __restrict__ children, int nchildren, F
     if (row >= K)
         return;
     const double* op = ops + (size_t) (((cx % d) * d + (cy % d)) * d + (cz % d)) * K * K;
-    double acc[NR];
-#pragma unroll
-    for (int r = 0; r < NR; r++)
-        acc[r] = 0.;
-    for (int k = 0; k < K; k++) {
-        const double o = op[(size_t) k * K + row];
+    if (NR == 1)
+        Lx[(Lc.base + cc) * K + row] += fm_op_row(op, row, K, fm_x);
+    else {
+        double acc[NR];
 #pragma unroll
         for (int r = 0; r < NR; r++)
-            if (NR == 1 || r < nrhs)
-                acc[r] = fma(o, fm_x[r * K + k], acc[r]);
-    }
+            acc[r] = 0.;
+        for (int k = 0; k < K; k++) {
+            const double o = op[(size_t) k * K + row];
 #pragma unroll
-    for (int r = 0; r < NR; r++)
-        if (NR == 1 || r < nrhs)
-            Lx[r * lstride + (Lc.base + cc) * K + row] += acc[r];
+            for (int r = 0; r < NR; r++)
+                if (r < nrhs)
+                    acc[r] = fma(o, fm_x[r * K + k], acc[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < NR; r++)
+            if (r < nrhs)
+                Lx[r * lstride + (Lc.base + cc) * K + row] += acc[r];
+    }
 }
 
 // M2L at one level: every flagged target cell receives the moments of the occupied cells of its
@@ -331,7 +355,9 @@ __global__ void fm_m2l_kernel(const int* __restrict__ targets, int ntargets, FmL
                 __syncthreads();
                 if (row < K && oi >= 0) {
                     const double* op = ops + (size_t) oi * K * K;
-                    if (NR == 1 || nrhs == NR) {
+                    if (NR == 1)
+                        acc[0] += fm_op_row(op, row, K, fm_x);
+                    else if (nrhs == NR) {
                         for (int k = 0; k < K; k++) {
                             const double o = op[(size_t) k * K + row];
 #pragma unroll
