@@ -137,21 +137,35 @@ __global__ void fm_p2m_kernel(const double* __restrict__ rec, const double* __re
 // element order, of src times the element's unit-density moments (em, from fm_p2m_kernel with
 // unit sources, kept from the tree's construction: the geometry fixes them). One warp per cell,
 // lanes over the K coefficients; run[c] = (first, count) of owner cell key[c] in em / order.
+template<int NR>
 __global__ void fm_cell_sum_kernel(const double* __restrict__ em, const double* __restrict__ src,
                                    const int* __restrict__ order, const int* __restrict__ key,
-                                   const int2* __restrict__ run, int ncells, int K, double* __restrict__ M)
+                                   const int2* __restrict__ run, int ncells, int K, double* __restrict__ M,
+                                   int nrhs, size_t n, size_t mstride)
 {
     const int c = (int) ((blockIdx.x * (size_t) blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (c >= ncells)
         return;
     const int2 rg = run[c];
-    double* dst = M + (size_t) key[c] * K;
     for (int i = lane; i < K; i += 32) {
-        double s = 0.;
-        for (int j = 0; j < rg.y; j++)
-            s += src[order[rg.x + j]] * em[(size_t) (rg.x + j) * K + i];
-        dst[i] = s;
+        // every cached moment read serves all right-hand sides
+        double s[NR];
+#pragma unroll
+        for (int r = 0; r < NR; r++)
+            s[r] = 0.;
+        for (int j = 0; j < rg.y; j++) {
+            const int e = order[rg.x + j];
+            const double m = em[(size_t) (rg.x + j) * K + i];
+#pragma unroll
+            for (int r = 0; r < NR; r++)
+                if (NR == 1 || r < nrhs)
+                    s[r] += src[r * n + e] * m;
+        }
+#pragma unroll
+        for (int r = 0; r < NR; r++)
+            if (NR == 1 || r < nrhs)
+                M[r * mstride + (size_t) key[c] * K + i] = s[r];
     }
 }
 
