@@ -57,6 +57,11 @@ Fixtures:
                  (KFastMultipoleMatrixGenerator, degree 8, depth 3) times the coax_small density
                  and times a seeded vector on mixed_small (Neumann rows and wires), with the world
                  cubes of those trees
+  c2_fftm        configuration 2's 44,000-element coax with its fixed density
+                 (geometry.coax_density) under the reference's fast multipole code with region
+                 estimation (degree 8, divisions 2, zeromask 1, depth 5): the world cube it
+                 estimated, the field at 2,000 seeded gap points, and its matrix
+                 (KFastMultipoleMatrixGenerator) times the density
   krylov         the reference's Krylov solvers on the coax_small system: the solver factory
                  (KBuildKrylovSolver, the path of KKrylovChargeDensitySolver) with gmres and
                  bicgstab, preconditioners none, jacobi and implicit_krylov (inner gmres on the
@@ -531,6 +536,19 @@ def fftm():
          coax_Ax_d3=coax_Ax, mixed_Ax_d3=mixed_Ax, mixed_world_d3=mixed_world)
 
 
+def c2_fftm():
+    from oracle import ref_fm
+
+    mesh = G.coax()
+    sigma = G.coax_density(mesh)
+    pts = G.gap_points(2000, seed=2049)
+    fr = ref_fm.FmRefProblem(mesh)
+    fr.set_sigma(sigma)
+    field, world = fr.field(pts, degree=8, maximum_tree_depth=5)
+    Ax = fr.matvec(sigma, degree=8, maximum_tree_depth=5)
+    save("c2_fftm", points=pts, field=field, world=world, Ax=Ax)
+
+
 def krylov():
     from oracle import ref_fm
 
@@ -568,7 +586,7 @@ def golden_mesh(name):
 
 FIXTURES = {f.__name__: f for f in (rules, integrators, lines, icosphere, mixed_small, coax_small, rk8, adjoint,
                                      robinhood, axisym, c1_sphere, c2_coax, c3_tracks, c4_adjoint, c5_rings, fftm,
-                                     krylov)}
+                                     krylov, c2_fftm)}
 
 if __name__ == "__main__":
     for name in sys.argv[1:] or list(FIXTURES):

@@ -273,3 +273,26 @@ def test_fftm_other_divisions_and_zeromask_equal_live_reference(t, d, zm, depth)
     got = ctx.FFTMField(P)
     err = np.abs(got - want).max(axis=0) / np.abs(want).max(axis=0)
     assert np.all(err[:3] <= 1e-11) and err[3] <= 1e-13, err
+
+
+def test_fftm_full_coax_equals_reference_fixture():
+    # configuration 2's coax at its stated size (44,000 elements) with its fixed density and the
+    # reference's own region estimate (no world cube given on either side): the same cube, the
+    # reference's field at 2,000 gap points and its matrix times the density
+    fx = golden.load("c2_fftm")
+    mesh = G.coax()
+    sigma = G.coax_density(mesh)
+    ctx = K.CUDAElectrostaticContext(0)
+    ctx.SetGeometry(mesh)
+    ctx.SetSigma(sigma)
+    ctx.ConfigureFFTM(degree=8, maximum_tree_depth=5)
+    info = ctx.FFTMInfo(5)
+    got_world = np.r_[info["world_center"], info["world_length"]]
+    assert np.abs(got_world - fx["world"]).max() <= 1e-9 * fx["world"][3]
+    got = ctx.FFTMField(fx["points"])
+    want = fx["field"]
+    err = np.abs(got - want).max(axis=0) / np.abs(want).max(axis=0)
+    # as on the reduced coax: the gap potential is a difference of much larger contributions
+    assert np.all(err[:3] <= 1e-11) and err[3] <= 2e-11, err
+    Ax = fx["Ax"]
+    assert np.abs(ctx.FFTMMultiply(sigma) - Ax).max() <= 1e-11 * np.abs(Ax).max()
