@@ -291,7 +291,7 @@ int kemcu_fma_peak(kemcu_ctx* ctx, double* fp64_tflops, double* fp32_tflops);
    interaction lists, ((2 (zeromask+1) divisions - 1)^3 - (2 zeromask + 1)^3) matrices of
    (degree+1)^4 doubles) must fit in 8 GB. */
 typedef struct {
-    int degree;                     /* expansion degree p, 1..15 (KFMElectrostaticParameters::degree) */
+    int degree;                     /* expansion degree p, 0..15 (KFMElectrostaticParameters::degree) */
     int top_level_divisions;        /* divisions of the root per dimension, 1..8 */
     int divisions;                  /* divisions of every further level per dimension, 2..8 (2) */
     int zeromask;                   /* neighbour order: cells within it are summed directly, 1..3 (1) */
@@ -329,8 +329,8 @@ int kemcu_fftm_info(const kemcu_ctx* ctx, double* world4, int* counts);
    degree = preconditioner_degree for the reference's "implicit_krylov" (a lower-degree
    operator on the same tree, KFMElectrostaticFastMultipoleBoundaryValueSolver.cc:726-745), or
    the preconditioner_electrostatic_parameters for "independent_implicit_krylov" (:831-848).
-   Degree 1..15 (the reference's default preconditioner_degree 0 is refused with
-   KEMCU_EINVAL). Replaces the previous preconditioner tree. */
+   Degree 0..15 (0, the reference's default preconditioner_degree, keeps the monopoles only).
+   Replaces the previous preconditioner tree. */
 int kemcu_fftm_configure_preconditioner(kemcu_ctx* ctx, const kemcu_fftm_params* prm);
 
 /* ---- Krylov charge-density solves with restarts and right preconditioners: the solver

@@ -559,7 +559,8 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
     {
         fPreMaxIterations = n >= (unsigned int) INT_MAX ? INT_MAX : (int) n;
     }
-    // the degree of the implicit_krylov preconditioner's tree (1..15)
+    // the degree of the implicit_krylov preconditioner's tree (0..15; 0 by default, as the
+    // reference's KFMElectrostaticFastMultipoleBoundaryValueSolverConfiguration)
     void SetPreconditionerDegree(unsigned int d)
     {
         fPreDegree = (int) d;
@@ -685,7 +686,7 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
     int fSolver = KEMCU_KRYLOV_GMRES, fPrecon = KEMCU_PRECON_NONE, fRestart = 0;
     bool fIndependent = false;
     double fPreTolerance = 0.01;
-    int fPreMaxIterations = 30, fPreDegree = 1, fPreMode = KEMCU_SOLVE_FP32;
+    int fPreMaxIterations = 30, fPreDegree = 0, fPreMode = KEMCU_SOLVE_FP32;
     kemcu_fftm_params fPreFftm = KCUDADefaultFastMultipoleParameters();
     kemcu_solve_stats fStats{};
 };

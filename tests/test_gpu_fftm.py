@@ -146,7 +146,7 @@ def test_fftm_state_and_argument_errors():
     ctx.SetSigma(np.ones(80) * 1e-9)
     with pytest.raises(K.KemcuError):
         ctx.FFTMField(np.zeros((4, 3)))  # not configured
-    for bad in ({"divisions": 1}, {"divisions": 9}, {"zeromask": 0}, {"zeromask": 4}, {"degree": 0}, {"degree": 16},
+    for bad in ({"divisions": 1}, {"divisions": 9}, {"zeromask": 0}, {"zeromask": 4}, {"degree": -1}, {"degree": 16},
                 {"maximum_tree_depth": 11}):
         with pytest.raises(K.KemcuError):
             ctx.ConfigureFFTM(**bad)

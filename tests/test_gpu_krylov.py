@@ -174,4 +174,21 @@ def test_krylov_argument_errors(coax):
     assert L.kemcu_krylov_solve(fresh._h, None, xp, 1, p2, None) == N.ESTATE
     fresh.ConfigureFFTM(degree=4, maximum_tree_depth=2)
     with pytest.raises(K.KemcuError):
-        fresh.ConfigureFFTMPreconditioner(degree=0, maximum_tree_depth=2)
+        fresh.ConfigureFFTMPreconditioner(degree=-1, maximum_tree_depth=2)
+
+
+@needs_ref_fm
+def test_fftm_degree0_preconditioner_matches_reference(coax_fftm):
+    # the reference's default preconditioner_degree 0: a monopole-only tree (KFMElectrostatic-
+    # FastMultipoleBoundaryValueSolverConfiguration), live against the reference's boundary-value
+    # solver with the same settings
+    ctx, fx, mesh = coax_fftm
+    ctx.ConfigureFFTMPreconditioner(degree=0, maximum_tree_depth=3)
+    x, st = ctx.KrylovSolve(solver="gmres", mode=K.SOLVE_FFTM, tol=1e-6, max_iter=200,
+                            preconditioner="implicit_krylov", preconditioner_mode=K.SOLVE_FFTM,
+                            preconditioner_tol=0.01, max_preconditioner_iter=30)
+    assert st["rel_residual"] <= 3e-6 and st["low_matvecs"] > 0
+    fr = ref_fm.FmRefProblem(mesh)
+    xr, _ = fr.solve("gmres", "implicit_krylov", tol=1e-6, max_iter=200, preconditioner_tol=0.01,
+                     max_preconditioner_iter=30, preconditioner_degree=0, degree=8, maximum_tree_depth=3)
+    assert np.abs(x - xr).max() <= 5e-5 * np.abs(xr).max()
