@@ -192,3 +192,31 @@ def test_fftm_degree0_preconditioner_matches_reference(coax_fftm):
     xr, _ = fr.solve("gmres", "implicit_krylov", tol=1e-6, max_iter=200, preconditioner_tol=0.01,
                      max_preconditioner_iter=30, preconditioner_degree=0, degree=8, maximum_tree_depth=3)
     assert np.abs(x - xr).max() <= 5e-5 * np.abs(xr).max()
+
+
+@pytest.mark.parametrize("pmode,mode", [(K.SOLVE_FP32, K.SOLVE_PLAIN), (K.SOLVE_MIXED, K.SOLVE_PLAIN),
+                                        (K.SOLVE_ASSEMBLED, K.SOLVE_ASSEMBLED_FP64)])
+def test_implicit_krylov_on_reduced_operators(coax, pmode, mode):
+    # the implicit Krylov preconditioner's inner GMRES on a cheaper form of the direct operator
+    # (FP32 far field, MIXED, or the FP32 copy of the assembled operator): the outer solve keeps
+    # the FP64 operator's accuracy and reaches the direct solution
+    ctx, fx, _ = coax
+    x, st = ctx.KrylovSolve(solver="gmres", mode=mode, tol=1e-9, max_iter=300, preconditioner="implicit_krylov",
+                            preconditioner_mode=pmode, preconditioner_tol=0.1, max_preconditioner_iter=10)
+    assert st["rel_residual"] <= 2e-9 and st["low_matvecs"] > 0
+    xd = fx["direct_sigma"]
+    assert np.abs(x - xd).max() <= 1e-6 * np.abs(xd).max()
+
+
+def test_axisymmetric_system_solvers_agree():
+    # conic sections: BiCGStab with the Jacobi preconditioner (the axisymmetric diagonal) and
+    # restarted GMRES reach the plain GMRES solution
+    from kassiopeia_b200 import geometry as G
+    ctx = K.CUDAElectrostaticContext(0)
+    ctx.SetGeometry(G.conic_sphere(120))
+    x0, _ = ctx.Solve(tol=1e-12, max_iter=300)
+    for kw in (dict(solver="bicgstab", preconditioner="jacobi"), dict(solver="gmres", restart=5),
+               dict(solver="gmres", preconditioner="jacobi")):
+        x, st = ctx.KrylovSolve(mode=K.SOLVE_PLAIN, tol=1e-11, max_iter=300, **kw)
+        assert st["rel_residual"] <= 1e-10, kw
+        assert np.abs(x - x0).max() <= 1e-8 * np.abs(x0).max(), kw
