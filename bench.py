@@ -445,10 +445,15 @@ def run_native(args, rank, world, dist):
         t8 = c5.last_kernel_ms
         _, s5 = c5.Solve(B, tol=TOL, mode=K.SOLVE_ASSEMBLED)  # allocates and assembles the operator
         _, s5r = c5.Solve(B, tol=TOL, mode=K.SOLVE_ASSEMBLED)
+        # the same refinement with the Jacobi preconditioner on its FP32 inner solves
+        _, s5j = c5.KrylovSolve(B, mode=K.SOLVE_ASSEMBLED, tol=TOL, max_iter=500, preconditioner="jacobi",
+                                raise_on_failure=False)
         extra["c5_stacked_rings_100k_8rhs"] = {
             "matrix_free_fp64_matvec_ms_1rhs": t1, "matrix_free_fp64_matvec_ms_8rhs": t8,
             "assembled_solve_s": s5["seconds"], "assembled_solve_repeat_s": s5r["seconds"],
-            "krylov_iterations": s5["iterations"], "rel_residual": s5["rel_residual"]}
+            "krylov_iterations": s5["iterations"], "rel_residual": s5["rel_residual"],
+            "assembled_jacobi_solve_s": s5j["seconds"], "assembled_jacobi_krylov_iterations": s5j["iterations"],
+            "assembled_jacobi_rel_residual": s5j["rel_residual"], "assembled_jacobi_converged": s5j["status"] == 0}
         # the same 8 right-hand sides on the FFTM operator (no assembled operator: it is released
         # with the geometry's other buffers when the tree is built on a fresh context)
         with K.CUDAElectrostaticContext(dev) as fc:

@@ -352,13 +352,20 @@ int kemcu_fftm_configure_preconditioner(kemcu_ctx* ctx, const kemcu_fftm_params*
    restarts), fp64_matvecs = applications of the system's operator, low_matvecs = of the
    preconditioner's, rel_residual = max over RHS of |b - A x| / |b| recomputed at the end with the
    system's operator, rel_residual_estimate = the solver's own residual norm over |b|. Returns
-   KEMCU_ENOTCONVERGED when the solver's residual norm is above the tolerance at the end. */
+   KEMCU_ENOTCONVERGED when the solver's residual norm (for the refinement modes the FP64 one) is
+   above the tolerance at the end. For the refinement modes, outer counts the refinement steps,
+   fp64_matvecs the FP64 products and low_matvecs the inner solves' and the preconditioner's. */
 enum kemcu_krylov_solver { KEMCU_KRYLOV_GMRES = 0, KEMCU_KRYLOV_BICGSTAB = 1 };
 enum kemcu_preconditioner { KEMCU_PRECON_NONE = 0, KEMCU_PRECON_JACOBI = 1, KEMCU_PRECON_IMPLICIT_KRYLOV = 2 };
 typedef struct {
     int solver;                         /* kemcu_krylov_solver ("solver_name": gmres, bicgstab) */
-    int mode;                           /* the system's operator: KEMCU_SOLVE_PLAIN (FP64 matrix-free),
-                                           KEMCU_SOLVE_ASSEMBLED_FP64 or KEMCU_SOLVE_FFTM */
+    int mode;                           /* kemcu_solve_mode: KEMCU_SOLVE_PLAIN (FP64 matrix-free),
+                                           KEMCU_SOLVE_ASSEMBLED_FP64 or KEMCU_SOLVE_FFTM solve that
+                                           operator; KEMCU_SOLVE_MIXED, _ASSEMBLED and _FP32 refine
+                                           as kemcu_gmres does (FP64 residuals, corrections from
+                                           inner solves on the reduced operator), the solver, its
+                                           restarts and the preconditioner applying to the inner
+                                           solves */
     double tolerance;                   /* "tolerance" */
     int max_iterations;                 /* "max_iterations" (bounds the GMRES basis kept on the device) */
     int iterations_between_restarts;    /* "iterations_between_restarts"; 0 = never */

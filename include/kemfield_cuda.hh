@@ -519,8 +519,8 @@ class KCUDAChargeDensitySolver : public KCUDAChargeDensitySolverBase
     // max_preconditioner_iterations and preconditioner_degree of krylov_bem_solver,
     // KKrylovChargeDensitySolverOldBuilder.hh, and the dispatch of
     // KFMElectrostaticFastMultipoleBoundaryValueSolver.cc:189-233). Plain GMRES without restarts
-    // runs kemcu_gmres (every mode); any other choice runs kemcu_krylov_solve on the modes plain,
-    // assembled_fp64 and fftm.
+    // runs kemcu_gmres; any other choice runs kemcu_krylov_solve (for the refinement modes mixed,
+    // assembled and fp32 the solver and preconditioner apply to the inner solves).
     void SetSolverName(const std::string& name)
     {
         if (name == "gmres")

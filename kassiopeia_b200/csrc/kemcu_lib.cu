@@ -1027,6 +1027,62 @@ double inner_tolerance()
     const char* s = getenv("KEMCU_INNER_TOL");
     return s ? atof(s) : 1e-6;
 }
+
+// Iterative refinement (solve modes KEMCU_SOLVE_MIXED, _ASSEMBLED and _FP32): x from 0, then
+// repeatedly a correction d from an inner solve of A_low d = r (inner(r, d, tol, iterations,
+// estimate, products)) and the residual r = b - A x with the FP64 operator hi_op, until the
+// worst right-hand side's |r| / |b| is at most rel_tol (or an inner solve makes no progress,
+// or 20 steps). The inner solve only has to bring the worst right-hand side to a tenth of the
+// target: from relative residual rel, a reduction by 0.1 rel_tol / rel suffices (the first
+// step, rel = 1, runs to the inner tolerance).
+template<class Inner>
+int refine_solve(kemcu_ctx* ctx, int hi_op, const double* d_b, double* d_x, double* d_r, double* d_d, int n_rhs,
+                 double rel_tol, Inner inner, int& iters, double& est, double& rel, int& steps, int& fp64, int& low)
+{
+    const int n = (int) ctx->n;
+    const size_t m = (size_t) n_rhs * n;
+    int rc;
+    const double tin = std::max(rel_tol, inner_tolerance());
+    KC(cudaMemsetAsync(d_x, 0, m * sizeof(double), ctx->stream));
+    KC(cudaMemcpyAsync(d_r, d_b, m * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    std::vector<double> hb(m);
+    KC(cudaMemcpyAsync(hb.data(), d_b, m * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    KC(cudaStreamSynchronize(ctx->stream));
+    std::vector<double> bn(n_rhs, 0.);
+    for (int r = 0; r < n_rhs; r++) {
+        for (int i = 0; i < n; i++)
+            bn[r] += hb[(size_t) r * n + i] * hb[(size_t) r * n + i];
+        bn[r] = std::sqrt(bn[r]);
+    }
+    rel = 1.;
+    for (int outer = 0; outer < 20; outer++) {
+        int it = 0;
+        const double tin_k = std::min(0.5, std::max(tin, 0.1 * rel_tol / rel));
+        if ((rc = inner(d_r, d_d, tin_k, it, est, low)))
+            return rc;
+        iters += it;
+        axpy_kernel<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(1., d_d, d_x, m);
+        KCHECK_LAUNCH();
+        if ((rc = apply_op(ctx, hi_op, d_x, d_r, n_rhs)))
+            return rc;
+        fp64++;
+        residual_kernel<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(d_b, d_r, m);
+        KCHECK_LAUNCH();
+        KC(cudaMemcpyAsync(hb.data(), d_r, m * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        KC(cudaStreamSynchronize(ctx->stream));
+        rel = 0.;
+        for (int r = 0; r < n_rhs; r++) {
+            double s = 0.;
+            for (int i = 0; i < n; i++)
+                s += hb[(size_t) r * n + i] * hb[(size_t) r * n + i];
+            rel = std::max(rel, bn[r] > 0. ? std::sqrt(s) / bn[r] : 0.);
+        }
+        steps = outer + 1;
+        if (rel <= rel_tol || it == 0)
+            break;
+    }
+    return KEMCU_OK;
+}
 }  // namespace
 
 // ------------------------------------------------------------------------------- C ABI
@@ -1612,48 +1668,12 @@ int kemcu_gmres(kemcu_ctx* ctx, const double* b, double* x, int n_rhs, double re
             low_op = kDense32;
             hi_op = kDense64;
         }
-        const double tin = std::max(rel_tol, inner_tolerance());
-        KC(cudaMemsetAsync(d_x, 0, m * sizeof(double), ctx->stream));
-        KC(cudaMemcpyAsync(d_r, d_b, m * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-        std::vector<double> hb(m);
-        KC(cudaMemcpyAsync(hb.data(), d_b, m * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        KC(cudaStreamSynchronize(ctx->stream));
-        std::vector<double> bn(n_rhs, 0.);
-        for (int r = 0; r < n_rhs; r++) {
-            for (int i = 0; i < n; i++)
-                bn[r] += hb[(size_t) r * n + i] * hb[(size_t) r * n + i];
-            bn[r] = std::sqrt(bn[r]);
-        }
-        rel = 1.;
-        for (int outer = 0; outer < 20; outer++) {
-            int it = 0;
-            // the inner solve only has to bring the worst right-hand side to a tenth of the
-            // target: from relative residual rel, a reduction by 0.1 rel_tol / rel suffices
-            // (the first step, rel = 1, runs to the inner tolerance)
-            const double tin_k = std::min(0.5, std::max(tin, 0.1 * rel_tol / rel));
-            if ((rc = gmres_core(ctx, low_op, d_r, d_d, n_rhs, tin_k, max_iter, it, est, low)))
-                return rc;
-            iters += it;
-            axpy_kernel<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(1., d_d, d_x, m);
-            KCHECK_LAUNCH();
-            if ((rc = apply_op(ctx, hi_op, d_x, d_r, n_rhs)))
-                return rc;
-            fp64++;
-            residual_kernel<<<(unsigned) ((m + 255) / 256), 256, 0, ctx->stream>>>(d_b, d_r, m);
-            KCHECK_LAUNCH();
-            KC(cudaMemcpyAsync(hb.data(), d_r, m * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-            KC(cudaStreamSynchronize(ctx->stream));
-            rel = 0.;
-            for (int r = 0; r < n_rhs; r++) {
-                double s = 0.;
-                for (int i = 0; i < n; i++)
-                    s += hb[(size_t) r * n + i] * hb[(size_t) r * n + i];
-                rel = std::max(rel, bn[r] > 0. ? std::sqrt(s) / bn[r] : 0.);
-            }
-            st.outer = outer + 1;
-            if (rel <= rel_tol || it == 0)
-                break;
-        }
+        auto inner = [&](const double* r, double* d, double tol, int& it, double& e, int& mv) {
+            return gmres_core(ctx, low_op, r, d, n_rhs, tol, max_iter, it, e, mv);
+        };
+        if ((rc = refine_solve(ctx, hi_op, d_b, d_x, d_r, d_d, n_rhs, rel_tol, inner, iters, est, rel, st.outer, fp64,
+                               low)))
+            return rc;
     }
     t.stop();
     st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -153,7 +153,7 @@ def test_krylov_argument_errors(coax):
     L.kemcu_krylov_default_params(prm)
     x = np.zeros(ctx.n)
     xp = x.ctypes.data_as(N._dp)
-    bad = [("solver", 7), ("mode", K.SOLVE_MIXED), ("tolerance", 0.), ("max_iterations", 0),
+    bad = [("solver", 7), ("mode", 9), ("tolerance", 0.), ("max_iterations", 0),
            ("iterations_between_restarts", -1), ("preconditioner", 3)]
     for field, value in bad:
         p2 = N.KrylovParams.from_buffer_copy(prm)
@@ -220,3 +220,15 @@ def test_axisymmetric_system_solvers_agree():
         x, st = ctx.KrylovSolve(mode=K.SOLVE_PLAIN, tol=1e-11, max_iter=300, **kw)
         assert st["rel_residual"] <= 1e-10, kw
         assert np.abs(x - x0).max() <= 1e-8 * np.abs(x0).max(), kw
+
+
+@pytest.mark.parametrize("mode", [K.SOLVE_ASSEMBLED, K.SOLVE_MIXED, K.SOLVE_FP32])
+@pytest.mark.parametrize("solver,pc", [("gmres", "jacobi"), ("bicgstab", "jacobi"), ("gmres", "none")])
+def test_refinement_modes_with_solver_choices(coax, mode, solver, pc):
+    # iterative refinement (FP64 residuals) with the inner solves by the chosen solver and
+    # preconditioner on the reduced operator: the FP64 accuracy of the plain solve
+    ctx, fx, _ = coax
+    x, st = ctx.KrylovSolve(solver=solver, mode=mode, tol=1e-10, max_iter=300, preconditioner=pc)
+    assert st["rel_residual"] <= 1e-10 and st["outer"] >= 1 and st["fp64_matvecs"] >= 2
+    xd = fx["direct_sigma"]
+    assert np.abs(x - xd).max() <= 1e-7 * np.abs(xd).max()
