@@ -235,6 +235,10 @@ def run_native(args, rank, world, dist):
         # far-field operator, FP64 residual and refinement
         x_f32, st_f32 = ctx.Solve(tol=TOL, max_iter=300, mode=K.SOLVE_FP32)
         st_asm["fp32_refined_matrix_free"] = st_f32
+        # the assembled refinement with the Jacobi preconditioner on its FP32 inner solves
+        _, st_aj = ctx.KrylovSolve(tol=TOL, max_iter=300, mode=K.SOLVE_ASSEMBLED, preconditioner="jacobi",
+                                   raise_on_failure=False)
+        st_asm["mixed_assembled_jacobi"] = st_aj
         sigma_diff = float(np.max(np.abs(x_asm - x_plain)) / np.max(np.abs(x_plain)))
     ctx.SetSigma(x_asm)
 
@@ -821,6 +825,11 @@ def gmres_summary(r):
         out["speedup_assembly_only"] = p["seconds"] / a64["repeat_seconds"]
     if a["seconds"] == a["seconds"] and a["seconds"] > 0:
         out["speedup_mixed_first_solve_over_plain_matrix_free"] = p["seconds"] / a["seconds"]
+    aj = a.get("mixed_assembled_jacobi")
+    if aj:
+        out["mixed_assembled_jacobi_s"] = aj["seconds"]
+        out["mixed_assembled_jacobi_iterations"] = aj["iterations"]
+        out["mixed_assembled_jacobi_rel_residual"] = aj["rel_residual"]
     f32 = a.get("fp32_refined_matrix_free")
     if f32:
         out["fp32_refined_matrix_free_s"] = f32["seconds"]
