@@ -774,6 +774,18 @@ __device__ __forceinline__ Out4 epi_far(const double* e, V3 P, V3 d, double r2, 
     return band == 2 ? cubq_pairs<6, kPair12, -1, POT, FIELD, MIXED>(e, d, r2) : cubq_pairs<3, kPair7, 0, POT, FIELD, MIXED>(e, d, r2);
 }
 
+// epi for a pair known to lie outside the analytic band (the caller has shown that its centre
+// distance exceeds the band-0 cut): the same band decision and quadrature as epi, with no call
+// to the analytic integrals in the code path
+template<bool MIXED, bool POT, bool FIELD, bool F32 = false> __device__ __forceinline__ Out4 epi_beyond_near(const double* e,
+                                                                                                           V3 P)
+{
+    V3 d;
+    double r2;
+    const int band = band_of(e, P, d, r2);
+    return epi_far<MIXED, POT, FIELD, F32>(e, P, d, r2, band);
+}
+
 template<bool MIXED, bool POT, bool FIELD, bool F32 = false> __device__ __forceinline__ Out4 epi(const double* e, V3 P)
 {
     V3 d;

@@ -299,6 +299,24 @@ __global__ void __launch_bounds__(kThreads, MINB) field_kernel(const double* __r
     };
     R.prologue(rec, side);
     const int ntiles = R.tiles();
+    // the warp's points in a bounding sphere (centre wc, radius wr; no sphere without active
+    // lanes, and then every tile takes the general path)
+    const int lane = threadIdx.x & 31;
+    V3 wc;
+    double wr;
+    {
+        double lo[3] = {active ? P.x : 1e300, active ? P.y : 1e300, active ? P.z : 1e300};
+        double hi[3] = {active ? P.x : -1e300, active ? P.y : -1e300, active ? P.z : -1e300};
+        for (int o = 16; o > 0; o >>= 1)
+            for (int c = 0; c < 3; c++) {
+                lo[c] = fmin(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
+                hi[c] = fmax(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
+            }
+        wc = v3(0.5 * (lo[0] + hi[0]), 0.5 * (lo[1] + hi[1]), 0.5 * (lo[2] + hi[2]));
+        wr = 0.5 * sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
+                        (hi[2] - lo[2]) * (hi[2] - lo[2]));
+    }
+    const bool warp_active = __any_sync(0xffffffffu, active);
     Kahan kx, ky, kz, kp;
     bool ok = true;
     for (int i = 0; i < ntiles; i++) {
@@ -306,20 +324,49 @@ __global__ void __launch_bounds__(kThreads, MINB) field_kernel(const double* __r
             ok = false;
             break;
         }
-        if (active) {
-            const int cnt = R.count(i);
-            double tx = 0., ty = 0., tz = 0., tp = 0.;
-            for (int j = 0; j < cnt; j++) {
-                const Out4 r = epi<MIXED, POT, FIELD, F32>(R.element(i, j), P);
-                const double sg = R.side(i, 0, j);
-                if (FIELD) {
-                    tx = fma(r.ex, sg, tx);
-                    ty = fma(r.ey, sg, ty);
-                    tz = fma(r.ez, sg, tz);
-                }
-                if (POT)
-                    tp = fma(r.phi, sg, tp);
+        const int cnt = R.count(i);
+        // far tile: every element of the tile is beyond its analytic band for every point of the
+        // warp (centre distance minus the sphere's radius, less a rounding allowance, above the
+        // band-0 cut distance with a relative margin), so the pair loop needs no analytic call
+        bool near = true;
+        if (warp_active) {
+            near = false;
+            for (int j = lane; j < cnt; j += 32) {
+                const double* e = R.element(i, j);
+                const double dx = e[rCen] - wc.x, dy = e[rCen + 1] - wc.y, dz = e[rCen + 2] - wc.z;
+                const double dist = sqrt(dx * dx + dy * dy + dz * dz);
+                const double dm = dist - wr - 1e-12 * (dist + wr);
+                near = near || !(dm > 0. && dm * dm > e[rCut] * (1. + 1e-6));
             }
+            near = __any_sync(0xffffffffu, near);
+        }
+        if (active) {
+            double tx = 0., ty = 0., tz = 0., tp = 0.;
+            if (!near) {
+                for (int j = 0; j < cnt; j++) {
+                    const Out4 r = epi_beyond_near<MIXED, POT, FIELD, F32>(R.element(i, j), P);
+                    const double sg = R.side(i, 0, j);
+                    if (FIELD) {
+                        tx = fma(r.ex, sg, tx);
+                        ty = fma(r.ey, sg, ty);
+                        tz = fma(r.ez, sg, tz);
+                    }
+                    if (POT)
+                        tp = fma(r.phi, sg, tp);
+                }
+            }
+            else
+                for (int j = 0; j < cnt; j++) {
+                    const Out4 r = epi<MIXED, POT, FIELD, F32>(R.element(i, j), P);
+                    const double sg = R.side(i, 0, j);
+                    if (FIELD) {
+                        tx = fma(r.ex, sg, tx);
+                        ty = fma(r.ey, sg, ty);
+                        tz = fma(r.ez, sg, tz);
+                    }
+                    if (POT)
+                        tp = fma(r.phi, sg, tp);
+                }
             if (FIELD) {
                 kx.add(tx);
                 ky.add(ty);
