@@ -269,6 +269,37 @@ template<int SIDE, int NP = kPipe, bool CYCLIC = false> struct ElementRing
     }
 };
 
+// A warp's points in a bounding sphere, and whether a tile of the element ring holds an element
+// within its analytic band of any of them: the element's centre distance from the sphere's
+// centre, less the radius and a 1e-12 rounding allowance, squared, must exceed the band-0 cut with
+// a 1e-6 margin for the tile to be far (then the fast band comparison of band_of decides band >= 1
+// for every pair, as the exact one would). Called by all 32 lanes.
+__device__ __forceinline__ void warp_sphere(bool active, V3 P, V3& wc, double& wr)
+{
+    double lo[3] = {active ? P.x : 1e300, active ? P.y : 1e300, active ? P.z : 1e300};
+    double hi[3] = {active ? P.x : -1e300, active ? P.y : -1e300, active ? P.z : -1e300};
+    for (int o = 16; o > 0; o >>= 1)
+        for (int c = 0; c < 3; c++) {
+            lo[c] = fmin(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
+            hi[c] = fmax(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
+        }
+    wc = v3(0.5 * (lo[0] + hi[0]), 0.5 * (lo[1] + hi[1]), 0.5 * (lo[2] + hi[2]));
+    wr = 0.5 * sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
+                    (hi[2] - lo[2]) * (hi[2] - lo[2]));
+}
+template<class Ring> __device__ __forceinline__ bool tile_near(const Ring& R, int i, int cnt, V3 wc, double wr)
+{
+    bool near = false;
+    for (int j = (int) (threadIdx.x & 31); j < cnt; j += 32) {
+        const double* e = R.element(i, j);
+        const double dx = e[rCen] - wc.x, dy = e[rCen + 1] - wc.y, dz = e[rCen + 2] - wc.z;
+        const double dist = sqrt(dx * dx + dy * dy + dz * dz);
+        const double dm = dist - wr - 1e-12 * (dist + wr);
+        near = near || !(dm > 0. && dm * dm > e[rCut] * (1. + 1e-6));
+    }
+    return __any_sync(0xffffffffu, near);
+}
+
 // K1: field and/or potential at points. out layout per point: (Ex, Ey, Ez, phi).
 // The analytic near-field pairs (band 0: RWG triangles and rectangles, analytic wires) are
 // evaluated in place through a non-inlined call: a design with a call-free quadrature kernel and
@@ -299,23 +330,11 @@ __global__ void __launch_bounds__(kThreads, MINB) field_kernel(const double* __r
     };
     R.prologue(rec, side);
     const int ntiles = R.tiles();
-    // the warp's points in a bounding sphere (centre wc, radius wr; no sphere without active
-    // lanes, and then every tile takes the general path)
-    const int lane = threadIdx.x & 31;
+    // the warp's points in a bounding sphere (no sphere without active lanes, and then every
+    // tile takes the general path)
     V3 wc;
     double wr;
-    {
-        double lo[3] = {active ? P.x : 1e300, active ? P.y : 1e300, active ? P.z : 1e300};
-        double hi[3] = {active ? P.x : -1e300, active ? P.y : -1e300, active ? P.z : -1e300};
-        for (int o = 16; o > 0; o >>= 1)
-            for (int c = 0; c < 3; c++) {
-                lo[c] = fmin(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
-                hi[c] = fmax(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
-            }
-        wc = v3(0.5 * (lo[0] + hi[0]), 0.5 * (lo[1] + hi[1]), 0.5 * (lo[2] + hi[2]));
-        wr = 0.5 * sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
-                        (hi[2] - lo[2]) * (hi[2] - lo[2]));
-    }
+    warp_sphere(active, P, wc, wr);
     const bool warp_active = __any_sync(0xffffffffu, active);
     Kahan kx, ky, kz, kp;
     bool ok = true;
@@ -326,20 +345,8 @@ __global__ void __launch_bounds__(kThreads, MINB) field_kernel(const double* __r
         }
         const int cnt = R.count(i);
         // far tile: every element of the tile is beyond its analytic band for every point of the
-        // warp (centre distance minus the sphere's radius, less a rounding allowance, above the
-        // band-0 cut distance with a relative margin), so the pair loop needs no analytic call
-        bool near = true;
-        if (warp_active) {
-            near = false;
-            for (int j = lane; j < cnt; j += 32) {
-                const double* e = R.element(i, j);
-                const double dx = e[rCen] - wc.x, dy = e[rCen + 1] - wc.y, dz = e[rCen + 2] - wc.z;
-                const double dist = sqrt(dx * dx + dy * dy + dz * dz);
-                const double dm = dist - wr - 1e-12 * (dist + wr);
-                near = near || !(dm > 0. && dm * dm > e[rCut] * (1. + 1e-6));
-            }
-            near = __any_sync(0xffffffffu, near);
-        }
+        // warp, so the pair loop needs no analytic call
+        const bool near = !warp_active || tile_near(R, i, cnt, wc, wr);
         if (active) {
             double tx = 0., ty = 0., tz = 0., tp = 0.;
             if (!near) {
@@ -472,6 +479,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) matvec_kernel(const doub
     };
     R.prologue(rec, side);
     const int ntiles = R.tiles();
+    // (the far-tile split of K1 was built here too and measured slower: the second pair loop
+    // costs this kernel's register allocation more than the call it saves)
     Kahan acc[NR];
     bool ok = true;
     for (int q = 0; q < ntiles; q++) {
