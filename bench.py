@@ -40,7 +40,7 @@ TOL = 1e-10
 # DRAM bytes (read + write) of one MIXED direct-sum launch over the default 1,000,000-point
 # workload, from a one-pass ncu capture of `python bench.py --profile --points 1000000`;
 # bench.py cannot run ncu itself, so the figure is reported only for that workload
-FIELD_TRAFFIC_BYTES_1M = 69.49e6 + 83.10e6
+FIELD_TRAFFIC_BYTES_1M = 74.04e6 + 105.28e6
 # algorithmic flops per element-point interaction (field + potential) by band:
 # cubature / Gauss with n nodes: 20 n + 30 (node sums, ratio test); analytic near field:
 # fixed counts of one pass through the non-degenerate branch (frozen here)
