@@ -39,12 +39,13 @@ __device__ __forceinline__ double block_sum(double v, double* sh)
 // 8 running sums (one w load serves 8 basis entries); warp shuffles then reduce the lanes,
 // shared memory the warps of a group, and the last CTA of a right-hand side sums the slices in
 // block order, so the result does not depend on scheduling.
-__global__ void __launch_bounds__(kDotThreads) multi_dot_kernel(const double* __restrict__ V, const double* __restrict__ w,
+__global__ void __launch_bounds__(kDotThreads, 4) multi_dot_kernel(const double* __restrict__ V, const double* __restrict__ w,
                                                                 int n, int nrhs, int k0, int nk, double* __restrict__ partial,
                                                                 unsigned* __restrict__ counter, double* __restrict__ h, int hs)
 {
     static_assert(kDotThreads == 256, "8 warps of 8 basis vectors cover the 64 vectors of a launch");
     __shared__ double s_red[8][8];
+    __shared__ double s_part[64 * (kDotBlocks + 1)];  // the last CTA's copy of the slices' sums
     __shared__ bool last;
     const int r = blockIdx.y;
     const int per = (n + gridDim.x - 1) / gridDim.x;
@@ -62,7 +63,29 @@ __global__ void __launch_bounds__(kDotThreads) multi_dot_kernel(const double* __
         const int kb = 8 * grp, kn = min(8, nk - kb);
         const size_t vstride = (size_t) nrhs * n;
         const double* vb = V + ((size_t) (k0 + kb) * nrhs + r) * n;
-        for (int i = i0 + 32 * slice + lane; i < i1; i += 32 * wpg) {
+        const int step = 32 * wpg;
+        int i = i0 + 32 * slice + lane;
+        // two rows per pass: the 18 loads are all issued before the FMAs, which keep the
+        // one-row-at-a-time order of each lane's sums
+        for (; i + step < i1; i += 2 * step) {
+            const double wa = wr[i], wb = wr[i + step];
+            double va[8], vc[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if (q < kn) {
+                    va[q] = vb[q * vstride + i];
+                    vc[q] = vb[q * vstride + i + step];
+                }
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if (q < kn)
+                    acc[q] = fma(va[q], wa, acc[q]);
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if (q < kn)
+                    acc[q] = fma(vc[q], wb, acc[q]);
+        }
+        if (i < i1) {
             const double wi = wr[i];
 #pragma unroll
             for (int q = 0; q < 8; q++)
@@ -96,12 +119,28 @@ __global__ void __launch_bounds__(kDotThreads) multi_dot_kernel(const double* __
     if (!last)
         return;
     __threadfence();
-    for (int k = threadIdx.x; k < nk; k += blockDim.x) {
-        double s = 0.;
-        for (int b = 0; b < (int) gridDim.x; b++)
-            s += __ldcg(partial + ((size_t) r * 64 + k) * gridDim.x + b);
-        h[(size_t) r * hs + k0 + k] = s;
+    const int nb = (int) gridDim.x;
+    const double* pr = partial + (size_t) r * 64 * nb;  // partial[r][k][b] for k < nk is contiguous
+    if (nb <= kDotBlocks) {
+        // the slices' sums go to shared memory with parallel loads (rows padded by one against
+        // bank conflicts); each thread then sums its k in block order as below
+        for (int t = threadIdx.x; t < nk * nb; t += blockDim.x)
+            s_part[(t / nb) * (nb + 1) + t % nb] = __ldcg(pr + t);
+        __syncthreads();
+        for (int k = threadIdx.x; k < nk; k += blockDim.x) {
+            double s = 0.;
+            for (int b = 0; b < nb; b++)
+                s += s_part[k * (nb + 1) + b];
+            h[(size_t) r * hs + k0 + k] = s;
+        }
     }
+    else
+        for (int k = threadIdx.x; k < nk; k += blockDim.x) {
+            double s = 0.;
+            for (int b = 0; b < nb; b++)
+                s += __ldcg(pr + (size_t) k * nb + b);
+            h[(size_t) r * hs + k0 + k] = s;
+        }
     if (threadIdx.x == 0)
         counter[r] = 0u;
 }
