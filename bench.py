@@ -578,6 +578,24 @@ def profile_fftm_matvec():
                           "ms": ctx.last_kernel_ms}), flush=True)
 
 
+def profile_refinement():
+    """profiling case for ncu: the refinement solve of KEMCU_SOLVE_ASSEMBLED (FP32 inner GMRES,
+    FP64 residuals) on a 24,000-triangle stacked-ring mesh (8 rings of 60 x 25 x 2 triangles,
+    a 6.9 GB operator pair) with 8 right-hand sides to 1e-10; the first solve assembles, the
+    second is the one to read"""
+    import kassiopeia_b200 as K
+    from kassiopeia_b200 import geometry as G
+
+    ctx = K.CUDAElectrostaticContext(int(os.environ.get("LOCAL_RANK", 0)), autotune=False)
+    rings = G.stacked_rings(n_phi=60, n_z=25)
+    ctx.SetGeometry(rings)
+    B = G.ring_potentials(rings, n_rhs=8)
+    for _ in range(2):
+        _, st = ctx.Solve(B, tol=TOL, mode=K.SOLVE_ASSEMBLED)
+        print(json.dumps({"refinement_solve": "24,000 triangles, 8 right-hand sides", "seconds": st["seconds"],
+                          "iterations": st["iterations"], "rel_residual": st["rel_residual"]}), flush=True)
+
+
 def profile_axisym():
     import kassiopeia_b200 as K
     from kassiopeia_b200 import geometry as G
@@ -668,6 +686,9 @@ def main():
     ap.add_argument("--profile-fftm-matvec", action="store_true",
                     help="profiling case for ncu: fast multipole operator products (coax; configuration 5 with 8 "
                          "right-hand sides)")
+    ap.add_argument("--profile-refinement", action="store_true",
+                    help="profiling case for ncu: the assembled refinement solve (FP32 inner GMRES) of a "
+                         "24,000-triangle stacked-ring mesh with 8 right-hand sides, twice")
     ap.add_argument("--tracking-c3", action="store_true",
                     help="configuration 3 as configured: 65,536 electrons to the end of every track (hit or "
                          "10,000 steps) in launches of --c3-chunk steps; prints one JSON line (several minutes)")
@@ -686,6 +707,9 @@ def main():
         return
     if args.profile_fftm_matvec:
         profile_fftm_matvec()
+        return
+    if args.profile_refinement:
+        profile_refinement()
         return
     if args.profile_operator:
         profile_operator()
